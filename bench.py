@@ -1,0 +1,410 @@
+#!/usr/bin/env python
+"""Benchmark: effective TFLOP/s (2MNK/t) of a fast algorithm vs classical GEMM on B200.
+
+Default workload: fast424_26_206 (<4,2,4;26> with common-subexpression
+elimination, namespace grey424_26_206), 16384 x 16384 x 16384, 2 recursive
+steps, FP64, seeded uniform [0, 1) inputs (A: stream 1, B: stream 2), alpha 1,
+beta 0.  One step = one FastMatmul of the whole product.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 (launched by torch.distributed.run): independent replicas, one per GPU
+(the product does not shard across GPUs); the only collectives are the
+barrier and the max over ranks of the timed region.
+
+Reported beside the headline: the engine's own classical FP64 GEMM and
+cuBLAS DGEMM on the same matrices, the error of the result against the
+classical product, per-phase kernel times with their roofline, an end-to-end
+number through the host-memory C entry point, clocks sampled during the
+timed region, and the reference's CPU path on a bounded sample.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "effective TFLOP/s (2MNK/t) fast vs classical GEMM, same B200, at stated error"
+NOMINAL_FP64_TFLOPS = 40.0
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--alg", default="grey424_26_206")
+    ap.add_argument("--num-steps", type=int, default=2)
+    ap.add_argument("--m", type=int, default=16384)
+    ap.add_argument("--k", type=int, default=16384)
+    ap.add_argument("--n", type=int, default=16384)
+    ap.add_argument("--schedule", default="auto", choices=["auto", "dfs", "bfs", "hybrid"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample", type=int, default=4096, help="edge of the CPU baseline sample")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU work budget of the baseline sample")
+    a = ap.parse_args(argv)
+    if a.warmup < 3 and a.impl == "ours":
+        a.warmup = 3
+    return a
+
+
+def workload_name(a):
+    return "%s %dx%dx%d, %d recursive steps, FP64, uniform[0,1)" % (a.alg, a.m, a.k, a.n, a.num_steps)
+
+
+# ---------------------------------------------------------------------------
+# reference CPU path (the oracle/_ref build of the reference's own headers)
+
+
+def cpu_reference_sample(alg, num_steps, edge, seconds, max_runs=None):
+    """Times the reference's FastMatmul on an edge^3 sample with all host
+    threads; returns (median ms, runs, threads)."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle  # the CPU baseline leg may load the reference build
+
+    if not oracle.ref_available():
+        raise RuntimeError("oracle/_ref/libfmm_ref.so is not built")
+    threads = os.cpu_count() or 1
+    oracle.ref_lib().fmmref_set_threads(threads)
+    A = oracle.uniform(edge, edge, 7, 1)
+    B = oracle.uniform(edge, edge, 7, 2)
+    C = oracle.uniform(edge, edge, 7, 3)
+    times = []
+    t_end = time.time() + seconds
+    oracle.ref_fast_matmul(alg, A, B, C, num_steps)  # warm (page faults, thread pool)
+    while time.time() < t_end or len(times) < 2:
+        t0 = time.perf_counter()
+        oracle.ref_fast_matmul(alg, A, B, C, num_steps)
+        times.append((time.perf_counter() - t0) * 1e3)
+        if max_runs and len(times) >= max_runs:
+            break
+    return statistics.median(times), len(times), threads
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    edge = a.cpu_sample
+    sample = "%s %d^3, %d recursive steps, uniform[0,1), median of timed runs" % (a.alg, edge, a.num_steps)
+    flops = 2.0 * edge ** 3
+    try:
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+        import oracle
+
+        if not oracle.ref_available():
+            raise RuntimeError("reference build oracle/_ref is missing")
+        threads = os.cpu_count() or 1
+        oracle.ref_lib().fmmref_set_threads(threads)
+        A = oracle.uniform(edge, edge, 7, 1)
+        B = oracle.uniform(edge, edge, 7, 2)
+        C = oracle.uniform(edge, edge, 7, 3)
+        for _ in range(a.warmup):
+            oracle.ref_fast_matmul(a.alg, A, B, C, a.num_steps)
+        times = []
+        for _ in range(a.steps):
+            t0 = time.perf_counter()
+            oracle.ref_fast_matmul(a.alg, A, B, C, a.num_steps)
+            times.append((time.perf_counter() - t0) * 1e3)
+    except Exception as ex:  # noqa: BLE001
+        print(json.dumps({"impl": "reference", "unavailable": str(ex)}))
+        return 0
+    ms = sum(times) / len(times)
+    value = flops / (ms * 1e-3) / 1e12
+    out = {
+        "impl": "reference",
+        "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": a.gpus, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": workload_name(a), "sample": sample, "parallelism": "host threads"},
+        "cpu_baseline": {"value": value, "unit": "TFLOP/s", "cores": threads, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# clocks
+
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:  # noqa: BLE001
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.3)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as fh:
+            for line in fh:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx = float(parts[2])
+                except ValueError:
+                    continue
+                for nm, val in zip(names, parts[5:9]):
+                    if val.lower().startswith("active"):
+                        reasons.add(nm)
+        os.unlink(self.path)
+        # samples under load: the upper part of the distribution (the
+        # sampler also sees the idle moments around the region)
+        busy = sorted(sm)[len(sm) // 4:] if sm else []
+        return {"sm_mhz": statistics.median(busy) if busy else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# our engine
+
+
+def measured_peaks():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            return json.load(fh), "measured"
+    except Exception:  # noqa: BLE001
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def committed_traffic():
+    """Per-launch DRAM bytes of the leaf GEMM from the committed ncu summary."""
+    path = os.path.join(REPO, "profiles", "roofline_traffic.json")
+    try:
+        with open(path) as fh:
+            return json.load(fh)
+    except Exception:  # noqa: BLE001
+        return None
+
+
+def run_ours(a):
+    import torch
+    import torch.distributed as dist
+
+    import fast_matmul_b200 as fmm
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    m, k, n = a.m, a.k, a.n
+    h = fmm.default_handle(local)
+    A = fmm.random_matrix(m, k, 1234 + rank, 1, device=local)
+    B = fmm.random_matrix(k, n, 1234 + rank, 2, device=local)
+    C = fmm.colmajor_empty(m, n, torch.device("cuda", local))
+    flops = 2.0 * m * n * k
+
+    def step():
+        fmm.fast_matmul(a.alg, A, B, C, a.num_steps, schedule=a.schedule, handle=h)
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.4)
+    h.profile(True)
+    h.profile_reset()
+    launches0 = h.launches()
+    barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(a.steps):
+        step()
+    ev1.record()
+    torch.cuda.synchronize()
+    barrier()
+    elapsed_ms = ev0.elapsed_time(ev1)
+    launches = h.launches() - launches0
+    prof = h.profile_read()
+    h.profile(False)
+    clk = clocks.stop()
+
+    t = torch.tensor([elapsed_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    t_max = float(t.item())
+    ms_step = t_max / a.steps
+    value = world * flops * a.steps / (t_max * 1e-3) / 1e12
+
+    # ---- classical comparators and error (outside the timed region)
+    Cc = fmm.colmajor_empty(m, n, torch.device("cuda", local))
+    fmm.matmul(A, B, Cc, handle=h)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    reps = 2
+    e0.record()
+    for _ in range(reps):
+        fmm.matmul(A, B, Cc, handle=h)
+    e1.record()
+    torch.cuda.synchronize()
+    classical_tf = flops * reps / (e0.elapsed_time(e1) * 1e-3) / 1e12
+    rel, absd = fmm.max_relative_diff(Cc, C, handle=h)
+    At, Bt = A, B
+    Ct = torch.matmul(At, Bt)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(reps):
+        torch.matmul(At, Bt, out=Ct)
+    e1.record()
+    torch.cuda.synchronize()
+    cublas_tf = flops * reps / (e0.elapsed_time(e1) * 1e-3) / 1e12
+    rel_cublas, _ = fmm.max_relative_diff(Ct.t().contiguous().t(), C, handle=h)
+    del Ct
+
+    # ---- end to end through the host-memory C entry point
+    e2e = None
+    if not a.no_e2e:
+        Ah = torch.empty((k, m), dtype=torch.float64, pin_memory=True).t()
+        Bh = torch.empty((n, k), dtype=torch.float64, pin_memory=True).t()
+        Ch = torch.empty((n, m), dtype=torch.float64, pin_memory=True).t()
+        Ah.copy_(A)
+        Bh.copy_(B)
+        fmm.fast_matmul_host(a.alg, Ah, Bh, Ch, a.num_steps, schedule=a.schedule, handle=h)  # warm
+        e2e_steps = max(2, min(a.steps, 3))
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            fmm.fast_matmul_host(a.alg, Ah, Bh, Ch, a.num_steps, schedule=a.schedule, handle=h)
+        e2e_s = time.perf_counter() - t0
+        te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e2e_s = float(te.item())
+        e2e = {"value": world * flops * e2e_steps / e2e_s / 1e12, "unit": "TFLOP/s",
+               "h2d_bytes_per_step": 8 * (m * k + k * n), "d2h_bytes_per_step": 8 * m * n,
+               "ms_per_step": e2e_s * 1e3 / e2e_steps, "api": "fmm_fast_matmul_host (include/fmm.h)"}
+        del Ah, Bh, Ch
+
+    # ---- roofline of the dominant kernel (grouped leaf FP64 GEMM)
+    peaks, peak_src = measured_peaks()
+    gemm_launches = max(prof["gemm_launches"], 1)
+    gemm_tf = prof["gemm_flops"] / (prof["gemm_ms"] * 1e-3) / 1e12 if prof["gemm_ms"] else 0.0
+    traffic = committed_traffic()
+    roofline = {
+        "kernel": "grouped_dgemm_kernel (leaf products)",
+        "bound": "tensor", "achieved": gemm_tf, "peak": cublas_tf, "unit": "TFLOP/s",
+        "frac": gemm_tf / cublas_tf if cublas_tf else None,
+        "peak_source": "cuBLAS DGEMM %dx%dx%d measured in this run (no FP64 figure in MEASURED_PEAKS.json); "
+                       "nominal B200 FP64 %.0f TFLOP/s" % (m, k, n, NOMINAL_FP64_TFLOPS),
+        "frac_of_nominal": gemm_tf / NOMINAL_FP64_TFLOPS,
+        "flops_per_launch": prof["gemm_flops"] / gemm_launches,
+        "ms_per_launch": prof["gemm_ms"] / gemm_launches,
+        "traffic": (traffic or {}).get("bytes_per_launch"),
+        "traffic_source": (traffic or {}).get("source"),
+    }
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    phases = {
+        "form": {"launches": prof["form_launches"], "ms": prof["form_ms"],
+                 "GB/s": prof["form_bytes"] / (prof["form_ms"] * 1e-3) / 1e9 if prof["form_ms"] else None},
+        "combine": {"launches": prof["combine_launches"], "ms": prof["combine_ms"],
+                    "GB/s": prof["combine_bytes"] / (prof["combine_ms"] * 1e-3) / 1e9 if prof["combine_ms"] else None},
+        "leaf_gemm": {"launches": prof["gemm_launches"], "ms": prof["gemm_ms"], "TFLOP/s": gemm_tf},
+        "peel_gemm": {"launches": prof["peel_launches"], "ms": prof["peel_ms"]},
+        "hbm_peak_gbs": hbm, "hbm_peak_source": peak_src,
+    }
+
+    out = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not a.no_cpu_baseline:
+            try:
+                ms_cpu, runs, threads = cpu_reference_sample(a.alg, a.num_steps, a.cpu_sample, a.cpu_seconds)
+                cpu = {"value": 2.0 * a.cpu_sample ** 3 / (ms_cpu * 1e-3) / 1e12, "unit": "TFLOP/s",
+                       "cores": threads, "kind": "reference",
+                       "sample": "%s %d^3, %d recursive steps, median of %d runs, host BLAS with %d threads"
+                                 % (a.alg, a.cpu_sample, a.num_steps, runs, threads)}
+            except Exception as ex:  # noqa: BLE001
+                cpu = {"value": None, "unit": "TFLOP/s", "cores": None, "kind": "reference",
+                       "sample": "unavailable: %s" % ex}
+        info = fmm.algorithm_info(a.alg)
+        out = {
+            "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": workload_name(a), "algorithm": info["name"],
+                       "base_case": "<%d,%d,%d;%d>" % (info["m0"], info["k0"], info["n0"], info["rank"]),
+                       "m": m, "k": k, "n": n, "num_steps": a.num_steps, "schedule": a.schedule,
+                       "precision": "fp64", "parallelism": "replicas" if world > 1 else "single GPU",
+                       "l2": "inputs larger than L2 (each operand %.1f GiB > 126 MB)" % (8.0 * m * k / 2**30)},
+            "error": {"max_rel_diff_vs_classical": rel, "max_abs_diff_vs_classical": absd,
+                      "max_rel_diff_vs_cublas": rel_cublas},
+            "classical": {"engine_dgemm_tflops": classical_tf, "cublas_dgemm_tflops": cublas_tf,
+                          "speedup_vs_engine_classical": value / world / classical_tf,
+                          "speedup_vs_cublas": value / world / cublas_tf},
+            "roofline": roofline,
+            "phases": phases,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "gpu_launches": launches,
+            "workspace_bytes": fmm.workspace_bytes(a.alg, m, k, n, a.num_steps, a.schedule, handle=h),
+        }
+        print(json.dumps(out))
+    if world > 1:
+        barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main(argv=None):
+    a = parse_args(argv)
+    if a.impl == "reference":
+        return run_reference(a)
+    return run_ours(a)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,23 @@
+"""B200-native fast matrix multiplication (Strassen-like recursive algorithms).
+
+The engine is libfmm.so (CUDA for sm_100a behind the C ABI in include/fmm.h);
+this package builds it and exposes the reference's operator surface to
+Python.  See api.py.
+"""
+
+from ._lib import FmmError, lib  # noqa: F401
+from .api import (  # noqa: F401
+    Handle,
+    algorithm_index,
+    algorithm_info,
+    algorithm_names,
+    colmajor_empty,
+    default_handle,
+    fast_matmul,
+    fast_matmul_host,
+    matmul,
+    max_relative_diff,
+    num_algorithms,
+    random_matrix,
+    workspace_bytes,
+)

@@ -1,0 +1,130 @@
+"""ctypes binding of libfmm.so (the C ABI declared in include/fmm.h).
+
+The library is built in-tree by ``python -m fast_matmul_b200.build``.  There
+is no fallback: if the library is missing or a call fails, an exception
+says so.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libfmm.so")
+
+_lock = threading.Lock()
+_lib = None
+
+c_double_p = ctypes.POINTER(ctypes.c_double)
+
+FMM_OK = 0
+STATUS_NAMES = {
+    0: "FMM_OK",
+    1: "FMM_ERR_INVALID_ARGUMENT",
+    2: "FMM_ERR_UNKNOWN_ALGORITHM",
+    3: "FMM_ERR_OUT_OF_MEMORY",
+    4: "FMM_ERR_CUDA",
+    5: "FMM_ERR_NOT_SUPPORTED",
+    6: "FMM_ERR_WORKSPACE_TOO_SMALL",
+    7: "FMM_ERR_TIMEOUT",
+}
+
+SCHEDULES = {"auto": 0, "dfs": 1, "bfs": 2, "hybrid": 3}
+PRECISIONS = {"fp64": 0, "split_bf16": 1}
+
+
+class FmmError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__("%s: %s" % (STATUS_NAMES.get(status, str(status)), message))
+        self.status = status
+
+
+class Options(ctypes.Structure):
+    _fields_ = [
+        ("schedule", ctypes.c_int),
+        ("precision", ctypes.c_int),
+        ("split_slices", ctypes.c_int),
+        ("dfs_levels", ctypes.c_int),
+        ("workspace_limit", ctypes.c_size_t),
+    ]
+
+
+class Profile(ctypes.Structure):
+    _fields_ = [
+        ("form_launches", ctypes.c_int64), ("gemm_launches", ctypes.c_int64),
+        ("peel_launches", ctypes.c_int64), ("combine_launches", ctypes.c_int64),
+        ("form_ms", ctypes.c_double), ("gemm_ms", ctypes.c_double),
+        ("peel_ms", ctypes.c_double), ("combine_ms", ctypes.c_double),
+        ("form_bytes", ctypes.c_double), ("combine_bytes", ctypes.c_double),
+        ("gemm_flops", ctypes.c_double), ("peel_flops", ctypes.c_double),
+    ]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+# name -> (restype, argtypes); every function declared in include/fmm.h
+SIGNATURES = {
+    "fmm_options_init": (None, [ctypes.POINTER(Options)]),
+    "fmm_handle_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int]),
+    "fmm_handle_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "fmm_set_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "fmm_set_workspace_limit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t]),
+    "fmm_last_error": (ctypes.c_char_p, []),
+    "fmm_num_algorithms": (ctypes.c_int, []),
+    "fmm_algorithm_name": (ctypes.c_char_p, [ctypes.c_int]),
+    "fmm_algorithm_header": (ctypes.c_char_p, [ctypes.c_int]),
+    "fmm_algorithm_lookup": (ctypes.c_int, [ctypes.c_char_p]),
+    "fmm_algorithm_info": (ctypes.c_int, [ctypes.c_int] + [ctypes.POINTER(ctypes.c_int)] * 5),
+    "fmm_fast_matmul": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int64,
+                                        ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64,
+                                        ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int,
+                                        ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                        ctypes.POINTER(Options)]),
+    "fmm_fast_matmul_host": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int64,
+                                             ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64,
+                                             ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int,
+                                             ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                             ctypes.POINTER(Options), c_double_p]),
+    "fmm_workspace_query": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_int64,
+                                            ctypes.c_int64, ctypes.c_int, ctypes.POINTER(Options),
+                                            ctypes.POINTER(ctypes.c_size_t)]),
+    "fmm_dgemm": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+                                  ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
+                                  ctypes.c_int64, ctypes.c_int64, ctypes.c_double, ctypes.c_double]),
+    "fmm_fill_uniform": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
+                                         ctypes.c_int64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_double,
+                                         ctypes.c_double]),
+    "fmm_max_relative_diff": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+                                              ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, c_double_p,
+                                              c_double_p]),
+    "fmm_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
+    "fmm_kernel_launch_count": (ctypes.c_int64, [ctypes.c_void_p]),
+    "fmm_profile_enable": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "fmm_profile_reset": (ctypes.c_int, [ctypes.c_void_p]),
+    "fmm_profile_read": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Profile)]),
+}
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded engine library; raises if it has not been built."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError("%s is missing: build it with `python -m fast_matmul_b200.build`" % LIB_PATH)
+            L = ctypes.CDLL(LIB_PATH)
+            for name, (res, args) in SIGNATURES.items():
+                fn = getattr(L, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = L
+        return _lib
+
+
+def check(status: int) -> None:
+    if status != FMM_OK:
+        msg = lib().fmm_last_error()
+        raise FmmError(status, msg.decode() if msg else "")

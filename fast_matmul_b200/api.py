@@ -1,0 +1,272 @@
+"""Python surface of the engine, mirroring the reference's operator API.
+
+The reference's user-facing calls are, per algorithm namespace,
+``<ns>::FastMatmul(A, B, C, num_steps, x, alpha, beta)``
+(algorithms/strassen.hpp:661-722), the classical ``MatMul(A, B, C, beta)``
+(linalg/linalg.hpp:261-269), ``RandomMatrix`` (linalg/linalg.hpp:422-433) and
+``MaxRelativeDiff`` (linalg/linalg.hpp:280-295).  The same names are exposed
+here over column-major FP64 matrices held in CUDA memory as torch tensors
+(``A.stride(0) == 1``, leading dimension ``A.stride(1)``); PyTorch only
+provides the memory and the stream -- all arithmetic runs in libfmm.so.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import threading
+from typing import Dict, Optional, Tuple
+
+from . import _lib
+from ._lib import Options, check, lib
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+# ---------------------------------------------------------------------------
+# algorithm registry
+
+
+def num_algorithms() -> int:
+    return lib().fmm_num_algorithms()
+
+
+def algorithm_names():
+    L = lib()
+    return [L.fmm_algorithm_name(i).decode() for i in range(L.fmm_num_algorithms())]
+
+
+def algorithm_index(name) -> int:
+    """Index of an algorithm by namespace (``grey424_26_206``), header
+    (``fast424_26_206.hpp``) or header stem (``fast424_26_206``)."""
+    if isinstance(name, int):
+        if not 0 <= name < num_algorithms():
+            raise _lib.FmmError(2, "unknown algorithm index %d" % name)
+        return name
+    idx = lib().fmm_algorithm_lookup(name.encode())
+    if idx < 0:
+        raise _lib.FmmError(2, "unknown algorithm %r" % name)
+    return idx
+
+
+def algorithm_info(name) -> Dict[str, int]:
+    idx = algorithm_index(name)
+    vals = [ctypes.c_int() for _ in range(5)]
+    check(lib().fmm_algorithm_info(idx, *[ctypes.byref(v) for v in vals]))
+    m0, k0, n0, rank, approx = [v.value for v in vals]
+    return {"index": idx, "name": lib().fmm_algorithm_name(idx).decode(), "m0": m0, "k0": k0, "n0": n0,
+            "rank": rank, "approximate": bool(approx)}
+
+
+# ---------------------------------------------------------------------------
+# handles
+
+
+class Handle:
+    """An engine handle on one device (fmm_handle_create / fmm_handle_destroy)."""
+
+    def __init__(self, device: int = 0):
+        self._h = ctypes.c_void_p()
+        check(lib().fmm_handle_create(ctypes.byref(self._h), device))
+        self.device = device
+
+    @property
+    def ptr(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            lib().fmm_handle_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def set_stream(self, stream_ptr: int):
+        check(lib().fmm_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
+
+    def bind_current_stream(self):
+        torch = _torch()
+        self.set_stream(torch.cuda.current_stream(self.device).cuda_stream)
+
+    def set_workspace_limit(self, nbytes: int):
+        check(lib().fmm_set_workspace_limit(self._h, nbytes))
+
+    def launches(self) -> int:
+        return int(lib().fmm_kernel_launch_count(self._h))
+
+    def synchronize(self):
+        check(lib().fmm_synchronize(self._h))
+
+    def profile(self, enable: bool = True):
+        """Bracket every launch with CUDA events (per-phase timing)."""
+        check(lib().fmm_profile_enable(self._h, 1 if enable else 0))
+
+    def profile_reset(self):
+        check(lib().fmm_profile_reset(self._h))
+
+    def profile_read(self) -> dict:
+        p = _lib.Profile()
+        check(lib().fmm_profile_read(self._h, ctypes.byref(p)))
+        return p.as_dict()
+
+
+_tls = threading.local()
+
+
+def default_handle(device: Optional[int] = None) -> Handle:
+    """The calling thread's handle for `device`, bound to torch's current stream."""
+    torch = _torch()
+    if device is None:
+        device = torch.cuda.current_device()
+    handles = getattr(_tls, "handles", None)
+    if handles is None:
+        handles = _tls.handles = {}
+    h = handles.get(device)
+    if h is None:
+        h = handles[device] = Handle(device)
+    h.bind_current_stream()
+    return h
+
+
+# ---------------------------------------------------------------------------
+# matrices
+
+
+def colmajor_empty(m: int, n: int, device="cuda"):
+    """Uninitialised column-major m x n FP64 matrix (leading dimension m)."""
+    torch = _torch()
+    return torch.empty((n, m), dtype=torch.float64, device=device).t()
+
+
+def _mat(t, rows: int, cols: int, name: str) -> Tuple[int, int]:
+    torch = _torch()
+    if t.dtype != torch.float64:
+        raise TypeError("%s must be float64" % name)
+    if tuple(t.shape) != (rows, cols):
+        raise ValueError("%s has shape %s, expected %s" % (name, tuple(t.shape), (rows, cols)))
+    if rows > 1 and cols > 1 and t.stride(0) != 1:
+        raise ValueError("%s must be column-major (stride(0) == 1)" % name)
+    ld = t.stride(1) if cols > 1 else max(rows, 1)
+    return t.data_ptr(), max(ld, rows, 1)
+
+
+def _options(schedule="auto", dfs_levels=-1, workspace_limit=0, precision="fp64", split_slices=0) -> Options:
+    o = Options()
+    lib().fmm_options_init(ctypes.byref(o))
+    o.schedule = _lib.SCHEDULES[schedule]
+    o.precision = _lib.PRECISIONS[precision]
+    o.split_slices = split_slices
+    o.dfs_levels = dfs_levels
+    o.workspace_limit = workspace_limit
+    return o
+
+
+def fast_matmul(alg, A, B, C, num_steps: int, x: float = 1e-8, alpha: float = 1.0, beta: float = 0.0,
+                schedule: str = "auto", dfs_levels: int = -1, workspace_limit: int = 0,
+                handle: Optional[Handle] = None) -> None:
+    """C := alpha * A * B + beta * C with `num_steps` levels of algorithm
+    `alg` -- <alg>::FastMatmul(A, B, C, num_steps, x, alpha, beta).
+    Queued on torch's current stream."""
+    idx = algorithm_index(alg)
+    m, k = A.shape
+    k2, n = B.shape
+    if k2 != k:
+        raise ValueError("inner dimensions differ")
+    pa, lda = _mat(A, m, k, "A")
+    pb, ldb = _mat(B, k, n, "B")
+    pc, ldc = _mat(C, m, n, "C")
+    h = handle or default_handle(C.device.index)
+    o = _options(schedule, dfs_levels, workspace_limit)
+    check(lib().fmm_fast_matmul(h.ptr, idx, pa, lda, pb, ldb, pc, ldc, m, k, n, num_steps, x, alpha, beta,
+                                ctypes.byref(o)))
+
+
+def workspace_bytes(alg, m: int, k: int, n: int, num_steps: int, schedule: str = "auto", dfs_levels: int = -1,
+                    workspace_limit: int = 0, handle: Optional[Handle] = None) -> int:
+    h = handle or default_handle()
+    o = _options(schedule, dfs_levels, workspace_limit)
+    out = ctypes.c_size_t()
+    check(lib().fmm_workspace_query(h.ptr, algorithm_index(alg), m, k, n, num_steps, ctypes.byref(o),
+                                    ctypes.byref(out)))
+    return out.value
+
+
+def fast_matmul_host(alg, A, B, C, num_steps: int, x: float = 1e-8, alpha: float = 1.0, beta: float = 0.0,
+                     schedule: str = "auto", handle: Optional[Handle] = None) -> float:
+    """Host-memory variant (fmm_fast_matmul_host): A, B, C are column-major
+    float64 host arrays (numpy, Fortran order) or CPU torch tensors; returns
+    the call's wall time in ms, copies included."""
+    import numpy as np
+
+    def info(a, rows, cols, name):
+        if hasattr(a, "data_ptr"):
+            if a.device.type != "cpu":
+                raise ValueError("%s must be in host memory" % name)
+            ld = a.stride(1) if cols > 1 else max(rows, 1)
+            if rows > 1 and cols > 1 and a.stride(0) != 1:
+                raise ValueError("%s must be column-major" % name)
+            return a.data_ptr(), max(ld, rows, 1)
+        arr = a
+        if arr.dtype != np.float64 or (rows > 1 and cols > 1 and not arr.flags.f_contiguous):
+            raise ValueError("%s must be a Fortran-ordered float64 array" % name)
+        return arr.ctypes.data, max(rows, 1)
+
+    m, k = A.shape
+    n = B.shape[1]
+    pa, lda = info(A, m, k, "A")
+    pb, ldb = info(B, k, n, "B")
+    pc, ldc = info(C, m, n, "C")
+    h = handle or default_handle()
+    o = _options(schedule)
+    ms = ctypes.c_double()
+    check(lib().fmm_fast_matmul_host(h.ptr, algorithm_index(alg), pa, lda, pb, ldb, pc, ldc, m, k, n, num_steps,
+                                     x, alpha, beta, ctypes.byref(o), ctypes.byref(ms)))
+    return ms.value
+
+
+def matmul(A, B, C, alpha: float = 1.0, beta: float = 0.0, handle: Optional[Handle] = None) -> None:
+    """Classical C := alpha * A * B + beta * C on the engine's FP64 GEMM
+    (MatMul with C's multiplier as alpha)."""
+    m, k = A.shape
+    n = B.shape[1]
+    pa, lda = _mat(A, m, k, "A")
+    pb, ldb = _mat(B, k, n, "B")
+    pc, ldc = _mat(C, m, n, "C")
+    h = handle or default_handle(C.device.index)
+    check(lib().fmm_dgemm(h.ptr, pa, lda, pb, ldb, pc, ldc, m, k, n, alpha, beta))
+
+
+def random_matrix(m: int, n: int, seed: int, stream: int = 0, lo: float = 0.0, hi: float = 1.0, device=None,
+                  handle: Optional[Handle] = None):
+    """Seeded column-major m x n matrix, entries lo + (hi - lo) * U[0, 1)."""
+    torch = _torch()
+    dev = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+    out = colmajor_empty(m, n, dev)
+    h = handle or default_handle(dev.index)
+    check(lib().fmm_fill_uniform(h.ptr, out.data_ptr(), m, n, max(m, 1), seed, stream, lo, hi))
+    return out
+
+
+def max_relative_diff(A, B, handle: Optional[Handle] = None) -> Tuple[float, float]:
+    """(max_ij |a-b|/|a|, max_ij |a-b|) -- MaxRelativeDiff and MaxAbsDiff."""
+    m, n = A.shape
+    pa, lda = _mat(A, m, n, "A")
+    pb, ldb = _mat(B, m, n, "B")
+    h = handle or default_handle(A.device.index)
+    rel = ctypes.c_double()
+    ab = ctypes.c_double()
+    check(lib().fmm_max_relative_diff(h.ptr, pa, lda, pb, ldb, m, n, ctypes.byref(rel), ctypes.byref(ab)))
+    return rel.value, ab.value

@@ -1,0 +1,83 @@
+// Runs a planned launch program on a stream (kept apart from the planner so
+// the planner also builds for host-only checking).
+
+#include "plan.h"
+
+namespace fmm {
+
+cudaEvent_t Profiler::get() {
+  if (used == pool.size()) {
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    pool.push_back(e);
+  }
+  return pool[used++];
+}
+
+void Profiler::reset() {
+  recs.clear();
+  used = 0;
+}
+
+Profiler::~Profiler() {
+  for (cudaEvent_t e : pool) cudaEventDestroy(e);
+}
+
+cudaError_t run_program(int alg, const Program& prog, const CoefSlots& cf, const void* h_desc_pinned, void* d_desc,
+                        int num_sms, cudaStream_t stream, int64_t* launches, Profiler* prof) {
+  if (!prog.desc.empty()) {
+    cudaError_t e = cudaMemcpyAsync(d_desc, h_desc_pinned, prog.desc.size(), cudaMemcpyHostToDevice, stream);
+    if (e != cudaSuccess) return e;
+  }
+  const unsigned char* base = static_cast<const unsigned char*>(d_desc);
+  int64_t count = 0;
+  for (const Op& op : prog.ops) {
+    cudaError_t e = cudaSuccess;
+    Profiler::Rec rec{op.kind, op.peel, op.flops, op.bytes, nullptr, nullptr};
+    if (prof) {
+      rec.start = prof->get();
+      rec.stop = prof->get();
+      if (!rec.start || !rec.stop) return cudaErrorMemoryAllocation;
+      cudaEventRecord(rec.start, stream);
+    }
+    switch (op.kind) {
+      case OpKind::kForm: {
+        FormLaunch L;
+        L.s_desc = reinterpret_cast<const FormDesc*>(base + op.desc_off);
+        L.t_desc = L.s_desc + op.n_s;
+        L.n_s = op.n_s;
+        L.n_t = op.n_t;
+        L.a_rows = op.a_rows;
+        L.a_cols = op.a_cols;
+        L.b_rows = op.b_rows;
+        L.b_cols = op.b_cols;
+        e = form_launch(alg, L, cf, op.vec2, num_sms, stream);
+        break;
+      }
+      case OpKind::kGemm:
+        e = gemm_launch(reinterpret_cast<const GemmDesc*>(base + op.desc_off), op.n, op.total_tiles, num_sms,
+                        stream);
+        break;
+      case OpKind::kCombine: {
+        CombineLaunch L;
+        L.desc = reinterpret_cast<const CombineDesc*>(base + op.desc_off);
+        L.n = op.n;
+        L.rows = op.rows;
+        L.cols = op.cols;
+        L.beta = op.beta;
+        e = combine_launch(alg, L, cf, op.vec2, num_sms, stream);
+        break;
+      }
+    }
+    if (e != cudaSuccess) return e;
+    if (prof) {
+      cudaEventRecord(rec.stop, stream);
+      prof->recs.push_back(rec);
+    }
+    ++count;
+  }
+  if (launches) *launches += count;
+  return cudaSuccess;
+}
+
+}  // namespace fmm

@@ -1,0 +1,546 @@
+// C ABI of the engine (include/fmm.h).  No exception crosses this boundary;
+// every entry point returns an fmm_status and leaves a message for
+// fmm_last_error() on failure.
+
+#include "fmm.h"
+
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "fmm_internal.h"
+#include "plan.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+fmm_status fail(fmm_status s, const std::string& msg) {
+  g_last_error = msg;
+  return s;
+}
+
+fmm_status cuda_fail(cudaError_t e, const char* where) {
+  return fail(FMM_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define FMM_CUDA_TRY(expr, where)            \
+  do {                                       \
+    cudaError_t e__ = (expr);                \
+    if (e__ != cudaSuccess) {                \
+      return cuda_fail(e__, where);          \
+    }                                        \
+  } while (0)
+
+// Restores the caller's current device on scope exit.
+class DeviceGuard {
+ public:
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev_) != cudaSuccess) prev_ = -1;
+    ok_ = cudaSetDevice(dev) == cudaSuccess;
+  }
+  ~DeviceGuard() {
+    if (prev_ >= 0) cudaSetDevice(prev_);
+  }
+  bool ok() const { return ok_; }
+
+ private:
+  int prev_ = -1;
+  bool ok_ = false;
+};
+
+}  // namespace
+
+struct fmm_handle_s {
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  size_t ws_limit = 0;
+  // device workspace pool (S/T/M temporaries), grown on demand
+  void* ws = nullptr;
+  size_t ws_cap = 0;
+  // launch descriptors: pinned host staging + device copy
+  void* h_desc = nullptr;
+  size_t h_desc_cap = 0;
+  void* d_desc = nullptr;
+  size_t d_desc_cap = 0;
+  cudaEvent_t desc_done = nullptr;  // staging buffer may be rewritten after this
+  bool desc_pending = false;
+  // device copies of host operands for fmm_fast_matmul_host
+  double* io = nullptr;
+  size_t io_cap = 0;
+  double* d_small = nullptr;  // two doubles for reductions
+  int64_t launches = 0;
+  fmm::Program prog;
+  bool profiling = false;
+  fmm::Profiler prof;
+};
+
+namespace {
+
+fmm_status ensure_device_buffer(fmm_handle h, void** buf, size_t* cap, size_t need, const char* what) {
+  if (need <= *cap) return FMM_OK;
+  if (*buf) {
+    // in-flight work on the handle's stream may still use the old buffer
+    FMM_CUDA_TRY(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    cudaFree(*buf);
+    *buf = nullptr;
+    *cap = 0;
+  }
+  size_t alloc = need + need / 8;
+  cudaError_t e = cudaMalloc(buf, alloc);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    e = cudaMalloc(buf, need);
+    alloc = need;
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *buf = nullptr;
+    return fail(FMM_ERR_OUT_OF_MEMORY, std::string("cannot allocate ") + std::to_string(need) + " bytes of " + what);
+  }
+  *cap = alloc;
+  return FMM_OK;
+}
+
+fmm_status stage_descriptors(fmm_handle h, const fmm::Program& prog) {
+  const size_t need = prog.desc.size();
+  if (need == 0) return FMM_OK;
+  if (h->desc_pending) {
+    FMM_CUDA_TRY(cudaEventSynchronize(h->desc_done), "cudaEventSynchronize");
+    h->desc_pending = false;
+  }
+  if (need > h->h_desc_cap) {
+    if (h->h_desc) cudaFreeHost(h->h_desc);
+    h->h_desc = nullptr;
+    h->h_desc_cap = 0;
+    const size_t alloc = need + need / 4;
+    FMM_CUDA_TRY(cudaMallocHost(&h->h_desc, alloc), "cudaMallocHost(descriptors)");
+    h->h_desc_cap = alloc;
+  }
+  fmm_status s = ensure_device_buffer(h, &h->d_desc, &h->d_desc_cap, need, "launch descriptors");
+  if (s != FMM_OK) return s;
+  std::memcpy(h->h_desc, prog.desc.data(), need);
+  return FMM_OK;
+}
+
+fmm_status run_staged(fmm_handle h, int alg, const fmm::Program& prog, const fmm::CoefSlots& cf) {
+  cudaError_t e = fmm::run_program(alg, prog, cf, h->h_desc, h->d_desc, h->num_sms, h->stream, &h->launches,
+                                   h->profiling ? &h->prof : nullptr);
+  if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+  if (!prog.desc.empty()) {
+    FMM_CUDA_TRY(cudaEventRecord(h->desc_done, h->stream), "cudaEventRecord");
+    h->desc_pending = true;
+  }
+  return FMM_OK;
+}
+
+fmm_status check_alg(int alg) {
+  if (alg < 0 || alg >= FMM_NUM_ALGORITHMS)
+    return fail(FMM_ERR_UNKNOWN_ALGORITHM, "unknown algorithm index " + std::to_string(alg));
+  return FMM_OK;
+}
+
+fmm_status check_dims(int64_t m, int64_t k, int64_t n, int64_t lda, int64_t ldb, int64_t ldc) {
+  if (m < 0 || k < 0 || n < 0) return fail(FMM_ERR_INVALID_ARGUMENT, "negative matrix dimension");
+  if (m > 2147483647 || k > 2147483647 || n > 2147483647)
+    return fail(FMM_ERR_INVALID_ARGUMENT, "matrix dimension above 2^31-1");
+  if (lda < (m > 1 ? m : 1) || ldb < (k > 1 ? k : 1) || ldc < (m > 1 ? m : 1))
+    return fail(FMM_ERR_INVALID_ARGUMENT, "leading dimension smaller than the number of rows");
+  return FMM_OK;
+}
+
+void resolve_options(const fmm_options* opts, fmm_options* out) {
+  fmm_options_init(out);
+  if (opts) *out = *opts;
+}
+
+// Depth-first levels for a schedule: the fewest that fit the limit.
+fmm_status choose_dfs_levels(fmm_handle h, int alg, int64_t m, int64_t k, int64_t n, int steps,
+                             const fmm_options& o, int* dfs_levels, size_t* bytes) {
+  const fmm_alg_table& t = fmm_algorithms[alg];
+  const size_t limit = o.workspace_limit ? o.workspace_limit : h->ws_limit;
+  auto fits = [&](int d, size_t* b) {
+    *b = fmm::workspace_bytes(t, m, k, n, steps, d);
+    return *b <= limit;
+  };
+  switch (o.schedule) {
+    case FMM_SCHEDULE_BFS:
+      *dfs_levels = 0;
+      *bytes = fmm::workspace_bytes(t, m, k, n, steps, 0);
+      break;
+    case FMM_SCHEDULE_DFS:
+      *dfs_levels = steps;
+      *bytes = fmm::workspace_bytes(t, m, k, n, steps, steps);
+      break;
+    case FMM_SCHEDULE_HYBRID:
+    case FMM_SCHEDULE_AUTO: {
+      int lo = 0;
+      if (o.schedule == FMM_SCHEDULE_HYBRID) {
+        if (o.dfs_levels >= 0) {
+          if (o.dfs_levels > steps) return fail(FMM_ERR_INVALID_ARGUMENT, "dfs_levels exceeds num_steps");
+          *dfs_levels = o.dfs_levels;
+          *bytes = fmm::workspace_bytes(t, m, k, n, steps, o.dfs_levels);
+          break;
+        }
+        // dfs_levels 0 and 1 plan identically (the root level has a single
+        // sub-problem); 2 is the first split that differs from BFS
+        lo = steps >= 3 ? 2 : 0;
+      }
+      int d = lo;
+      size_t b = 0;
+      while (d < steps && !fits(d, &b)) ++d;
+      if (d == steps) fits(d, &b);
+      *dfs_levels = d;
+      *bytes = b;
+      break;
+    }
+    default:
+      return fail(FMM_ERR_INVALID_ARGUMENT, "unknown schedule");
+  }
+  if (*bytes > limit)
+    return fail(FMM_ERR_OUT_OF_MEMORY, "workspace of " + std::to_string(*bytes) + " bytes exceeds the limit of " +
+                                           std::to_string(limit) + " bytes");
+  return FMM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void fmm_options_init(fmm_options* opts) {
+  if (!opts) return;
+  opts->schedule = FMM_SCHEDULE_AUTO;
+  opts->precision = FMM_PRECISION_FP64;
+  opts->split_slices = 0;
+  opts->dfs_levels = -1;
+  opts->workspace_limit = 0;
+}
+
+const char* fmm_last_error(void) { return g_last_error.c_str(); }
+
+fmm_status fmm_handle_create(fmm_handle* out, int device) {
+  if (!out) return fail(FMM_ERR_INVALID_ARGUMENT, "null handle pointer");
+  *out = nullptr;
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    return fail(FMM_ERR_CUDA, std::string("no CUDA device: ") + cudaGetErrorString(e));
+  }
+  if (device < 0 || device >= count) return fail(FMM_ERR_INVALID_ARGUMENT, "device index out of range");
+  DeviceGuard g(device);
+  if (!g.ok()) return fail(FMM_ERR_CUDA, "cudaSetDevice failed");
+  cudaDeviceProp prop;
+  FMM_CUDA_TRY(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
+  if (prop.major != 10)
+    return fail(FMM_ERR_NOT_SUPPORTED, std::string("device ") + prop.name + " is not sm_100 (B200)");
+  fmm_handle h = new (std::nothrow) fmm_handle_s();
+  if (!h) return fail(FMM_ERR_OUT_OF_MEMORY, "host allocation failed");
+  h->device = device;
+  h->num_sms = prop.multiProcessorCount;
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = (size_t)8 << 30;
+  h->ws_limit = (size_t)(0.6 * (double)free_b);
+  if (cudaEventCreateWithFlags(&h->desc_done, cudaEventDisableTiming) != cudaSuccess ||
+      cudaMalloc(&h->d_small, 2 * sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    if (h->desc_done) cudaEventDestroy(h->desc_done);
+    delete h;
+    return fail(FMM_ERR_CUDA, "handle setup failed");
+  }
+  *out = h;
+  return FMM_OK;
+}
+
+fmm_status fmm_handle_destroy(fmm_handle h) {
+  if (!h) return FMM_OK;
+  DeviceGuard g(h->device);
+  cudaStreamSynchronize(h->stream);
+  if (h->ws) cudaFree(h->ws);
+  if (h->d_desc) cudaFree(h->d_desc);
+  if (h->h_desc) cudaFreeHost(h->h_desc);
+  if (h->io) cudaFree(h->io);
+  if (h->d_small) cudaFree(h->d_small);
+  if (h->desc_done) cudaEventDestroy(h->desc_done);
+  delete h;
+  return FMM_OK;
+}
+
+fmm_status fmm_set_stream(fmm_handle h, void* stream) {
+  if (!h) return fail(FMM_ERR_INVALID_ARGUMENT, "null handle");
+  h->stream = static_cast<cudaStream_t>(stream);
+  return FMM_OK;
+}
+
+fmm_status fmm_set_workspace_limit(fmm_handle h, size_t bytes) {
+  if (!h) return fail(FMM_ERR_INVALID_ARGUMENT, "null handle");
+  if (bytes == 0) {
+    DeviceGuard g(h->device);
+    size_t free_b = 0, total_b = 0;
+    FMM_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+    bytes = (size_t)(0.6 * (double)(free_b + h->ws_cap));
+  }
+  h->ws_limit = bytes;
+  return FMM_OK;
+}
+
+int fmm_num_algorithms(void) { return FMM_NUM_ALGORITHMS; }
+
+const char* fmm_algorithm_name(int alg) {
+  if (alg < 0 || alg >= FMM_NUM_ALGORITHMS) return nullptr;
+  return fmm_algorithms[alg].name;
+}
+
+const char* fmm_algorithm_header(int alg) {
+  if (alg < 0 || alg >= FMM_NUM_ALGORITHMS) return nullptr;
+  return fmm_algorithms[alg].header;
+}
+
+int fmm_algorithm_lookup(const char* name) {
+  if (!name) return -1;
+  for (int i = 0; i < FMM_NUM_ALGORITHMS; ++i) {
+    if (std::strcmp(fmm_algorithms[i].name, name) == 0) return i;
+    if (std::strcmp(fmm_algorithms[i].header, name) == 0) return i;
+    // header name without the .hpp suffix, e.g. "fast424_26_206"
+    const char* hd = fmm_algorithms[i].header;
+    const size_t len = std::strlen(hd);
+    if (len > 4 && std::strlen(name) == len - 4 && std::strncmp(hd, name, len - 4) == 0) return i;
+  }
+  return -1;
+}
+
+fmm_status fmm_algorithm_info(int alg, int* m0, int* k0, int* n0, int* rank, int* approximate) {
+  fmm_status s = check_alg(alg);
+  if (s != FMM_OK) return s;
+  const fmm_alg_table& t = fmm_algorithms[alg];
+  if (m0) *m0 = t.m0;
+  if (k0) *k0 = t.k0;
+  if (n0) *n0 = t.n0;
+  if (rank) *rank = t.rank;
+  if (approximate) *approximate = t.approximate;
+  return FMM_OK;
+}
+
+fmm_status fmm_workspace_query(fmm_handle h, int alg, int64_t m, int64_t k, int64_t n, int num_steps,
+                               const fmm_options* opts, size_t* bytes) {
+  if (!h || !bytes) return fail(FMM_ERR_INVALID_ARGUMENT, "null argument");
+  fmm_status s = check_alg(alg);
+  if (s != FMM_OK) return s;
+  if (num_steps < 0) return fail(FMM_ERR_INVALID_ARGUMENT, "num_steps < 0");
+  fmm_options o;
+  resolve_options(opts, &o);
+  int d = 0;
+  return choose_dfs_levels(h, alg, m, k, n, num_steps, o, &d, bytes);
+}
+
+fmm_status fmm_fast_matmul(fmm_handle h, int alg, const double* A, int64_t lda, const double* B, int64_t ldb,
+                           double* C, int64_t ldc, int64_t m, int64_t k, int64_t n, int num_steps, double x,
+                           double alpha, double beta, const fmm_options* opts) {
+  if (!h) return fail(FMM_ERR_INVALID_ARGUMENT, "null handle");
+  fmm_status s = check_alg(alg);
+  if (s != FMM_OK) return s;
+  if ((s = check_dims(m, k, n, lda, ldb, ldc)) != FMM_OK) return s;
+  if (num_steps < 0 || num_steps > 16) return fail(FMM_ERR_INVALID_ARGUMENT, "num_steps must be in [0, 16]");
+  if (m == 0 || n == 0) return FMM_OK;
+  if (!C || (k > 0 && (!A || !B))) return fail(FMM_ERR_INVALID_ARGUMENT, "null matrix pointer");
+  fmm_options o;
+  resolve_options(opts, &o);
+  if (o.precision != FMM_PRECISION_FP64)
+    return fail(FMM_ERR_NOT_SUPPORTED, "only FMM_PRECISION_FP64 is available in this build");
+  DeviceGuard g(h->device);
+  if (!g.ok()) return fail(FMM_ERR_CUDA, "cudaSetDevice failed");
+  int d = 0;
+  size_t bytes = 0;
+  if ((s = choose_dfs_levels(h, alg, m, k, n, num_steps, o, &d, &bytes)) != FMM_OK) return s;
+  if ((s = ensure_device_buffer(h, &h->ws, &h->ws_cap, bytes ? bytes : 256, "workspace")) != FMM_OK) return s;
+  try {
+    fmm::build_program(alg, m, k, n, num_steps, x, alpha, beta, d, fmm::Operand{const_cast<double*>(A), lda},
+                       fmm::Operand{const_cast<double*>(B), ldb}, fmm::Operand{C, ldc}, h->ws, &h->prog);
+  } catch (const std::exception& ex) {
+    return fail(FMM_ERR_OUT_OF_MEMORY, std::string("planning failed: ") + ex.what());
+  }
+  if ((s = stage_descriptors(h, h->prog)) != FMM_OK) return s;
+  fmm::CoefSlots cf;
+  fmm_algorithms[alg].eval(x, cf.v);
+  return run_staged(h, alg, h->prog, cf);
+}
+
+fmm_status fmm_fast_matmul_host(fmm_handle h, int alg, const double* A, int64_t lda, const double* B, int64_t ldb,
+                                double* C, int64_t ldc, int64_t m, int64_t k, int64_t n, int num_steps, double x,
+                                double alpha, double beta, const fmm_options* opts, double* elapsed_ms) {
+  auto t0 = std::chrono::steady_clock::now();
+  if (!h) return fail(FMM_ERR_INVALID_ARGUMENT, "null handle");
+  fmm_status s = check_alg(alg);
+  if (s != FMM_OK) return s;
+  if ((s = check_dims(m, k, n, lda, ldb, ldc)) != FMM_OK) return s;
+  if (m == 0 || n == 0) {
+    if (elapsed_ms) *elapsed_ms = 0.0;
+    return FMM_OK;
+  }
+  DeviceGuard g(h->device);
+  if (!g.ok()) return fail(FMM_ERR_CUDA, "cudaSetDevice failed");
+  const size_t na = (size_t)m * (size_t)k, nb = (size_t)k * (size_t)n, nc = (size_t)m * (size_t)n;
+  void* io = h->io;
+  size_t cap = h->io_cap;
+  if ((s = ensure_device_buffer(h, &io, &cap, (na + nb + nc) * sizeof(double) + 512, "host-call operands")) != FMM_OK)
+    return s;
+  h->io = static_cast<double*>(io);
+  h->io_cap = cap;
+  double* dA = h->io;
+  double* dB = dA + ((na + 31) & ~(size_t)31);
+  double* dC = dB + ((nb + 31) & ~(size_t)31);
+  const int64_t ldA = m, ldB = k > 0 ? k : 1, ldC = m;
+  if (na)
+    FMM_CUDA_TRY(cudaMemcpy2DAsync(dA, ldA * sizeof(double), A, lda * sizeof(double), m * sizeof(double), k,
+                                   cudaMemcpyHostToDevice, h->stream),
+                 "copy A to device");
+  if (nb)
+    FMM_CUDA_TRY(cudaMemcpy2DAsync(dB, ldB * sizeof(double), B, ldb * sizeof(double), k * sizeof(double), n,
+                                   cudaMemcpyHostToDevice, h->stream),
+                 "copy B to device");
+  if (beta != 0.0 && num_steps > 0)
+    FMM_CUDA_TRY(cudaMemcpy2DAsync(dC, ldC * sizeof(double), C, ldc * sizeof(double), m * sizeof(double), n,
+                                   cudaMemcpyHostToDevice, h->stream),
+                 "copy C to device");
+  s = fmm_fast_matmul(h, alg, dA, ldA, dB, ldB, dC, ldC, m, k, n, num_steps, x, alpha, beta, opts);
+  if (s != FMM_OK) return s;
+  FMM_CUDA_TRY(cudaMemcpy2DAsync(C, ldc * sizeof(double), dC, ldC * sizeof(double), m * sizeof(double), n,
+                                 cudaMemcpyDeviceToHost, h->stream),
+               "copy C to host");
+  FMM_CUDA_TRY(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+  if (elapsed_ms)
+    *elapsed_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  return FMM_OK;
+}
+
+fmm_status fmm_dgemm(fmm_handle h, const double* A, int64_t lda, const double* B, int64_t ldb, double* C,
+                     int64_t ldc, int64_t m, int64_t k, int64_t n, double alpha, double beta) {
+  if (!h) return fail(FMM_ERR_INVALID_ARGUMENT, "null handle");
+  fmm_status s = check_dims(m, k, n, lda, ldb, ldc);
+  if (s != FMM_OK) return s;
+  if (m == 0 || n == 0) return FMM_OK;
+  if (!C || (k > 0 && (!A || !B))) return fail(FMM_ERR_INVALID_ARGUMENT, "null matrix pointer");
+  DeviceGuard g(h->device);
+  if (!g.ok()) return fail(FMM_ERR_CUDA, "cudaSetDevice failed");
+  fmm::Program& prog = h->prog;
+  prog.ops.clear();
+  prog.desc.clear();
+  fmm::GemmDesc d{};
+  d.A = A;
+  d.B = B;
+  d.C = C;
+  d.lda = lda;
+  d.ldb = ldb;
+  d.ldc = ldc;
+  d.m = (int)m;
+  d.n = (int)n;
+  d.k = (int)k;
+  d.alpha = alpha;
+  d.beta = beta;
+  const int64_t tiles = fmm::gemm_prepare(&d, 1);
+  prog.desc.resize(sizeof(d));
+  std::memcpy(prog.desc.data(), &d, sizeof(d));
+  fmm::Op op;
+  op.kind = fmm::OpKind::kGemm;
+  op.n = 1;
+  op.total_tiles = tiles;
+  op.desc_off = 0;
+  op.flops = 2.0 * (double)m * (double)n * (double)k;
+  prog.ops.push_back(op);
+  if ((s = stage_descriptors(h, prog)) != FMM_OK) return s;
+  fmm::CoefSlots cf{};
+  return run_staged(h, 0, prog, cf);
+}
+
+fmm_status fmm_fill_uniform(fmm_handle h, double* out, int64_t rows, int64_t cols, int64_t ld, uint64_t seed,
+                            uint64_t stream, double lo, double hi) {
+  if (!h) return fail(FMM_ERR_INVALID_ARGUMENT, "null handle");
+  if (rows < 0 || cols < 0 || ld < (rows > 1 ? rows : 1))
+    return fail(FMM_ERR_INVALID_ARGUMENT, "bad matrix shape");
+  if (rows * cols > 0 && !out) return fail(FMM_ERR_INVALID_ARGUMENT, "null matrix pointer");
+  DeviceGuard g(h->device);
+  FMM_CUDA_TRY(fmm::fill_uniform_launch(out, rows, cols, ld, seed, stream, lo, hi, h->stream), "fill_uniform");
+  ++h->launches;
+  return FMM_OK;
+}
+
+fmm_status fmm_max_relative_diff(fmm_handle h, const double* a, int64_t lda, const double* b, int64_t ldb,
+                                 int64_t m, int64_t n, double* max_rel, double* max_abs) {
+  if (!h) return fail(FMM_ERR_INVALID_ARGUMENT, "null handle");
+  if (m < 0 || n < 0 || lda < (m > 1 ? m : 1) || ldb < (m > 1 ? m : 1))
+    return fail(FMM_ERR_INVALID_ARGUMENT, "bad matrix shape");
+  DeviceGuard g(h->device);
+  FMM_CUDA_TRY(fmm::max_rel_diff_launch(a, lda, b, ldb, m, n, h->d_small, h->stream), "max_rel_diff");
+  ++h->launches;
+  double res[2] = {0.0, 0.0};
+  FMM_CUDA_TRY(cudaMemcpyAsync(res, h->d_small, sizeof(res), cudaMemcpyDeviceToHost, h->stream), "copy result");
+  FMM_CUDA_TRY(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+  if (max_rel) *max_rel = res[0];
+  if (max_abs) *max_abs = res[1];
+  return FMM_OK;
+}
+
+fmm_status fmm_synchronize(fmm_handle h) {
+  if (!h) return fail(FMM_ERR_INVALID_ARGUMENT, "null handle");
+  DeviceGuard g(h->device);
+  FMM_CUDA_TRY(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+  return FMM_OK;
+}
+
+int64_t fmm_kernel_launch_count(fmm_handle h) { return h ? h->launches : 0; }
+
+fmm_status fmm_profile_enable(fmm_handle h, int enable) {
+  if (!h) return fail(FMM_ERR_INVALID_ARGUMENT, "null handle");
+  h->profiling = enable != 0;
+  return FMM_OK;
+}
+
+fmm_status fmm_profile_reset(fmm_handle h) {
+  if (!h) return fail(FMM_ERR_INVALID_ARGUMENT, "null handle");
+  DeviceGuard g(h->device);
+  FMM_CUDA_TRY(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+  h->prof.reset();
+  return FMM_OK;
+}
+
+fmm_status fmm_profile_read(fmm_handle h, fmm_profile* out) {
+  if (!h || !out) return fail(FMM_ERR_INVALID_ARGUMENT, "null argument");
+  DeviceGuard g(h->device);
+  FMM_CUDA_TRY(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+  std::memset(out, 0, sizeof(*out));
+  for (const fmm::Profiler::Rec& r : h->prof.recs) {
+    float ms = 0.f;
+    FMM_CUDA_TRY(cudaEventElapsedTime(&ms, r.start, r.stop), "cudaEventElapsedTime");
+    switch (r.kind) {
+      case fmm::OpKind::kForm:
+        out->form_launches++;
+        out->form_ms += ms;
+        out->form_bytes += r.bytes;
+        break;
+      case fmm::OpKind::kCombine:
+        out->combine_launches++;
+        out->combine_ms += ms;
+        out->combine_bytes += r.bytes;
+        break;
+      case fmm::OpKind::kGemm:
+        if (r.peel) {
+          out->peel_launches++;
+          out->peel_ms += ms;
+          out->peel_flops += r.flops;
+        } else {
+          out->gemm_launches++;
+          out->gemm_ms += ms;
+          out->gemm_flops += r.flops;
+        }
+        break;
+    }
+  }
+  return FMM_OK;
+}
+
+}  // extern "C"

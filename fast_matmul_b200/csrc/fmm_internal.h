@@ -1,0 +1,92 @@
+// Internal interfaces shared by the engine's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "generated/fmm_algorithms.h"
+
+namespace fmm {
+
+// ---------------------------------------------------------------------------
+// Grouped FP64 GEMM: C_p = alpha_p * A_p * B_p + beta_p * C_p for a list of
+// problems of any shapes, all in one persistent launch (dgemm_dmma.cu).
+struct GemmDesc {
+  const double* A;
+  const double* B;
+  double* C;
+  int64_t lda, ldb, ldc;
+  int m, n, k;
+  int tiles_m;      // ceil(m / tile rows)
+  int tile_begin;   // first global tile index of this problem
+  int flags;        // bit 0: A allows 16-byte copies, bit 1: B allows 16-byte copies
+  double alpha, beta;
+};
+
+constexpr int kGemmBM = 128;
+constexpr int kGemmBN = 128;
+
+// Fills tiles_m / tile_begin / flags for descs[0..n) and returns the total
+// number of tiles.
+int64_t gemm_prepare(GemmDesc* descs, int n);
+// Launches the grouped GEMM over descs (device copy) with `total_tiles` tiles.
+cudaError_t gemm_launch(const GemmDesc* d_descs, int n, int64_t total_tiles, int num_sms, cudaStream_t stream);
+
+// ---------------------------------------------------------------------------
+// Operand formation and product combination (block_adds.cu).
+//
+// Form: for each sub-problem, read the M0*K0 (K0*N0) blocks of its input
+// operand once and write every materialised S (T) operand of the level.
+struct FormDesc {
+  const double* in;   // sub-problem's A (or B) operand, column-major
+  int64_t ld_in;
+  double* out;        // first materialised output block
+  int64_t ld_out;
+  int64_t out_stride; // distance between consecutive output blocks (doubles)
+};
+
+// Combine: for each sub-problem, read its R product blocks once and write the
+// M0*N0 blocks of its C operand (+ beta * C).
+struct CombineDesc {
+  const double* m;    // first product block M_1
+  int64_t ld_m;
+  int64_t m_stride;   // distance between consecutive product blocks (doubles)
+  double* c;          // sub-problem's C operand
+  int64_t ld_c;
+};
+
+struct CoefSlots {
+  double v[FMM_MAX_SLOTS > 0 ? FMM_MAX_SLOTS : 1];
+};
+
+struct FormLaunch {
+  const FormDesc* s_desc;  // A side
+  const FormDesc* t_desc;  // B side
+  int n_s, n_t;            // number of sub-problems on each side
+  int64_t a_rows, a_cols;  // dims of one A block (output S has the same dims)
+  int64_t b_rows, b_cols;  // dims of one B block
+};
+
+struct CombineLaunch {
+  const CombineDesc* desc;
+  int n;
+  int64_t rows, cols;  // dims of one C block (= one product block)
+  double beta;
+};
+
+cudaError_t form_launch(int alg, const FormLaunch& L, const CoefSlots& cf, bool vec2, int num_sms,
+                        cudaStream_t stream);
+cudaError_t combine_launch(int alg, const CombineLaunch& L, const CoefSlots& cf, bool vec2, int num_sms,
+                           cudaStream_t stream);
+
+// ---------------------------------------------------------------------------
+// Utilities (util_kernels.cu).
+cudaError_t fill_uniform_launch(double* out, int64_t rows, int64_t cols, int64_t ld, uint64_t seed, uint64_t stream_id,
+                                double lo, double hi, cudaStream_t stream);
+// Writes {max_rel, max_abs} as two doubles into d_out (device).
+cudaError_t max_rel_diff_launch(const double* a, int64_t lda, const double* b, int64_t ldb, int64_t m, int64_t n,
+                                double* d_out, cudaStream_t stream);
+
+}  // namespace fmm

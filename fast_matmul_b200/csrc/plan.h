@@ -1,0 +1,88 @@
+// Recursion planner: turns one FastMatmul call into a list of grouped
+// launches (operand formation, leaf products, combination, peeling) over a
+// device workspace laid out level by level.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <vector>
+
+#include "fmm_internal.h"
+
+namespace fmm {
+
+struct Operand {
+  double* ptr;
+  int64_t ld;
+};
+
+enum class OpKind { kForm, kGemm, kCombine };
+
+struct Op {
+  OpKind kind;
+  size_t desc_off = 0;  // byte offset of this launch's descriptors in Program::desc
+  int n = 0;            // descriptors
+  // form
+  int n_s = 0, n_t = 0;
+  int64_t a_rows = 0, a_cols = 0, b_rows = 0, b_cols = 0;
+  // combine
+  int64_t rows = 0, cols = 0;
+  double beta = 0.0;
+  // gemm
+  int64_t total_tiles = 0;
+  bool vec2 = false;
+  bool peel = false;     // gemm: dynamic-peeling fringe products
+  int level = 0;         // recursion level the launch belongs to (steps = leaves)
+  double flops = 0.0;    // gemm: 2 * m * n * k summed over the problems
+  double bytes = 0.0;    // form / combine: algorithmic HBM bytes (each input read once, each output written once)
+};
+
+// Per-launch timing with CUDA events (fmm_profile_* in include/fmm.h).
+struct Profiler {
+  struct Rec {
+    OpKind kind;
+    bool peel;
+    double flops, bytes;
+    cudaEvent_t start, stop;
+  };
+  std::vector<Rec> recs;
+  std::vector<cudaEvent_t> pool;
+  size_t used = 0;
+  cudaEvent_t get();
+  void reset();
+  ~Profiler();
+};
+
+struct Program {
+  std::vector<Op> ops;
+  std::vector<unsigned char> desc;
+  size_t workspace_bytes = 0;
+  int dfs_levels = 0;
+  double leaf_flops = 0.0;  // 2 * m * n * k summed over leaf products
+  double peel_flops = 0.0;
+  int64_t leaf_count = 0;
+};
+
+struct LevelDims {
+  int64_t m, k, n;
+};
+
+// Dimensions of the sub-problems at each level 0..steps (floor splitting,
+// linalg/linalg.hpp:179-184).
+std::vector<LevelDims> level_dims(const fmm_alg_table& t, int64_t m, int64_t k, int64_t n, int steps);
+
+// Workspace bytes for `dfs_levels` depth-first levels (0 = all breadth-first).
+size_t workspace_bytes(const fmm_alg_table& t, int64_t m, int64_t k, int64_t n, int steps, int dfs_levels);
+
+// Builds the launch program.  ws must hold workspace_bytes(...) bytes.
+void build_program(int alg, int64_t m, int64_t k, int64_t n, int steps, double x, double alpha, double beta,
+                   int dfs_levels, Operand A, Operand B, Operand C, void* ws, Program* out);
+
+// Runs a built program: one host-to-device copy of all descriptors to
+// d_desc (which must hold prog.desc.size() bytes), then the launches in order.
+// Returns the number of kernels launched through *launches.
+// When prof is non-null every launch is bracketed by CUDA events.
+cudaError_t run_program(int alg, const Program& prog, const CoefSlots& cf, const void* h_desc_pinned, void* d_desc,
+                        int num_sms, cudaStream_t stream, int64_t* launches, Profiler* prof = nullptr);
+
+}  // namespace fmm

@@ -1,0 +1,167 @@
+/*
+ * fmm.h -- C ABI of the B200 fast-matrix-multiplication engine (libfmm.so).
+ *
+ * Plain pointers and sizes only; no exceptions cross this boundary.  All
+ * matrices are column-major doubles, as in the reference's Matrix<Scalar>
+ * view (linalg/linalg.hpp:41-192): element (i, j) of a matrix with leading
+ * dimension ld is at ptr[i + j * ld].  Unless a function says "host", its
+ * matrix pointers are CUDA device pointers on the handle's device.
+ *
+ * The engine replaces the reference's per-algorithm entry point
+ *   template <class Scalar> double <ns>::FastMatmul(Matrix<Scalar>& A,
+ *       Matrix<Scalar>& B, Matrix<Scalar>& C, int num_steps, double x = 1e-8,
+ *       Scalar alpha = 1, Scalar beta = 0)
+ * (algorithms/strassen.hpp:661-722 and every other algorithms/*.hpp), the
+ * classical MatMul (linalg/linalg.hpp:261-269) and the error metric
+ * MaxRelativeDiff (linalg/linalg.hpp:280-295).  include/fmm/algorithms.hpp
+ * re-creates the reference's C++ surface on top of these functions.
+ */
+#ifndef FMM_H_
+#define FMM_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum fmm_status {
+  FMM_OK = 0,
+  FMM_ERR_INVALID_ARGUMENT = 1,
+  FMM_ERR_UNKNOWN_ALGORITHM = 2,
+  FMM_ERR_OUT_OF_MEMORY = 3,
+  FMM_ERR_CUDA = 4,
+  FMM_ERR_NOT_SUPPORTED = 5,
+  FMM_ERR_WORKSPACE_TOO_SMALL = 6,
+  FMM_ERR_TIMEOUT = 7
+} fmm_status;
+
+/* Recursion schedules.  The numbering follows the reference's parallel
+ * modes _DFS_PAR_=1, _BFS_PAR_=2, _HYBRID_PAR_=3 (util/common.hpp:13-15).
+ *   DFS     one sub-problem at a time at every level; the R products of a
+ *           deepest-level sub-problem go out as one grouped launch.
+ *   BFS     every level is one grouped launch over all its sub-problems
+ *           (all R^l operand formations, all R^steps leaf products).
+ *   HYBRID  depth-first over the top levels, breadth-first below; the split
+ *           is the shallowest one whose workspace fits the limit, with at
+ *           least two depth-first levels when num_steps >= 3 (one
+ *           depth-first level plans exactly like BFS, since the top level
+ *           has a single sub-problem).
+ *   AUTO    breadth-first as deep as the workspace limit allows. */
+typedef enum fmm_schedule {
+  FMM_SCHEDULE_AUTO = 0,
+  FMM_SCHEDULE_DFS = 1,
+  FMM_SCHEDULE_BFS = 2,
+  FMM_SCHEDULE_HYBRID = 3
+} fmm_schedule;
+
+typedef enum fmm_precision {
+  FMM_PRECISION_FP64 = 0,      /* leaf products in FP64 (DMMA) */
+  FMM_PRECISION_SPLIT_BF16 = 1 /* leaf products on the BF16 tensor cores over split operands */
+} fmm_precision;
+
+typedef struct fmm_handle_s* fmm_handle;
+
+typedef struct fmm_options {
+  fmm_schedule schedule;    /* default FMM_SCHEDULE_AUTO */
+  fmm_precision precision;  /* default FMM_PRECISION_FP64 */
+  int split_slices;         /* BF16 slices per operand for SPLIT_BF16 (0 = default) */
+  int dfs_levels;           /* HYBRID only: depth-first levels; -1 = choose */
+  size_t workspace_limit;   /* bytes; 0 = the handle's limit */
+} fmm_options;
+
+/* Fills *opts with the defaults above. */
+void fmm_options_init(fmm_options* opts);
+
+/* Handles: one per host thread (a handle is not internally locked). */
+fmm_status fmm_handle_create(fmm_handle* out, int device);
+fmm_status fmm_handle_destroy(fmm_handle h);
+/* Stream for all work of the handle (a cudaStream_t; NULL = legacy default). */
+fmm_status fmm_set_stream(fmm_handle h, void* stream);
+/* Upper bound on the workspace the handle may allocate (0 = 60% of the
+ * device memory that is free when the handle is created). */
+fmm_status fmm_set_workspace_limit(fmm_handle h, size_t bytes);
+/* Message for the last failing call on this host thread ("" if none). */
+const char* fmm_last_error(void);
+
+/* Algorithm registry: every algorithm the reference generates headers for. */
+int fmm_num_algorithms(void);
+const char* fmm_algorithm_name(int alg); /* the reference namespace, e.g. "grey424_26_206" */
+const char* fmm_algorithm_header(int alg); /* the reference header, e.g. "fast424_26_206.hpp" */
+int fmm_algorithm_lookup(const char* name_or_header); /* -1 if unknown */
+fmm_status fmm_algorithm_info(int alg, int* m0, int* k0, int* n0, int* rank, int* approximate);
+
+/* C := alpha * A * B + beta * C with `num_steps` recursive levels of
+ * algorithm `alg` and parameter x (lambda of approximate algorithms),
+ * exactly as <ns>::FastMatmul(A, B, C, num_steps, x, alpha, beta) computes it
+ * (algorithms/strassen.hpp:661-722): the same floor sub-blocking, operand
+ * additions in the same order and rounding, multipliers folded into the leaf
+ * products' alpha, M->C combination with beta at the top level, and dynamic
+ * peeling of the fringes at every level (linalg/linalg.hpp:201-244).  As in
+ * the reference, num_steps == 0 is one classical product that ignores beta.
+ * Device pointers; runs on the handle's stream; returns once the work is
+ * queued (the call does not synchronise).  opts may be NULL. */
+fmm_status fmm_fast_matmul(fmm_handle h, int alg, const double* A, int64_t lda, const double* B, int64_t ldb,
+                           double* C, int64_t ldc, int64_t m, int64_t k, int64_t n, int num_steps, double x,
+                           double alpha, double beta, const fmm_options* opts);
+
+/* Same with HOST matrices (pageable or pinned): A, B and (when beta != 0 and
+ * num_steps > 0) C are copied to the device, the product runs, C is copied
+ * back; the call returns when C is on the host.  *elapsed_ms (may be NULL)
+ * receives the wall time of the whole call, copies included. */
+fmm_status fmm_fast_matmul_host(fmm_handle h, int alg, const double* A, int64_t lda, const double* B, int64_t ldb,
+                                double* C, int64_t ldc, int64_t m, int64_t k, int64_t n, int num_steps, double x,
+                                double alpha, double beta, const fmm_options* opts, double* elapsed_ms);
+
+/* Device workspace the call above needs (bytes), for the schedule chosen. */
+fmm_status fmm_workspace_query(fmm_handle h, int alg, int64_t m, int64_t k, int64_t n, int num_steps,
+                               const fmm_options* opts, size_t* bytes);
+
+/* Classical product C := alpha * A * B + beta * C with the engine's own FP64
+ * tensor-core GEMM (the leaf kernel); MatMul in linalg/linalg.hpp:261-269
+ * with alpha taken from C's multiplier.  beta == 0 does not read C. */
+fmm_status fmm_dgemm(fmm_handle h, const double* A, int64_t lda, const double* B, int64_t ldb, double* C,
+                     int64_t ldc, int64_t m, int64_t k, int64_t n, double alpha, double beta);
+
+/* Seeded input generator: out(i, j) = lo + (hi - lo) * u, u in [0, 1) from a
+ * counter-based splitmix64 stream (element index i + j * rows), identical to
+ * the host generator used by the tests. */
+fmm_status fmm_fill_uniform(fmm_handle h, double* out, int64_t rows, int64_t cols, int64_t ld, uint64_t seed,
+                            uint64_t stream, double lo, double hi);
+
+/* max_ij |a_ij - b_ij| / |a_ij| (MaxRelativeDiff, linalg/linalg.hpp:280-295)
+ * and max_ij |a_ij - b_ij|; blocks until the result is on the host. */
+fmm_status fmm_max_relative_diff(fmm_handle h, const double* a, int64_t lda, const double* b, int64_t ldb,
+                                 int64_t m, int64_t n, double* max_rel, double* max_abs);
+
+/* Waits for all work queued on the handle's stream. */
+fmm_status fmm_synchronize(fmm_handle h);
+
+/* Number of kernels the handle has launched since it was created. */
+int64_t fmm_kernel_launch_count(fmm_handle h);
+
+/* Per-phase timing (the reference times only the whole call,
+ * algorithms/strassen.hpp:708-721).  While enabled, every launch of
+ * fmm_fast_matmul / fmm_dgemm is bracketed by CUDA events on the handle's
+ * stream; fmm_profile_read synchronises and returns the totals since the
+ * last reset, with the algorithmic work of those launches: FLOPs of the
+ * leaf and fringe products, and HBM bytes of the operand formations and
+ * combinations counted as every input block read once and every output
+ * block written once. */
+typedef struct fmm_profile {
+  int64_t form_launches, gemm_launches, peel_launches, combine_launches;
+  double form_ms, gemm_ms, peel_ms, combine_ms;
+  double form_bytes, combine_bytes;
+  double gemm_flops, peel_flops;
+} fmm_profile;
+
+fmm_status fmm_profile_enable(fmm_handle h, int enable);
+fmm_status fmm_profile_reset(fmm_handle h);
+fmm_status fmm_profile_read(fmm_handle h, fmm_profile* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FMM_H_ */

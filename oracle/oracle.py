@@ -1,0 +1,179 @@
+"""TEST INFRASTRUCTURE ONLY -- Python access to the CPU oracle.
+
+Only tests/, the smoke check and the benchmark's CPU-baseline leg may import
+this module, and only as the checker (or, for the baseline, as the timed
+reference CPU path).  Nothing in the product imports it.
+
+  liboracle.so        plain-C restatement of the reference recursion
+                      (oracle/fmm_oracle.c); always buildable with gcc.
+  _ref/libfmm_ref.so  the reference's own headers compiled unchanged
+                      (oracle/ref_shim.cpp); built where the reference tree
+                      is available, shipped with the repository snapshot.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_LIB = os.path.join(HERE, "liboracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libfmm_ref.so")
+
+_P = ctypes.POINTER(ctypes.c_double)
+_D = ctypes.c_double
+_I = ctypes.c_int
+_L = ctypes.c_long
+
+_oracle = None
+_ref = None
+
+
+def build(ref: bool = True) -> None:
+    """Builds liboracle.so and, when the reference tree exists, _ref/libfmm_ref.so."""
+    subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
+    if ref and os.path.isdir("/root/reference/algorithms"):
+        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+
+
+def oracle_lib() -> ctypes.CDLL:
+    global _oracle
+    if _oracle is None:
+        if not os.path.exists(ORACLE_LIB):
+            build(ref=False)
+        L = ctypes.CDLL(ORACLE_LIB)
+        L.oracle_fast_matmul.argtypes = [_I, _P, _L, _P, _L, _P, _L, _I, _I, _I, _I, _D, _D, _D]
+        L.oracle_fast_matmul.restype = _I
+        L.oracle_matmul.argtypes = [_P, _L, _P, _L, _P, _L, _I, _I, _I, _D, _D]
+        L.oracle_matmul.restype = None
+        L.oracle_max_relative_diff.argtypes = [_P, _L, _P, _L, _I, _I]
+        L.oracle_max_relative_diff.restype = _D
+        L.oracle_algorithm_name.argtypes = [_I]
+        L.oracle_algorithm_name.restype = ctypes.c_char_p
+        L.oracle_algorithm_index.argtypes = [ctypes.c_char_p]
+        L.oracle_algorithm_index.restype = _I
+        L.oracle_fill_uniform.argtypes = [_P, _L, ctypes.c_uint64, ctypes.c_uint64, _D, _D]
+        L.oracle_fill_uniform.restype = None
+        L.oracle_set_leaf_gemm.argtypes = [ctypes.c_void_p]
+        L.oracle_set_leaf_gemm.restype = None
+        _oracle = L
+    return _oracle
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_LIB)
+
+
+def ref_lib() -> Optional[ctypes.CDLL]:
+    global _ref
+    if _ref is None:
+        if not ref_available():
+            return None
+        L = ctypes.CDLL(REF_LIB)
+        L.fmmref_fast_matmul.argtypes = [ctypes.c_char_p, _P, _I, _P, _I, _P, _I, _I, _I, _I, _I, _D, _D, _D]
+        L.fmmref_fast_matmul.restype = _D
+        L.fmmref_matmul.argtypes = [_P, _I, _P, _I, _P, _I, _I, _I, _I, _D, _D]
+        L.fmmref_matmul.restype = None
+        L.fmmref_set_threads.argtypes = [_I]
+        L.fmmref_set_threads.restype = None
+        L.fmmref_num_algorithms.restype = _I
+        L.fmmref_algorithm_name.argtypes = [_I]
+        L.fmmref_algorithm_name.restype = ctypes.c_char_p
+        _ref = L
+    return _ref
+
+
+def _p(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.f_contiguous
+    return a.ctypes.data_as(_P)
+
+
+# --------------------------------------------------------------------------
+# seeded inputs: counter-based splitmix64, identical to fmm_fill_uniform
+
+
+_GOLD = np.uint64(0x9E3779B97F4A7C15)
+
+
+def uniform(rows: int, cols: int, seed: int, stream: int, lo: float = 0.0, hi: float = 1.0) -> np.ndarray:
+    """Column-major rows x cols matrix; element e = i + j * rows."""
+    with np.errstate(over="ignore"):
+        key = np.uint64(seed) * np.uint64(0xD1B54A32D192ED03) + np.uint64(stream) * np.uint64(0x8CB92BA72F3D8DD7)
+        e = np.arange(1, rows * cols + 1, dtype=np.uint64)
+        z = key + e * _GOLD
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    u = (z >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+    vals = lo + (hi - lo) * u
+    return np.asfortranarray(vals.reshape(cols, rows).T)
+
+
+# --------------------------------------------------------------------------
+# calls
+
+
+def fast_matmul(alg: str, A: np.ndarray, B: np.ndarray, C: np.ndarray, num_steps: int, x: float = 1e-8,
+                alpha: float = 1.0, beta: float = 0.0) -> None:
+    """The C restatement of <alg>::FastMatmul on Fortran-ordered arrays (C in place)."""
+    L = oracle_lib()
+    idx = L.oracle_algorithm_index(alg.encode())
+    if idx < 0:
+        raise KeyError(alg)
+    m, k = A.shape
+    n = B.shape[1]
+    rc = L.oracle_fast_matmul(idx, _p(A), max(m, 1), _p(B), max(k, 1), _p(C), max(m, 1), m, k, n, num_steps, x,
+                              alpha, beta)
+    if rc != 0:
+        raise RuntimeError("oracle failed")
+
+
+def matmul(A: np.ndarray, B: np.ndarray, C: np.ndarray, alpha: float = 1.0, beta: float = 0.0) -> None:
+    L = oracle_lib()
+    m, k = A.shape
+    n = B.shape[1]
+    L.oracle_matmul(_p(A), max(m, 1), _p(B), max(k, 1), _p(C), max(m, 1), m, k, n, alpha, beta)
+
+
+def ref_fast_matmul(alg: str, A: np.ndarray, B: np.ndarray, C: np.ndarray, num_steps: int, x: float = 1e-8,
+                    alpha: float = 1.0, beta: float = 0.0) -> float:
+    """The reference itself (compiled headers + host BLAS); returns its ms."""
+    L = ref_lib()
+    if L is None:
+        raise RuntimeError("reference build oracle/_ref is not available")
+    m, k = A.shape
+    n = B.shape[1]
+    ms = L.fmmref_fast_matmul(alg.encode(), _p(A), max(m, 1), _p(B), max(k, 1), _p(C), max(m, 1), m, k, n,
+                              num_steps, x, alpha, beta)
+    if ms < 0:
+        raise KeyError(alg)
+    return ms
+
+
+def ref_matmul(A, B, C, alpha=1.0, beta=0.0) -> None:
+    L = ref_lib()
+    m, k = A.shape
+    n = B.shape[1]
+    L.fmmref_matmul(_p(A), max(m, 1), _p(B), max(k, 1), _p(C), max(m, 1), m, k, n, alpha, beta)
+
+
+def use_reference_leaf(enabled: bool) -> None:
+    """Route the restatement's leaf products through the reference's BLAS."""
+    L = oracle_lib()
+    if enabled:
+        R = ref_lib()
+        L.oracle_set_leaf_gemm(ctypes.cast(R.fmmref_matmul, ctypes.c_void_p))
+    else:
+        L.oracle_set_leaf_gemm(None)
+
+
+def max_relative_diff(a: np.ndarray, b: np.ndarray) -> float:
+    """max_ij |a_ij - b_ij| / |a_ij| (linalg/linalg.hpp:280-295), NaN terms skipped."""
+    with np.errstate(divide="ignore", invalid="ignore"):
+        r = np.abs(a - b) / np.abs(a)
+    r = r[~np.isnan(r)]
+    return float(r.max()) if r.size else 0.0

@@ -1,0 +1,113 @@
+"""Pins the CPU oracle to the reference.
+
+* the seeded generator against its known answer;
+* the C restatement against the golden vectors that the reference itself
+  produced (tests/golden/make_golden.py);
+* where the reference build oracle/_ref is present: the restatement with the
+  reference's own leaf BLAS is bit-identical to the reference for every
+  algorithm, and the reference reproduces the golden vectors bit for bit.
+"""
+
+import numpy as np
+import pytest
+
+import oracle
+from helpers import decode_matrix, load_golden
+
+G = load_golden()
+FULL = [c for c in G["cases"] if c["kind"] == "full"]
+DIGEST = [c for c in G["cases"] if c["kind"] == "digest"]
+APPROX = {"bini322_10_52_approx", "schonhage333_21_117_approx", "smirnov333_20_182_approx"}
+
+
+def inputs(c):
+    A = oracle.uniform(c["m"], c["k"], c["seed"], 1)
+    B = oracle.uniform(c["k"], c["n"], c["seed"], 2)
+    C0 = oracle.uniform(c["m"], c["n"], c["seed"], 3)
+    return A, B, C0
+
+
+def classical(A, B, C0, alpha, beta):
+    C = C0.copy(order="F")
+    oracle.matmul(A, B, C, alpha, beta)
+    return C
+
+
+def test_generator_known_answer():
+    ka = G["uniform_known_answer"]
+    got = oracle.uniform(ka["rows"], ka["cols"], ka["seed"], ka["stream"])
+    assert [float(v).hex() for v in got.T.ravel()] == ka["values"]
+
+
+def test_generator_matches_c_implementation():
+    import ctypes
+    a = oracle.uniform(7, 5, 11, 2, -1.0, 1.0)
+    b = np.zeros((7, 5), order="F")
+    oracle.oracle_lib().oracle_fill_uniform(b.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 35, 11, 2, -1.0, 1.0)
+    assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("c", FULL, ids=["%s-%dx%dx%d-s%d" % (c["alg"], c["m"], c["k"], c["n"], c["steps"]) for c in FULL])
+def test_restatement_matches_reference_golden(c):
+    A, B, C0 = inputs(c)
+    C = C0.copy(order="F")
+    oracle.fast_matmul(c["alg"], A, B, C, c["steps"], c["x"], c["alpha"], c["beta"])
+    ref = decode_matrix(c["C"], c["m"], c["n"])
+    if c["alg"] in APPROX:
+        err = oracle.max_relative_diff(classical(A, B, C0, c["alpha"], c["beta"] if c["steps"] else 0.0), C)
+        assert err <= 2.0 * c["ref_err"] + 1e-15
+    else:
+        assert oracle.max_relative_diff(ref, C) <= 1e-13
+
+
+@pytest.mark.parametrize("c", DIGEST, ids=["%s-%dx%dx%d-s%d" % (c["alg"], c["m"], c["k"], c["n"], c["steps"]) for c in DIGEST])
+def test_restatement_matches_reference_digests(c):
+    A, B, C0 = inputs(c)
+    C = C0.copy(order="F")
+    oracle.fast_matmul(c["alg"], A, B, C, c["steps"], c["x"], c["alpha"], c["beta"])
+    if c["alg"] in APPROX:
+        err = oracle.max_relative_diff(classical(A, B, C0, 1.0, 0.0), C)
+        assert err <= 2.0 * c["ref_err"] + 1e-15
+        return
+    colsum = np.array([float.fromhex(v) for v in c["colsum"]])
+    assert np.max(np.abs(C.sum(axis=0)[: len(colsum)] - colsum) / np.abs(colsum)) <= 1e-13
+    for i, j, v in c["samples"]:
+        want = float.fromhex(v)
+        assert abs(C[i, j] - want) <= 1e-13 * abs(want)
+
+
+needs_ref = pytest.mark.skipif(not oracle.ref_available(), reason="oracle/_ref not built")
+
+
+@needs_ref
+def test_reference_build_reproduces_golden():
+    oracle.ref_lib().fmmref_set_threads(1)
+    for c in FULL:
+        A, B, C0 = inputs(c)
+        C = C0.copy(order="F")
+        oracle.ref_fast_matmul(c["alg"], A, B, C, c["steps"], c["x"], c["alpha"], c["beta"])
+        assert np.array_equal(C, decode_matrix(c["C"], c["m"], c["n"])), c["alg"]
+
+
+@needs_ref
+def test_restatement_is_bit_exact_with_reference_leaves():
+    """Same leaf BLAS => every addition, multiplier and fringe identical."""
+    L = oracle.oracle_lib()
+    oracle.ref_lib().fmmref_set_threads(1)
+    oracle.use_reference_leaf(True)
+    try:
+        for i in range(L.oracle_num_algorithms()):
+            alg = L.oracle_algorithm_name(i).decode()
+            for (m, k, n, steps, alpha, beta) in [(57, 40, 35, 2, 1.0, 0.0), (30, 33, 29, 3, -1.2, 2.5),
+                                                  (67, 91, 55, 1, 7.0, -1.3)]:
+                A = oracle.uniform(m, k, 3, 1)
+                B = oracle.uniform(k, n, 3, 2)
+                C0 = oracle.uniform(m, n, 3, 3)
+                x = 1e-4 if alg in APPROX else 1e-8
+                C1 = C0.copy(order="F")
+                C2 = C0.copy(order="F")
+                oracle.ref_fast_matmul(alg, A, B, C1, steps, x, alpha, beta)
+                oracle.fast_matmul(alg, A, B, C2, steps, x, alpha, beta)
+                assert np.array_equal(C1, C2, equal_nan=True), (alg, m, k, n, steps)
+    finally:
+        oracle.use_reference_leaf(False)

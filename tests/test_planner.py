@@ -1,0 +1,82 @@
+"""The engine's planner, executed on the CPU by the test interpreter.
+
+tests/native/plan_emulator.cpp links the product planner (plan.cpp) and runs
+each planned launch on the host with the generated addition code, in a
+NaN-poisoned workspace.  Its result must equal the CPU oracle bit for bit
+for every algorithm, shape, alpha/beta and DFS/BFS/HYBRID split.
+"""
+
+import ctypes
+
+import numpy as np
+import pytest
+
+import oracle
+from helpers import emulator
+
+P = ctypes.POINTER(ctypes.c_double)
+L_ORACLE = oracle.oracle_lib()
+NAMES = [L_ORACLE.oracle_algorithm_name(i).decode() for i in range(L_ORACLE.oracle_num_algorithms())]
+APPROX = {"bini322_10_52_approx", "schonhage333_21_117_approx", "smirnov333_20_182_approx"}
+
+SHAPES = [
+    (57, 40, 35, 2, 1.0, 0.0),
+    (64, 64, 64, 2, 1.0, 0.0),
+    (101, 80, 74, 1, 7.0, -1.3),
+    (30, 33, 29, 3, -1.2, 2.5),
+    (7, 5, 3, 2, 1.0, 0.5),    # blocks of size zero: everything by peeling
+    (19, 23, 17, 0, 2.0, 3.0),  # num_steps 0: one product, beta ignored
+]
+
+
+def run_emu(E, idx, A, B, C, steps, x, alpha, beta, d):
+    m, k = A.shape
+    n = B.shape[1]
+    stats = (ctypes.c_int64 * 5)()
+    rc = E.emu_fast_matmul(idx, A.ctypes.data_as(P), m, B.ctypes.data_as(P), k, C.ctypes.data_as(P), m, m, k, n,
+                           steps, x, alpha, beta, d, stats)
+    assert rc == 0
+    return list(stats)
+
+
+@pytest.mark.parametrize("alg", NAMES)
+def test_planner_matches_oracle_bit_exact(alg):
+    E = emulator()
+    idx = NAMES.index(alg)
+    for si, (m, k, n, steps, alpha, beta) in enumerate(SHAPES):
+        A = oracle.uniform(m, k, si, 1)
+        B = oracle.uniform(k, n, si, 2)
+        C0 = oracle.uniform(m, n, si, 3)
+        x = 1e-4 if alg in APPROX else 1e-8
+        want = C0.copy(order="F")
+        oracle.fast_matmul(alg, A, B, want, steps, x, alpha, beta)
+        for d in range(steps + 1):
+            got = C0.copy(order="F")
+            run_emu(E, idx, A, B, got, steps, x, alpha, beta, d)
+            assert not np.isnan(got).any() or np.isnan(want).any()
+            assert np.array_equal(want, got, equal_nan=True), (alg, m, k, n, steps, d)
+
+
+def test_breadth_first_groups_each_level_into_one_launch():
+    E = emulator()
+    idx = NAMES.index("strassen")
+    A = oracle.uniform(64, 64, 1, 1)
+    B = oracle.uniform(64, 64, 1, 2)
+    C = np.zeros((64, 64), order="F")
+    s_bfs = run_emu(E, idx, A, B, C, 2, 1e-8, 1.0, 0.0, 0)
+    s_dfs = run_emu(E, idx, A, B, C, 2, 1e-8, 1.0, 0.0, 2)
+    # BFS: one formation + one combination per level, one leaf GEMM launch
+    assert s_bfs[:3] == [2, 1, 2] and s_bfs[3] == 49
+    # DFS: 1 + 7 formations, 7 leaf launches (7 leaves each), 7 + 1 combinations
+    assert s_dfs[:3] == [8, 7, 8] and s_dfs[3] == 49
+    assert s_bfs[4] > s_dfs[4]
+
+
+def test_workspace_scales_with_breadth_first_levels():
+    E = emulator()
+    idx = NAMES.index("grey424_26_206")
+    sizes = [E.emu_workspace_bytes(idx, 16384, 16384, 16384, 3, d) for d in range(4)]
+    # the root level has one sub-problem, so one depth-first level plans like BFS
+    assert sizes[0] == sizes[1] > sizes[2] > sizes[3] > 0
+    # the reference's MemoryManager needs ~209.7 GiB here; pure DFS needs a small fraction
+    assert sizes[3] < 20 * 2**30
