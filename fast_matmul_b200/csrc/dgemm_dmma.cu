@@ -8,12 +8,14 @@
 // for column-major operands with arbitrary leading dimensions, so sub-block
 // views and workspace buffers are used in place.
 //
-// Tile: 128 x 128 per CTA, 16-deep k slices, 4-stage cp.async pipeline
+// Tile: 128 x BN per CTA, BK-deep k slices, multi-stage cp.async pipeline
 // (16-byte copies where the operand's base and leading dimension allow it,
-// 8-byte copies otherwise, zero fill outside the matrix), 8 warps each
-// owning a 64 x 32 sub-tile as 4 x 4 m16n8k4 FP64 MMAs.  Shared-memory rows
-// are padded so that every fragment load is two wavefronts (the minimum
-// for 64-bit loads).  CTAs loop over the tiles of all problems.
+// 8-byte copies otherwise, zero fill outside the matrix), 2 x BN/32 warps
+// each owning a 64 x 32 sub-tile as 4 x 4 m16n8k16 FP64 MMAs per 16 k.  On
+// B200 the k16 form sustains about 37 TFLOP/s where m16n8k4 issues at most
+// about 29 (both measured with a register-only probe).  Shared-memory rows
+// are padded so that every fragment load is conflict-free.  CTAs loop over
+// the tiles of all problems.
 
 #include <cuda_runtime.h>
 
@@ -24,18 +26,45 @@
 namespace fmm {
 namespace {
 
-constexpr int BM = kGemmBM;
-constexpr int BN = kGemmBN;
-constexpr int BK = 16;
-constexpr int STAGES = 4;
-constexpr int THREADS = 256;
-constexpr int A_LD = BM + 8;  // doubles per k-row of the A tile   [BK][A_LD]
-constexpr int B_LD = BK + 4;  // doubles per column of the B tile  [BN][B_LD]
-constexpr int A_STAGE = BK * A_LD;
-constexpr int B_STAGE = BN * B_LD;
-constexpr size_t SMEM_BYTES = (size_t)STAGES * (A_STAGE + B_STAGE) * sizeof(double);
+// 64-bit shared loads are served per half-warp: a fragment load is
+// conflict-free when the 16 lanes of each half (4 row groups x 4 k lanes)
+// hit 16 distinct 8-byte bank pairs, i.e. when a row pitch is 32 bytes
+// modulo 128.
+//
+// BK: k-slice depth (a multiple of 16), STAGES: pipeline depth, BN: tile
+// columns, MINB: CTAs per SM, BM: tile rows, WTM: warp-tile rows (64 or 32;
+// warp tiles are WTM x 32).
+template <int BK_, int STAGES_, int BN_ = 128, int MINB_ = 1, int BM_ = 128, int WTM_ = 64>
+struct GemmCfg {
+  static constexpr int BK = BK_;
+  static constexpr int STAGES = STAGES_;
+  static constexpr int BN = BN_;
+  static constexpr int BM = BM_;
+  static constexpr int MINB = MINB_;
+  static constexpr int WTM = WTM_;
+  static constexpr int MT = WTM / 16;  // m16 tiles per warp
+  static constexpr int WARPS_M = BM / WTM;
+  static constexpr int WARPS_N = BN / 32;
+  static constexpr int THREADS = 32 * WARPS_M * WARPS_N;
+  static constexpr int A_LD = BM + 4;  // doubles per k-row of the A tile [BK][A_LD]: 32 mod 128 bytes
+  static constexpr int B_LD = BK + 4;  // doubles per column of the B tile [BN][B_LD]: 32 mod 128 bytes
+  static constexpr int A_STAGE = BK * A_LD;
+  static constexpr int B_STAGE = BN * B_LD;
+  static constexpr int A_CHUNKS = BK * BM / 2 / THREADS;  // 16-byte A copies per thread per slice
+  static constexpr int B_CHUNKS = BK * BN / 2 / THREADS;
+  static constexpr size_t SMEM_BYTES = (size_t)STAGES * (A_STAGE + B_STAGE) * sizeof(double);
+  static_assert(BK % 16 == 0, "k slices are whole m16n8k16 steps");
+  static_assert((B_LD * 8) % 128 == 32, "conflict-free B fragments");
+  static_assert(SMEM_BYTES * MINB <= 227 * 1024, "shared memory budget");
+  static_assert(THREADS % (BK / 2) == 0 && THREADS % (BM / 2) == 0, "copy mapping");
+  static_assert((A_LD * 8) % 128 == 32, "conflict-free A fragments");
+};
 
-static_assert(SMEM_BYTES <= 227 * 1024, "shared memory budget");
+// 128 x 64 tiles, 4 warps, 32-deep slices, 2 stages, two CTAs per SM: one
+// CTA's slice barrier and epilogue overlap the other's MMAs.  Measured on
+// B200 (FP64, 8192^3 and grouped 1024x4096x1024 / 2048^3): 33.7-33.9
+// TFLOP/s against 31-32 for one 8-warp CTA of 128 x 128 and 36 for cuBLAS.
+using DefaultGemmCfg = GemmCfg<32, 2, kGemmBN, 2, kGemmBM, 64>;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -49,6 +78,21 @@ __device__ __forceinline__ void cp_async8(uint32_t dst, const void* src, int src
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
 }
 
+template <class T>
+__device__ __forceinline__ T* launder(T* p) {
+  uint64_t v = reinterpret_cast<uint64_t>(p);
+  asm volatile("mov.b64 %0, %0;" : "+l"(v));
+  return reinterpret_cast<T*>(v);
+}
+__device__ __forceinline__ int64_t launder(int64_t v) {
+  asm volatile("mov.b64 %0, %0;" : "+l"(v));
+  return v;
+}
+__device__ __forceinline__ int launder(int v) {
+  asm volatile("mov.b32 %0, %0;" : "+r"(v));
+  return v;
+}
+
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 
 template <int N>
@@ -56,63 +100,100 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// D(16x8) += A(16x4, row) * B(4x8, col), FP64.
-__device__ __forceinline__ void dmma_16x8x4(double (&d)[4], double a0, double a1, double b0) {
+// D(16x8) += A(16x16, row) * B(16x8, col), FP64.  Fragments (lane = 4 * g + t):
+// a[2j] = A(g, t + 4j), a[2j+1] = A(g + 8, t + 4j), b[j] = B(t + 4j, g),
+// d[2h + q] = D(g + 8h, 2t + q).
+__device__ __forceinline__ void dmma_16x8x16(double (&d)[4], const double (&a)[8], const double (&b)[4]) {
   asm volatile(
-      "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
+      "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
+      "{%12,%13,%14,%15}, {%0,%1,%2,%3};\n"
       : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
-      : "d"(a0), "d"(a1), "d"(b0));
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]), "d"(b[0]),
+        "d"(b[1]), "d"(b[2]), "d"(b[3]));
 }
 
-__device__ __forceinline__ void load_stage(const GemmDesc& d, int row0, int col0, int kt, double* sA, double* sB,
-                                           int tid) {
+// Per-thread copy state for one tile, computed once so the descriptor is
+// not re-read inside the k loop.  Thread `tid` copies, per k slice:
+//   A: rows r2, r2+1 (r2 = 2 * (tid % (BM/2))) of slice columns
+//      kk = tid / (BM/2) + (THREADS / (BM/2)) * it,
+//   B: slice rows kk2, kk2+1 (kk2 = 2 * (tid % (BK/2))) of tile columns
+//      j = tid / (BK/2) + (THREADS / (BK/2)) * it.
+struct TileCopy {
+  const double* a;   // A(row0 + r2, tid / 64), advanced by 16 columns per slice
+  const double* b;   // B(kk2, col0 + tid / 8), advanced by 16 rows per slice
+  int64_t a_it;      // (THREADS / (BM/2)) * lda
+  int64_t b_it;      // (THREADS / (BK/2)) * ldb
+  int64_t a_slice;   // BK * lda
+  const double* a0;  // valid fallback addresses for zero-byte copies
+  const double* b0;
+  int k;             // inner dimension
+  int kk_a;          // tid / (BM/2)
+  int kk2;           // 2 * (tid % (BK/2))
+  int a_rows;        // bytes of the row pair inside the matrix: 0, 8 or 16
+  unsigned b_cols;   // bit it: the column of copy `it` lies inside the matrix
+  bool a16, b16;     // 16-byte copies allowed
+};
+
+template <class Cfg>
+__device__ __forceinline__ void load_stage(const TileCopy& tc, int kt, double* sA, double* sB, int tid) {
+  constexpr int BK = Cfg::BK;
+  constexpr int BM = Cfg::BM;
+  constexpr int A_LD = Cfg::A_LD;
+  constexpr int B_LD = Cfg::B_LD;
+  constexpr int THREADS = Cfg::THREADS;
+  constexpr int BCOLS_PER_IT = THREADS / (BK / 2);
   const int k0 = kt * BK;
-  // A slice: BK columns of BM contiguous rows.
+  const double* pa = tc.a + (int64_t)kt * tc.a_slice;
+  const double* pb = tc.b + k0;
+  const int r2 = (tid % (BM / 2)) * 2;
 #pragma unroll
-  for (int it = 0; it < 4; ++it) {
-    const int c = tid + it * THREADS;  // 0..1023
-    const int kk = c >> 6;             // 0..15
-    const int r2 = (c & 63) * 2;       // 0..126
-    const int gr = row0 + r2;
-    const int gk = k0 + kk;
+  for (int it = 0; it < Cfg::A_CHUNKS; ++it) {
+    const int kk = tc.kk_a + (THREADS / (BM / 2)) * it;
     const uint32_t dst = smem_u32(sA + kk * A_LD + r2);
-    const double* src = d.A + gr + (int64_t)gk * d.lda;
-    const bool kin = gk < d.k;
-    if (d.flags & 1) {
-      const int bytes = (kin && gr < d.m) ? ((gr + 1 < d.m) ? 16 : 8) : 0;
-      cp_async16(dst, bytes ? src : d.A, bytes);
+    const double* src = pa + it * tc.a_it;
+    const int bytes = (k0 + kk < tc.k) ? tc.a_rows : 0;
+    if (tc.a16) {
+      cp_async16(dst, bytes ? src : tc.a0, bytes);
     } else {
-      const int b0 = (kin && gr < d.m) ? 8 : 0;
-      const int b1 = (kin && gr + 1 < d.m) ? 8 : 0;
-      cp_async8(dst, b0 ? src : d.A, b0);
-      cp_async8(dst + 8, b1 ? src + 1 : d.A, b1);
+      const int b0 = bytes >= 8 ? 8 : 0;
+      const int b1 = bytes >= 16 ? 8 : 0;
+      cp_async8(dst, b0 ? src : tc.a0, b0);
+      cp_async8(dst + 8, b1 ? src + 1 : tc.a0, b1);
     }
   }
-  // B slice: BN columns, each BK contiguous k values.
+  const int gk = k0 + tc.kk2;
+  const int kbytes = gk < tc.k ? ((gk + 1 < tc.k) ? 16 : 8) : 0;
 #pragma unroll
-  for (int it = 0; it < 4; ++it) {
-    const int c = tid + it * THREADS;  // 0..1023
-    const int j = c >> 3;              // 0..127
-    const int kk2 = (c & 7) * 2;       // 0..14
-    const int gc = col0 + j;
-    const int gk = k0 + kk2;
-    const uint32_t dst = smem_u32(sB + j * B_LD + kk2);
-    const double* src = d.B + gk + (int64_t)gc * d.ldb;
-    const bool cin = gc < d.n;
-    if (d.flags & 2) {
-      const int bytes = (cin && gk < d.k) ? ((gk + 1 < d.k) ? 16 : 8) : 0;
-      cp_async16(dst, bytes ? src : d.B, bytes);
+  for (int it = 0; it < Cfg::B_CHUNKS; ++it) {
+    const int j = tid / (BK / 2) + BCOLS_PER_IT * it;
+    const uint32_t dst = smem_u32(sB + j * B_LD + tc.kk2);
+    const double* src = pb + it * tc.b_it;
+    const int bytes = ((tc.b_cols >> it) & 1) ? kbytes : 0;
+    if (tc.b16) {
+      cp_async16(dst, bytes ? src : tc.b0, bytes);
     } else {
-      const int b0 = (cin && gk < d.k) ? 8 : 0;
-      const int b1 = (cin && gk + 1 < d.k) ? 8 : 0;
-      cp_async8(dst, b0 ? src : d.B, b0);
-      cp_async8(dst + 8, b1 ? src + 1 : d.B, b1);
+      const int b0 = bytes >= 8 ? 8 : 0;
+      const int b1 = bytes >= 16 ? 8 : 0;
+      cp_async8(dst, b0 ? src : tc.b0, b0);
+      cp_async8(dst + 8, b1 ? src + 1 : tc.b0, b1);
     }
   }
 }
 
-__global__ void __launch_bounds__(THREADS, 1)
+template <class Cfg>
+__global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
     grouped_dgemm_kernel(const GemmDesc* __restrict__ descs, int nprob, int total_tiles) {
+  constexpr int BK = Cfg::BK;
+  constexpr int BM = Cfg::BM;
+  constexpr int BN = Cfg::BN;
+  constexpr int THREADS = Cfg::THREADS;
+  constexpr int MT = Cfg::MT;
+  constexpr int WTM = Cfg::WTM;
+  constexpr int A_LD = Cfg::A_LD;
+  constexpr int STAGES = Cfg::STAGES;
+  constexpr int A_STAGE = Cfg::A_STAGE;
+  constexpr int B_STAGE = Cfg::B_STAGE;
+  constexpr int B_LD = Cfg::B_LD;
   extern __shared__ __align__(128) double smem[];
   double* sA_all = smem;
   double* sB_all = smem + STAGES * A_STAGE;
@@ -122,8 +203,8 @@ __global__ void __launch_bounds__(THREADS, 1)
   const int warp = tid >> 5;
   const int g = lane >> 2;
   const int tig = lane & 3;
-  const int wm = warp & 1;   // 2 warps along M (64 rows each)
-  const int wn = warp >> 1;  // 4 warps along N (32 columns each)
+  const int wm = warp % Cfg::WARPS_M;  // warps along M (WTM rows each)
+  const int wn = warp / Cfg::WARPS_M;  // warps along N (32 columns each)
 
   for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
     // problem owning this tile: last p with tile_begin <= tile
@@ -133,15 +214,49 @@ __global__ void __launch_bounds__(THREADS, 1)
       if (descs[mid].tile_begin <= tile) lo = mid;
       else hi = mid - 1;
     }
-    const GemmDesc d = descs[lo];
+    const GemmDesc& d = descs[lo];
+    // values laundered through a register move cannot be re-read from the
+    // descriptor inside the k loop
+    const double* dA = launder(d.A);
+    const double* dB = launder(d.B);
     const int local = tile - d.tile_begin;
     const int row0 = (local % d.tiles_m) * BM;
-    const int col0 = (local / d.tiles_m) * BN;
-    const int ktiles = (d.k + BK - 1) / BK;
-
-    double acc[4][4][4];
+    const int col0 = (local / d.tiles_m) * BN;  // tiles_m / tile_begin count tiles of this BN
+    const int K = launder(d.k);
+    const int ktiles = (K + BK - 1) / BK;
+    TileCopy tc;
+    {
+      const int64_t lda = launder(d.lda), ldb = launder(d.ldb);
+      const int r2 = (tid % (BM / 2)) * 2;
+      const int gr = row0 + r2;
+      tc.a0 = dA;
+      tc.b0 = dB;
+      tc.k = K;
+      tc.kk_a = tid / (BM / 2);
+      tc.kk2 = (tid % (BK / 2)) * 2;
+      tc.a = dA + gr + (int64_t)tc.kk_a * lda;
+      tc.b = dB + tc.kk2 + (int64_t)(col0 + tid / (BK / 2)) * ldb;
+      tc.a_it = (int64_t)(THREADS / (BM / 2)) * lda;
+      tc.b_it = (int64_t)(THREADS / (BK / 2)) * ldb;
+      tc.a_slice = (int64_t)BK * lda;
+      tc.a_rows = gr < d.m ? (gr + 1 < d.m ? 16 : 8) : 0;
+      unsigned cols = 0;
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+      for (int it = 0; it < Cfg::B_CHUNKS; ++it)
+        if (col0 + tid / (BK / 2) + (THREADS / (BK / 2)) * it < d.n) cols |= 1u << it;
+      tc.b_cols = cols;
+      tc.a16 = (d.flags & 1) != 0;
+      tc.b16 = (d.flags & 2) != 0;
+    }
+    const int M = d.m, N = d.n;
+    double* const Cp = d.C;
+    const int64_t ldc = d.ldc;
+    const double alpha = d.alpha;
+    const double beta = d.beta;
+
+    double acc[MT][4][4];
+#pragma unroll
+    for (int a = 0; a < MT; ++a)
 #pragma unroll
       for (int b = 0; b < 4; ++b)
 #pragma unroll
@@ -149,7 +264,7 @@ __global__ void __launch_bounds__(THREADS, 1)
 
 #pragma unroll
     for (int s = 0; s < STAGES - 1; ++s) {
-      if (s < ktiles) load_stage(d, row0, col0, s, sA_all + s * A_STAGE, sB_all + s * B_STAGE, tid);
+      if (s < ktiles) load_stage<Cfg>(tc, s, sA_all + s * A_STAGE, sB_all + s * B_STAGE, tid);
       cp_async_commit();
     }
 
@@ -160,49 +275,50 @@ __global__ void __launch_bounds__(THREADS, 1)
         const int nk = kt + STAGES - 1;
         if (nk < ktiles) {
           const int ns = nk % STAGES;
-          load_stage(d, row0, col0, nk, sA_all + ns * A_STAGE, sB_all + ns * B_STAGE, tid);
+          load_stage<Cfg>(tc, nk, sA_all + ns * A_STAGE, sB_all + ns * B_STAGE, tid);
         }
         cp_async_commit();
       }
       const int st = kt % STAGES;
-      const double* a_base = sA_all + st * A_STAGE + tig * A_LD + wm * 64 + g;
-      const double* b_base = sB_all + st * B_STAGE + (wn * 32 + g) * B_LD + tig;
 #pragma unroll
-      for (int ks = 0; ks < BK / 4; ++ks) {
-        double af[4][2];
-        double bf[4];
+      for (int ks = 0; ks < BK / 16; ++ks) {
+        const double* a_base = sA_all + st * A_STAGE + (ks * 16 + tig) * A_LD + wm * WTM + g;
+        const double* b_base = sB_all + st * B_STAGE + (wn * 32 + g) * B_LD + ks * 16 + tig;
+        double bf[4][4];
 #pragma unroll
-        for (int mt = 0; mt < 4; ++mt) {
-          af[mt][0] = a_base[ks * 4 * A_LD + mt * 16];
-          af[mt][1] = a_base[ks * 4 * A_LD + mt * 16 + 8];
+        for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) bf[nt][j] = b_base[nt * 8 * B_LD + 4 * j];
+#pragma unroll
+        for (int mt = 0; mt < MT; ++mt) {
+          double af[8];
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            af[2 * j] = a_base[4 * j * A_LD + mt * 16];
+            af[2 * j + 1] = a_base[4 * j * A_LD + mt * 16 + 8];
+          }
+#pragma unroll
+          for (int nt = 0; nt < 4; ++nt) dmma_16x8x16(acc[mt][nt], af, bf[nt]);
         }
-#pragma unroll
-        for (int nt = 0; nt < 4; ++nt) bf[nt] = b_base[nt * 8 * B_LD + ks * 4];
-#pragma unroll
-        for (int mt = 0; mt < 4; ++mt)
-#pragma unroll
-          for (int nt = 0; nt < 4; ++nt) dmma_16x8x4(acc[mt][nt], af[mt][0], af[mt][1], bf[nt]);
       }
     }
     cp_async_wait<0>();
     __syncthreads();  // shared buffers are refilled by the next tile
 
     // epilogue: C = alpha * acc + beta * C
-    const double alpha = d.alpha;
-    const double beta = d.beta;
 #pragma unroll
-    for (int mt = 0; mt < 4; ++mt) {
+    for (int mt = 0; mt < MT; ++mt) {
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
-        const int r = row0 + wm * 64 + mt * 16 + g + h * 8;
-        if (r >= d.m) continue;
+        const int r = row0 + wm * WTM + mt * 16 + g + h * 8;
+        if (r >= M) continue;
 #pragma unroll
         for (int nt = 0; nt < 4; ++nt) {
 #pragma unroll
           for (int q = 0; q < 2; ++q) {
             const int cidx = col0 + wn * 32 + nt * 8 + tig * 2 + q;
-            if (cidx < d.n) {
-              double* cp = d.C + r + (int64_t)cidx * d.ldc;
+            if (cidx < N) {
+              double* cp = Cp + r + (int64_t)cidx * ldc;
               double v = alpha * acc[mt][nt][h * 2 + q];
               if (beta != 0.0) v += beta * *cp;
               *cp = v;
@@ -216,14 +332,20 @@ __global__ void __launch_bounds__(THREADS, 1)
 
 }  // namespace
 
-cudaError_t gemm_launch(const GemmDesc* d_descs, int n, int64_t total_tiles, int num_sms, cudaStream_t stream) {
+template <class Cfg>
+cudaError_t gemm_launch_cfg(const GemmDesc* d_descs, int n, int64_t total_tiles, int num_sms, cudaStream_t stream) {
   if (total_tiles <= 0 || n <= 0) return cudaSuccess;
-  cudaError_t err = cudaFuncSetAttribute(grouped_dgemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)SMEM_BYTES);
+  cudaError_t err = cudaFuncSetAttribute(grouped_dgemm_kernel<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)Cfg::SMEM_BYTES);
   if (err != cudaSuccess) return err;
-  const int64_t grid = total_tiles < num_sms ? total_tiles : num_sms;
-  grouped_dgemm_kernel<<<(unsigned)grid, THREADS, SMEM_BYTES, stream>>>(d_descs, n, (int)total_tiles);
+  const int64_t slots = (int64_t)num_sms * Cfg::MINB;
+  const int64_t grid = total_tiles < slots ? total_tiles : slots;
+  grouped_dgemm_kernel<Cfg><<<(unsigned)grid, Cfg::THREADS, Cfg::SMEM_BYTES, stream>>>(d_descs, n, (int)total_tiles);
   return cudaGetLastError();
+}
+
+cudaError_t gemm_launch(const GemmDesc* d_descs, int n, int64_t total_tiles, int num_sms, cudaStream_t stream) {
+  return gemm_launch_cfg<DefaultGemmCfg>(d_descs, n, total_tiles, num_sms, stream);
 }
 
 }  // namespace fmm

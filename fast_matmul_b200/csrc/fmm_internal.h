@@ -26,11 +26,11 @@ struct GemmDesc {
 };
 
 constexpr int kGemmBM = 128;
-constexpr int kGemmBN = 128;
+constexpr int kGemmBN = 64;   // tile columns of the launched configuration
 
 // Fills tiles_m / tile_begin / flags for descs[0..n) and returns the total
-// number of tiles.
-int64_t gemm_prepare(GemmDesc* descs, int n);
+// number of tile_m x tile_n tiles.
+int64_t gemm_prepare(GemmDesc* descs, int n, int tile_n = kGemmBN, int tile_m = kGemmBM);
 // Launches the grouped GEMM over descs (device copy) with `total_tiles` tiles.
 cudaError_t gemm_launch(const GemmDesc* d_descs, int n, int64_t total_tiles, int num_sms, cudaStream_t stream);
 

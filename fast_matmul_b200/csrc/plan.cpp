@@ -336,12 +336,12 @@ class Builder {
 
 }  // namespace
 
-int64_t gemm_prepare(GemmDesc* descs, int n) {
+int64_t gemm_prepare(GemmDesc* descs, int n, int tile_n, int tile_m) {
   int64_t total = 0;
   for (int i = 0; i < n; ++i) {
     GemmDesc& d = descs[i];
-    const int tm = (d.m + kGemmBM - 1) / kGemmBM;
-    const int tn = (d.n + kGemmBN - 1) / kGemmBN;
+    const int tm = (d.m + tile_m - 1) / tile_m;
+    const int tn = (d.n + tile_n - 1) / tile_n;
     d.tiles_m = tm > 0 ? tm : 1;
     d.tile_begin = (int)total;
     int flags = 0;

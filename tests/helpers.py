@@ -75,3 +75,11 @@ def to_device(a):
 
 def to_host(t):
     return np.asfortranarray(t.t().contiguous().cpu().numpy().T)
+
+
+def colmajor_copy(t):
+    """A new column-major tensor with t's values (never an alias of t)."""
+    import torch
+    out = torch.empty((t.shape[1], t.shape[0]), dtype=t.dtype, device=t.device).t()
+    out.copy_(t)
+    return out

@@ -17,7 +17,7 @@ import numpy as np
 import pytest
 
 import oracle
-from helpers import decode_matrix, default_x, gpu_available, load_golden, to_device, to_host
+from helpers import colmajor_copy, decode_matrix, default_x, gpu_available, load_golden, to_device, to_host
 
 pytestmark = pytest.mark.gpu
 
@@ -140,11 +140,13 @@ def test_schedules_are_bit_identical(alg, shape, steps):
     C0 = to_device(oracle.uniform(m, n, 41, 3))
     outs = []
     for sched, d in [("bfs", -1), ("dfs", -1), ("hybrid", 2), ("auto", -1)]:
-        C = C0.t().contiguous().t()
+        C = colmajor_copy(C0)
         fmm.fast_matmul(alg, A, B, C, steps, default_x(alg, steps), 1.5, 0.25, schedule=sched, dfs_levels=d)
         outs.append(C)
     torch.cuda.synchronize()
+    assert not torch.equal(outs[0], C0)
     for o in outs[1:]:
+        assert o.data_ptr() != outs[0].data_ptr()
         assert torch.equal(outs[0], o)
 
 

@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 import oracle
-from helpers import gpu_available, to_device, to_host
+from helpers import colmajor_copy, gpu_available, to_device, to_host
 
 pytestmark = pytest.mark.gpu
 
@@ -21,7 +21,7 @@ TOL = 1e-12
 
 def cm(t):
     """Column-major copy of a torch matrix."""
-    return t.t().contiguous().t()
+    return colmajor_copy(t)
 
 
 def view(m, n, seed, stream, offset=0, pad=0):
