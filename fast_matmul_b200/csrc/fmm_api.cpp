@@ -457,6 +457,47 @@ fmm_status fmm_dgemm(fmm_handle h, const double* A, int64_t lda, const double* B
   return run_staged(h, 0, prog, cf);
 }
 
+fmm_status fmm_dgemm_host(fmm_handle h, const double* A, int64_t lda, const double* B, int64_t ldb, double* C,
+                          int64_t ldc, int64_t m, int64_t k, int64_t n, double alpha, double beta) {
+  if (!h) return fail(FMM_ERR_INVALID_ARGUMENT, "null handle");
+  fmm_status s = check_dims(m, k, n, lda, ldb, ldc);
+  if (s != FMM_OK) return s;
+  if (m == 0 || n == 0) return FMM_OK;
+  if (!C || (k > 0 && (!A || !B))) return fail(FMM_ERR_INVALID_ARGUMENT, "null matrix pointer");
+  DeviceGuard g(h->device);
+  if (!g.ok()) return fail(FMM_ERR_CUDA, "cudaSetDevice failed");
+  const size_t na = (size_t)m * (size_t)k, nb = (size_t)k * (size_t)n, nc = (size_t)m * (size_t)n;
+  void* io = h->io;
+  size_t cap = h->io_cap;
+  if ((s = ensure_device_buffer(h, &io, &cap, (na + nb + nc) * sizeof(double) + 512, "host-call operands")) != FMM_OK)
+    return s;
+  h->io = static_cast<double*>(io);
+  h->io_cap = cap;
+  double* dA = h->io;
+  double* dB = dA + ((na + 31) & ~(size_t)31);
+  double* dC = dB + ((nb + 31) & ~(size_t)31);
+  const int64_t ldA = m, ldB = k > 0 ? k : 1, ldC = m;
+  if (na)
+    FMM_CUDA_TRY(cudaMemcpy2DAsync(dA, ldA * sizeof(double), A, lda * sizeof(double), m * sizeof(double), k,
+                                   cudaMemcpyHostToDevice, h->stream),
+                 "copy A to device");
+  if (nb)
+    FMM_CUDA_TRY(cudaMemcpy2DAsync(dB, ldB * sizeof(double), B, ldb * sizeof(double), k * sizeof(double), n,
+                                   cudaMemcpyHostToDevice, h->stream),
+                 "copy B to device");
+  if (beta != 0.0)
+    FMM_CUDA_TRY(cudaMemcpy2DAsync(dC, ldC * sizeof(double), C, ldc * sizeof(double), m * sizeof(double), n,
+                                   cudaMemcpyHostToDevice, h->stream),
+                 "copy C to device");
+  s = fmm_dgemm(h, dA, ldA, dB, ldB, dC, ldC, m, k, n, alpha, beta);
+  if (s != FMM_OK) return s;
+  FMM_CUDA_TRY(cudaMemcpy2DAsync(C, ldc * sizeof(double), dC, ldC * sizeof(double), m * sizeof(double), n,
+                                 cudaMemcpyDeviceToHost, h->stream),
+               "copy C to host");
+  FMM_CUDA_TRY(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+  return FMM_OK;
+}
+
 fmm_status fmm_fill_uniform(fmm_handle h, double* out, int64_t rows, int64_t cols, int64_t ld, uint64_t seed,
                             uint64_t stream, double lo, double hi) {
   if (!h) return fail(FMM_ERR_INVALID_ARGUMENT, "null handle");

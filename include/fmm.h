@@ -11,7 +11,7 @@
  *   template <class Scalar> double <ns>::FastMatmul(Matrix<Scalar>& A,
  *       Matrix<Scalar>& B, Matrix<Scalar>& C, int num_steps, double x = 1e-8,
  *       Scalar alpha = 1, Scalar beta = 0)
- * (algorithms/strassen.hpp:661-722 and every other algorithms/*.hpp), the
+ * (algorithms/strassen.hpp:661-722 and every other header in algorithms/), the
  * classical MatMul (linalg/linalg.hpp:261-269) and the error metric
  * MaxRelativeDiff (linalg/linalg.hpp:280-295).  include/fmm/algorithms.hpp
  * re-creates the reference's C++ surface on top of these functions.
@@ -123,6 +123,13 @@ fmm_status fmm_workspace_query(fmm_handle h, int alg, int64_t m, int64_t k, int6
  * with alpha taken from C's multiplier.  beta == 0 does not read C. */
 fmm_status fmm_dgemm(fmm_handle h, const double* A, int64_t lda, const double* B, int64_t ldb, double* C,
                      int64_t ldc, int64_t m, int64_t k, int64_t n, double alpha, double beta);
+
+/* Same with HOST matrices: A, B (and C when beta != 0) are copied in, the
+ * product runs on the engine's GEMM, C is copied back; returns when C is on
+ * the host.  MatMul(A, B, C, beta) of linalg/linalg.hpp:261-269 over host
+ * buffers, for the C++ adapter (include/fmm/matrix.hpp). */
+fmm_status fmm_dgemm_host(fmm_handle h, const double* A, int64_t lda, const double* B, int64_t ldb, double* C,
+                          int64_t ldc, int64_t m, int64_t k, int64_t n, double alpha, double beta);
 
 /* Seeded input generator: out(i, j) = lo + (hi - lo) * u, u in [0, 1) from a
  * counter-based splitmix64 stream (element index i + j * rows), identical to

@@ -1,0 +1,70 @@
+// Drop-in check of the C++ surface: a driver written against the
+// reference's API (RunAlgorithm, <ns>::FastMatmul, MatMul, MaxRelativeDiff,
+// RandomMatrix) built unchanged against include/fmm and libfmm.so.
+// Exit status 0 when every error is within its bound.
+#include <cstdio>
+#include <cstdlib>
+
+#include "fmm/all_algorithms.hpp"
+
+static int failures = 0;
+
+static void expect(bool ok, const char* what, double val) {
+  std::printf("%-56s %.3e %s\n", what, val, ok ? "ok" : "FAIL");
+  if (!ok) ++failures;
+}
+
+int main() {
+  std::srand(7);
+  // RunAlgorithm against classical MatMul (tests/matmul_tests.cpp:19-27 pattern)
+  const int algs[] = {STRASSEN, FAST424_26_206, FAST333_23_125, SMIRNOV333_23_128, FAST323_15_89, MKL};
+  for (int alg : algs) {
+    for (int steps = 1; steps <= 2; ++steps) {
+      Matrix<double> A = RandomMatrix<double>(402, 500);
+      Matrix<double> B = RandomMatrix<double>(500, 562);
+      Matrix<double> C1(402, 562), C2(402, 562);
+      RunAlgorithm(alg, A, B, C1, steps);
+      MatMul(A, B, C2);
+      char name[96];
+      std::snprintf(name, sizeof name, "%s steps=%d max rel diff", Alg2Str(alg).c_str(), steps);
+      expect(MaxRelativeDiff(C1, C2) <= 1e-13, name, MaxRelativeDiff(C1, C2));
+    }
+  }
+  // approximate algorithm: error of the reference's order of magnitude
+  {
+    Matrix<double> A = RandomMatrix<double>(300, 200);
+    Matrix<double> B = RandomMatrix<double>(200, 250);
+    Matrix<double> C1(300, 250), C2(300, 250);
+    RunAlgorithm(BINI322_10_52_APPROX, A, B, C1, 1);
+    MatMul(A, B, C2);
+    expect(MaxRelativeDiff(C1, C2) <= 1e-3, "BINI322_10_52_APPROX steps=1 max rel diff", MaxRelativeDiff(C1, C2));
+  }
+  // C := alpha * A * B + beta * C (tests/matmul_tests.cpp:47-135 pattern)
+  {
+    const double alpha = 7.0, beta = -1.3;
+    Matrix<double> A = RandomMatrix<double>(1001, 200);
+    Matrix<double> B = RandomMatrix<double>(200, 309);
+    Matrix<double> C1 = RandomMatrix<double>(1001, 309);
+    Matrix<double> C2 = C1;
+    C2.set_multiplier(alpha);
+    MatMul(A, B, C2, beta);
+    smirnov333_23_128::FastMatmul(A, B, C1, 2, 0, alpha, beta);
+    expect(MaxRelativeDiff(C1, C2) <= 1e-12, "smirnov333_23_128 alpha=7 beta=-1.3 max rel diff", MaxRelativeDiff(C1, C2));
+    // multiplier side effect of the reference: C keeps alpha, A and B are reset
+    expect(C1.multiplier() == alpha && A.multiplier() == 1.0 && B.multiplier() == 1.0, "multiplier side effects",
+           C1.multiplier());
+  }
+  // views: a sub-block product written into a sub-block of a larger C
+  {
+    Matrix<double> A = RandomMatrix<double>(600, 600);
+    Matrix<double> B = RandomMatrix<double>(600, 600);
+    Matrix<double> C1(600, 600), C2(600, 600);
+    Matrix<double> A11 = A.Subblock(2, 2, 1, 1), B12 = B.Subblock(2, 2, 1, 2);
+    Matrix<double> C1v = C1.Subblock(2, 2, 2, 2), C2v = C2.Subblock(2, 2, 2, 2);
+    strassen::FastMatmul(A11, B12, C1v, 2);
+    MatMul(A11, B12, C2v);
+    expect(MaxRelativeDiff(C1v, C2v) <= 1e-13, "strassen on strided views max rel diff", MaxRelativeDiff(C1v, C2v));
+  }
+  std::printf("%s\n", failures ? "FAILED" : "PASSED");
+  return failures ? 1 : 0;
+}
