@@ -105,6 +105,10 @@ SIGNATURES = {
                                               c_double_p]),
     "fmm_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
     "fmm_kernel_launch_count": (ctypes.c_int64, [ctypes.c_void_p]),
+    "fmm_fast_matmul_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+                                                ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
+                                                ctypes.c_int64, ctypes.c_int64, ctypes.c_int, ctypes.c_double,
+                                                ctypes.c_double, ctypes.c_double, ctypes.c_void_p]),
     "fmm_profile_enable": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "fmm_profile_reset": (ctypes.c_int, [ctypes.c_void_p]),
     "fmm_profile_read": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Profile)]),

@@ -55,6 +55,10 @@ class DeviceGuard {
 
 }  // namespace
 
+namespace fmm {
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace fmm
+
 struct fmm_handle_s {
   int device = 0;
   int num_sms = 148;

@@ -89,4 +89,7 @@ cudaError_t fill_uniform_launch(double* out, int64_t rows, int64_t cols, int64_t
 cudaError_t max_rel_diff_launch(const double* a, int64_t lda, const double* b, int64_t ldb, int64_t m, int64_t n,
                                 double* d_out, cudaStream_t stream);
 
+// Sets the message fmm_last_error() returns on this host thread.
+void set_last_error(const std::string& msg);
+
 }  // namespace fmm

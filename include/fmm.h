@@ -167,6 +167,38 @@ fmm_status fmm_profile_enable(fmm_handle h, int enable);
 fmm_status fmm_profile_reset(fmm_handle h);
 fmm_status fmm_profile_read(fmm_handle h, fmm_profile* out);
 
+/* Allocation-free FastMatmul.  No counterpart in the reference.
+ *
+ * For callers that may not allocate device memory at all: code whose device
+ * memory belongs to another framework's pool or to a fixed budget, and
+ * latency-critical loops where cudaMalloc's implicit device synchronisation
+ * is not acceptable.  The call computes exactly what fmm_fast_matmul
+ * computes, with the same kernels, but takes its workspace and launch
+ * descriptors from a static device array of FMM_NOALLOC_SCRATCH_BYTES that
+ * the library defines; it needs no handle and calls no cudaMalloc,
+ * cudaFree, pinned-host allocation or other device-allocating routine
+ * (host-side planning uses ordinary heap memory).
+ *
+ *  - Limit: every GPU that loads the library holds the 64 MiB array until
+ *    the process exits; 1 MiB of it holds launch descriptors, the rest the
+ *    S/T/M temporaries.  The call picks the most breadth-first schedule that
+ *    fits and returns FMM_ERR_WORKSPACE_TOO_SMALL, with the sizes in
+ *    fmm_last_error(), when even the depth-first one does not (for
+ *    Strassen with one step: dimensions up to about 1400).
+ *  - The first call on a device looks up the array's device address (with
+ *    that device current); make that first call before any stream capture.
+ *  - Every call shares the array and it keeps the last call's contents;
+ *    nothing in it has to start at zero.  Calls that overlap on the GPU
+ *    (different streams, or several host threads) race on it.
+ *  - Device pointers on the current device; the work is queued on `stream`
+ *    (a cudaStream_t, NULL = legacy default) and the call returns once it is
+ *    queued (copying the launch descriptors from host memory may first wait
+ *    for earlier work on that stream). */
+#define FMM_NOALLOC_SCRATCH_BYTES ((size_t)64 << 20)
+fmm_status fmm_fast_matmul_noalloc(int alg, const double* A, int64_t lda, const double* B, int64_t ldb, double* C,
+                                   int64_t ldc, int64_t m, int64_t k, int64_t n, int num_steps, double x,
+                                   double alpha, double beta, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
