@@ -53,6 +53,13 @@ def parse_args(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=4096, help="edge of the CPU baseline sample")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU work budget of the baseline sample")
+    ap.add_argument("--workload", default="product", choices=["product", "batch"],
+                    help="product: one large FastMatmul (the headline); batch: 4096 independent products "
+                         "with log-uniform dimensions in [64, 1024] in one CUDA-graph plan")
+    ap.add_argument("--batch-count", type=int, default=4096)
+    ap.add_argument("--sweep", action="store_true",
+                    help="time every configuration of the fast-vs-classical study (one JSON line each) "
+                         "instead of the single headline line")
     a = ap.parse_args(argv)
     if a.warmup < 3 and a.impl == "ours":
         a.warmup = 3
@@ -402,10 +409,158 @@ def run_ours(a):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# sweep over the study's configurations
+
+
+SWEEP_SHAPES = [
+    ("square 4096^3", 4096, 4096, 4096, [("strassen", (1, 2))]),
+    ("square 16384^3", 16384, 16384, 16384,
+     [("strassen", (1, 2, 3)), ("grey424_26_206", (1, 2, 3)), ("grey333_23_125", (1, 2, 3)),
+      ("smirnov333_23_128", (1, 2, 3))]),
+    ("outer-product-like 16384x1600x16384", 16384, 1600, 16384,
+     [("grey424_26_206", (1, 2, 3)), ("grey333_23_125", (1, 2, 3)), ("smirnov333_23_128", (1, 2, 3))]),
+    ("tall-skinny 65536x2400x2400", 65536, 2400, 2400,
+     [("grey424_26_206", (1, 2, 3)), ("grey333_23_125", (1, 2, 3)), ("smirnov333_23_128", (1, 2, 3))]),
+]
+
+
+def run_sweep(a):
+    import torch
+
+    import fast_matmul_b200 as fmm
+
+    torch.cuda.set_device(0)
+    h = fmm.default_handle(0)
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    for label, m, k, n, algs in SWEEP_SHAPES:
+        A = fmm.random_matrix(m, k, 11, 1)
+        B = fmm.random_matrix(k, n, 11, 2)
+        C = fmm.colmajor_empty(m, n)
+        Cc = fmm.colmajor_empty(m, n)
+        flops = 2.0 * m * n * k
+        ms_cls = timed(lambda: fmm.matmul(A, B, Cc, handle=h), 2)
+        Ct = torch.matmul(A, B)
+        ms_cub = timed(lambda: torch.matmul(A, B, out=Ct), 2)
+        del Ct
+        print(json.dumps({"sweep": label, "alg": "classical", "engine_dgemm_tflops": flops / ms_cls / 1e9,
+                          "cublas_dgemm_tflops": flops / ms_cub / 1e9}), flush=True)
+        for alg, steps_list in algs:
+            for steps in steps_list:
+                for sched in ("bfs", "hybrid", "dfs"):
+                    if sched == "hybrid" and steps < 3:
+                        continue
+                    rec = {"sweep": label, "alg": alg, "num_steps": steps, "schedule": sched}
+                    try:
+                        ws = fmm.workspace_bytes(alg, m, k, n, steps, sched, handle=h)
+                        ms = timed(lambda: fmm.fast_matmul(alg, A, B, C, steps, schedule=sched, handle=h), 2)
+                        rel, _ = fmm.max_relative_diff(Cc, C, handle=h)
+                        rec.update({"tflops_effective": flops / ms / 1e9, "ms": ms,
+                                    "speedup_vs_engine_classical": ms_cls / ms, "speedup_vs_cublas": ms_cub / ms,
+                                    "max_rel_diff_vs_classical": rel, "workspace_gib": ws / 2**30})
+                    except fmm.FmmError as ex:
+                        rec["skipped"] = str(ex)[:160]
+                    print(json.dumps(rec), flush=True)
+        del A, B, C, Cc
+        torch.cuda.empty_cache()
+    return 0
+
+
+def run_batch_workload(a):
+    """4096 independent products, M, K, N each floor(exp(U(ln 64, ln 1024))) from
+    a seed, entries uniform [-1, 1); the autotuner picks algorithm and depth
+    per shape bucket; the whole batch is one CUDA-graph plan (all leaf
+    products in one persistent grouped GEMM launch).  Compared with the same
+    products launched one call at a time."""
+    import numpy as np
+    import torch
+
+    import fast_matmul_b200 as fmm
+
+    torch.cuda.set_device(0)
+    h = fmm.default_handle(0)
+    rng = np.random.default_rng(2024)
+    dims = np.floor(np.exp(rng.uniform(np.log(64), np.log(1024), size=(a.batch_count, 3)))).astype(int)
+    probs = []
+    for i, (m, k, n) in enumerate(dims):
+        probs.append({"A": fmm.random_matrix(int(m), int(k), 7000 + i, 1, -1.0, 1.0, handle=h),
+                      "B": fmm.random_matrix(int(k), int(n), 7000 + i, 2, -1.0, 1.0, handle=h),
+                      "C": fmm.colmajor_empty(int(m), int(n)), "alg": fmm.AUTO})
+    flops = float(sum(2.0 * m * n * k for m, k, n in dims))
+    t0 = time.perf_counter()
+    fmm.autotune([tuple(int(v) for v in d) for d in dims], max_steps=1, handle=h)
+    tune_s = time.perf_counter() - t0
+    choices = {}
+    for m, k, n in dims:
+        c = fmm.autotune_choice(int(m), int(k), int(n), handle=h)
+        choices[c] = choices.get(c, 0) + 1
+    plan = fmm.Plan.for_batch(probs, handle=h)
+
+    def timed(fn, reps):
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    for _ in range(a.warmup):
+        plan.execute()
+    launches0 = h.launches()
+    ms = timed(plan.execute, a.steps)
+    launches = (h.launches() - launches0) // max(a.steps, 1)
+
+    def one_at_a_time():
+        for p, (m, k, n) in zip(probs, dims):
+            alg, steps = fmm.autotune_choice(int(m), int(k), int(n), handle=h)
+            if alg == fmm.CLASSICAL:
+                fmm.matmul(p["A"], p["B"], p["C"], handle=h)
+            else:
+                fmm.fast_matmul(alg, p["A"], p["B"], p["C"], steps, handle=h)
+
+    one_at_a_time()
+    ms_single = timed(one_at_a_time, 1)
+    out = {
+        "metric": METRIC, "value": flops / (ms * 1e-3) / 1e12, "unit": "TFLOP/s", "n_gpus": 1, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "batch of %d independent FP64 products, M,K,N log-uniform in [64,1024], "
+                               "uniform[-1,1), autotuned per shape bucket, one CUDA-graph plan" % a.batch_count,
+                   "total_gflop": flops / 1e9, "autotune_seconds": tune_s,
+                   "choices": {("classical" if k[0] == fmm.CLASSICAL else "%s/%d" % (fmm.algorithm_names()[k[0]], k[1])): v
+                               for k, v in choices.items()}},
+        "one_at_a_time": {"value": flops / (ms_single * 1e-3) / 1e12, "ms": ms_single,
+                          "speedup_of_batched": ms_single / ms},
+        "gpu_launches": launches,
+    }
+    print(json.dumps(out))
+    plan.close()
+    return 0
+
+
 def main(argv=None):
     a = parse_args(argv)
     if a.impl == "reference":
         return run_reference(a)
+    if a.sweep:
+        return run_sweep(a)
+    if a.workload == "batch":
+        return run_batch_workload(a)
     return run_ours(a)
 
 

@@ -7,7 +7,15 @@ Python.  See api.py.
 
 from ._lib import FmmError, lib  # noqa: F401
 from .api import (  # noqa: F401
+    AUTO,
+    CLASSICAL,
     Handle,
+    Plan,
+    autotune,
+    autotune_choice,
+    autotune_load,
+    autotune_table,
+    fast_matmul_batched,
     algorithm_index,
     algorithm_info,
     algorithm_names,

@@ -65,6 +65,21 @@ class Profile(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+FMM_ALG_AUTO = -1
+FMM_ALG_CLASSICAL = -2
+
+
+class BatchItem(ctypes.Structure):
+    _fields_ = [
+        ("alg", ctypes.c_int), ("num_steps", ctypes.c_int),
+        ("A", ctypes.c_void_p), ("lda", ctypes.c_int64),
+        ("B", ctypes.c_void_p), ("ldb", ctypes.c_int64),
+        ("C", ctypes.c_void_p), ("ldc", ctypes.c_int64),
+        ("m", ctypes.c_int64), ("k", ctypes.c_int64), ("n", ctypes.c_int64),
+        ("x", ctypes.c_double), ("alpha", ctypes.c_double), ("beta", ctypes.c_double),
+    ]
+
+
 # name -> (restype, argtypes); every function declared in include/fmm.h
 SIGNATURES = {
     "fmm_options_init": (None, [ctypes.POINTER(Options)]),
@@ -109,6 +124,24 @@ SIGNATURES = {
                                                 ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
                                                 ctypes.c_int64, ctypes.c_int64, ctypes.c_int, ctypes.c_double,
                                                 ctypes.c_double, ctypes.c_double, ctypes.c_void_p]),
+    "fmm_fast_matmul_batched": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(BatchItem), ctypes.c_int]),
+    "fmm_autotune_choice": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
+                                            ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    "fmm_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64), ctypes.c_int,
+                                     ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int]),
+    "fmm_autotune_export": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t,
+                                            ctypes.POINTER(ctypes.c_size_t)]),
+    "fmm_autotune_import": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),
+    "fmm_plan_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int64,
+                                        ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64,
+                                        ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int,
+                                        ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.POINTER(Options),
+                                        ctypes.POINTER(ctypes.c_void_p)]),
+    "fmm_plan_create_batched": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(BatchItem), ctypes.c_int,
+                                                ctypes.POINTER(ctypes.c_void_p)]),
+    "fmm_plan_execute": (ctypes.c_int, [ctypes.c_void_p]),
+    "fmm_plan_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "fmm_plan_kernel_count": (ctypes.c_int64, [ctypes.c_void_p]),
     "fmm_profile_enable": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "fmm_profile_reset": (ctypes.c_int, [ctypes.c_void_p]),
     "fmm_profile_read": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Profile)]),

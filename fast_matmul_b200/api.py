@@ -270,3 +270,127 @@ def max_relative_diff(A, B, handle: Optional[Handle] = None) -> Tuple[float, flo
     ab = ctypes.c_double()
     check(lib().fmm_max_relative_diff(h.ptr, pa, lda, pb, ldb, m, n, ctypes.byref(rel), ctypes.byref(ab)))
     return rel.value, ab.value
+
+
+# ---------------------------------------------------------------------------
+# batches, autotuning and CUDA-graph plans (no counterpart in the reference)
+
+CLASSICAL = _lib.FMM_ALG_CLASSICAL
+AUTO = _lib.FMM_ALG_AUTO
+
+
+def _batch_items(problems):
+    """problems: iterable of dicts with A, B, C (column-major CUDA tensors) and
+    optional alg (name, index, AUTO or CLASSICAL), num_steps, x, alpha, beta."""
+    problems = list(problems)
+    arr = (_lib.BatchItem * len(problems))()
+    for i, p in enumerate(problems):
+        A, B, C = p["A"], p["B"], p["C"]
+        m, k = A.shape
+        n = B.shape[1]
+        pa, lda = _mat(A, m, k, "A")
+        pb, ldb = _mat(B, k, n, "B")
+        pc, ldc = _mat(C, m, n, "C")
+        alg = p.get("alg", AUTO)
+        if not (isinstance(alg, int) and alg < 0):
+            alg = algorithm_index(alg)
+        it = arr[i]
+        it.alg = alg
+        it.num_steps = int(p.get("num_steps", 1))
+        it.A, it.lda, it.B, it.ldb, it.C, it.ldc = pa, lda, pb, ldb, pc, ldc
+        it.m, it.k, it.n = m, k, n
+        it.x = float(p.get("x", 1e-8))
+        it.alpha = float(p.get("alpha", 1.0))
+        it.beta = float(p.get("beta", 0.0))
+    return arr
+
+
+def fast_matmul_batched(problems, handle: Optional[Handle] = None) -> None:
+    """Independent products in one program (fmm_fast_matmul_batched)."""
+    arr = _batch_items(problems)
+    h = handle or default_handle()
+    check(lib().fmm_fast_matmul_batched(h.ptr, arr, len(arr)))
+
+
+def autotune(shapes, candidates=None, max_steps: int = 2, handle: Optional[Handle] = None) -> None:
+    flat = [int(v) for s in shapes for v in s]
+    sh = (ctypes.c_int64 * len(flat))(*flat)
+    h = handle or default_handle()
+    if candidates:
+        idx = [algorithm_index(c) for c in candidates]
+        ca = (ctypes.c_int * len(idx))(*idx)
+        check(lib().fmm_autotune(h.ptr, sh, len(shapes), ca, len(idx), max_steps))
+    else:
+        check(lib().fmm_autotune(h.ptr, sh, len(shapes), None, 0, max_steps))
+
+
+def autotune_choice(m: int, k: int, n: int, handle: Optional[Handle] = None):
+    h = handle or default_handle()
+    a = ctypes.c_int()
+    s = ctypes.c_int()
+    check(lib().fmm_autotune_choice(h.ptr, m, k, n, ctypes.byref(a), ctypes.byref(s)))
+    return a.value, s.value
+
+
+def autotune_table(handle: Optional[Handle] = None) -> str:
+    h = handle or default_handle()
+    n = ctypes.c_size_t()
+    check(lib().fmm_autotune_export(h.ptr, None, 0, ctypes.byref(n)))
+    buf = ctypes.create_string_buffer(n.value)
+    check(lib().fmm_autotune_export(h.ptr, buf, n.value, ctypes.byref(n)))
+    return buf.value.decode()
+
+
+def autotune_load(text: str, handle: Optional[Handle] = None) -> None:
+    h = handle or default_handle()
+    check(lib().fmm_autotune_import(h.ptr, text.encode()))
+
+
+class Plan:
+    """A product or batch captured once as a CUDA graph (fmm_plan_*)."""
+
+    def __init__(self, ptr, handle):
+        self._p = ptr
+        self.handle = handle
+
+    @classmethod
+    def for_product(cls, alg, A, B, C, num_steps, x=1e-8, alpha=1.0, beta=0.0, schedule="auto",
+                    handle: Optional[Handle] = None):
+        m, k = A.shape
+        n = B.shape[1]
+        pa, lda = _mat(A, m, k, "A")
+        pb, ldb = _mat(B, k, n, "B")
+        pc, ldc = _mat(C, m, n, "C")
+        h = handle or default_handle(C.device.index)
+        out = ctypes.c_void_p()
+        o = _options(schedule)
+        check(lib().fmm_plan_create(h.ptr, algorithm_index(alg), pa, lda, pb, ldb, pc, ldc, m, k, n, num_steps, x,
+                                    alpha, beta, ctypes.byref(o), ctypes.byref(out)))
+        return cls(out, h)
+
+    @classmethod
+    def for_batch(cls, problems, handle: Optional[Handle] = None):
+        arr = _batch_items(problems)
+        h = handle or default_handle()
+        out = ctypes.c_void_p()
+        check(lib().fmm_plan_create_batched(h.ptr, arr, len(arr), ctypes.byref(out)))
+        return cls(out, h)
+
+    def execute(self):
+        self.handle.bind_current_stream()
+        check(lib().fmm_plan_execute(self._p))
+
+    @property
+    def kernels(self) -> int:
+        return int(lib().fmm_plan_kernel_count(self._p))
+
+    def close(self):
+        if self._p:
+            lib().fmm_plan_destroy(self._p)
+            self._p = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,84 @@
+// Handle state and helpers shared by the C-ABI translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <string>
+#include <tuple>
+#include <utility>
+
+#include "fmm.h"
+#include "fmm_internal.h"
+#include "plan.h"
+
+#define FMM_CUDA_TRY(expr, where)                  \
+  do {                                             \
+    cudaError_t e__ = (expr);                      \
+    if (e__ != cudaSuccess) {                      \
+      return ::fmm::api::cuda_fail(e__, where);    \
+    }                                              \
+  } while (0)
+
+struct fmm_handle_s {
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  size_t ws_limit = 0;
+  // device workspace pool (S/T/M temporaries), grown on demand
+  void* ws = nullptr;
+  size_t ws_cap = 0;
+  // launch descriptors: pinned host staging + device copy
+  void* h_desc = nullptr;
+  size_t h_desc_cap = 0;
+  void* d_desc = nullptr;
+  size_t d_desc_cap = 0;
+  cudaEvent_t desc_done = nullptr;  // staging buffer may be rewritten after this
+  bool desc_pending = false;
+  // device copies of host operands for the host-memory entry points
+  double* io = nullptr;
+  size_t io_cap = 0;
+  double* d_small = nullptr;  // two doubles for reductions
+  int64_t launches = 0;
+  fmm::Program prog;
+  bool profiling = false;
+  fmm::Profiler prof;
+  // autotuner: shape bucket (ceil log2 of m, k, n) -> (algorithm or -2 for classical, steps)
+  std::map<std::tuple<int, int, int>, std::pair<int, int>> tuned;
+};
+
+namespace fmm {
+namespace api {
+
+fmm_status fail(fmm_status s, const std::string& msg);
+fmm_status cuda_fail(cudaError_t e, const char* where);
+
+// Restores the caller's current device on scope exit.
+class DeviceGuard {
+ public:
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev_) != cudaSuccess) prev_ = -1;
+    ok_ = cudaSetDevice(dev) == cudaSuccess;
+  }
+  ~DeviceGuard() {
+    if (prev_ >= 0) cudaSetDevice(prev_);
+  }
+  bool ok() const { return ok_; }
+
+ private:
+  int prev_ = -1;
+  bool ok_ = false;
+};
+
+fmm_status ensure_device_buffer(fmm_handle h, void** buf, size_t* cap, size_t need, const char* what);
+fmm_status stage_descriptors(fmm_handle h, const fmm::Program& prog);
+fmm_status run_staged(fmm_handle h, const fmm::Program& prog);
+fmm_status check_alg(int alg);
+fmm_status check_dims(int64_t m, int64_t k, int64_t n, int64_t lda, int64_t ldb, int64_t ldc);
+void resolve_options(const fmm_options* opts, fmm_options* out);
+fmm_status choose_dfs_levels(fmm_handle h, int alg, int64_t m, int64_t k, int64_t n, int steps,
+                             const fmm_options& o, int* dfs_levels, size_t* bytes);
+
+}  // namespace api
+}  // namespace fmm

@@ -72,8 +72,8 @@ __global__ void __launch_bounds__(kAddThreads) form_kernel(FormLaunch L, CoefSlo
   for (int pp = blockIdx.y; pp < nall; pp += gridDim.y) {
     const bool s_side = pp < L.n_s;
     const FormDesc d = s_side ? L.s_desc[pp] : L.t_desc[pp - L.n_s];
-    const int64_t rows = s_side ? L.a_rows : L.b_rows;
-    const int64_t cols = s_side ? L.a_cols : L.b_cols;
+    const int64_t rows = d.rows;
+    const int64_t cols = d.cols;
     const int nbc = s_side ? ALG::kK0 : ALG::kN0;
     const int64_t rows_v = rows / VEC;
     const int64_t chunks = (rows_v + kAddThreads - 1) / kAddThreads;
@@ -97,15 +97,16 @@ __global__ void __launch_bounds__(kAddThreads) form_kernel(FormLaunch L, CoefSlo
   }
 }
 
-template <class ALG, int VEC, bool BETA>
+template <class ALG, int VEC>
 __global__ void __launch_bounds__(kAddThreads) combine_kernel(CombineLaunch L, CoefSlots cf) {
   using T = typename VecT<VEC>::T;
-  const int64_t rows = L.rows, cols = L.cols;
-  const int64_t rows_v = rows / VEC;
-  const int64_t chunks = (rows_v + kAddThreads - 1) / kAddThreads;
-  const int64_t items = chunks * cols;
   for (int p = blockIdx.y; p < L.n; p += gridDim.y) {
     const CombineDesc d = L.desc[p];
+    const int64_t rows = d.rows, cols = d.cols;
+    const int64_t rows_v = rows / VEC;
+    const int64_t chunks = (rows_v + kAddThreads - 1) / kAddThreads;
+    const int64_t items = chunks * cols;
+    const bool with_beta = d.beta != 0.0;
     for (int64_t w = blockIdx.x; w < items; w += gridDim.x) {
       const int64_t j = w / chunks;
       const int64_t i = ((w - j * chunks) * kAddThreads + threadIdx.x) * VEC;
@@ -119,7 +120,10 @@ __global__ void __launch_bounds__(kAddThreads) combine_kernel(CombineLaunch L, C
       };
       auto ldc = [&](int c) -> T { return ld_block<T>(cptr(c)); };
       auto st = [&](int c, T v) { st_block<T>(cptr(c), v); };
-      ALG::template combine<T, BETA>(cf.v, L.beta, ld, ldc, st);
+      if (with_beta)
+        ALG::template combine<T, true>(cf.v, d.beta, ld, ldc, st);
+      else
+        ALG::template combine<T, false>(cf.v, 0.0, ld, ldc, st);
     }
   }
 }
@@ -139,17 +143,7 @@ template <class ALG>
 cudaError_t launch_form(const FormLaunch& L, const CoefSlots& cf, bool vec2, int num_sms, cudaStream_t stream) {
   const int nall = L.n_s + L.n_t;
   if (nall == 0) return cudaSuccess;
-  const int vec = vec2 ? 2 : 1;
-  auto items = [&](int64_t rows, int64_t cols) {
-    const int64_t rv = rows / vec;
-    return ((rv + kAddThreads - 1) / kAddThreads) * cols;
-  };
-  int64_t it = 0;
-  if (L.n_s) it = items(L.a_rows, L.a_cols);
-  if (L.n_t) {
-    const int64_t t = items(L.b_rows, L.b_cols);
-    if (t > it) it = t;
-  }
+  const int64_t it = L.max_items;
   if (it == 0) return cudaSuccess;
   dim3 grid;
   add_grid(it, nall, num_sms, &grid);
@@ -162,24 +156,13 @@ cudaError_t launch_form(const FormLaunch& L, const CoefSlots& cf, bool vec2, int
 
 template <class ALG>
 cudaError_t launch_combine(const CombineLaunch& L, const CoefSlots& cf, bool vec2, int num_sms, cudaStream_t stream) {
-  if (L.n == 0 || L.rows == 0 || L.cols == 0) return cudaSuccess;
-  const int vec = vec2 ? 2 : 1;
-  const int64_t rv = L.rows / vec;
-  const int64_t it = ((rv + kAddThreads - 1) / kAddThreads) * L.cols;
+  if (L.n == 0 || L.max_items == 0) return cudaSuccess;
   dim3 grid;
-  add_grid(it, L.n, num_sms, &grid);
-  const bool beta = L.beta != 0.0;
-  if (vec2) {
-    if (beta)
-      combine_kernel<ALG, 2, true><<<grid, kAddThreads, 0, stream>>>(L, cf);
-    else
-      combine_kernel<ALG, 2, false><<<grid, kAddThreads, 0, stream>>>(L, cf);
-  } else {
-    if (beta)
-      combine_kernel<ALG, 1, true><<<grid, kAddThreads, 0, stream>>>(L, cf);
-    else
-      combine_kernel<ALG, 1, false><<<grid, kAddThreads, 0, stream>>>(L, cf);
-  }
+  add_grid(L.max_items, L.n, num_sms, &grid);
+  if (vec2)
+    combine_kernel<ALG, 2><<<grid, kAddThreads, 0, stream>>>(L, cf);
+  else
+    combine_kernel<ALG, 1><<<grid, kAddThreads, 0, stream>>>(L, cf);
   return cudaGetLastError();
 }
 

@@ -335,9 +335,18 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
 template <class Cfg>
 cudaError_t gemm_launch_cfg(const GemmDesc* d_descs, int n, int64_t total_tiles, int num_sms, cudaStream_t stream) {
   if (total_tiles <= 0 || n <= 0) return cudaSuccess;
-  cudaError_t err = cudaFuncSetAttribute(grouped_dgemm_kernel<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)Cfg::SMEM_BYTES);
+  // the shared-memory opt-in is per device; set it once so launches can be
+  // captured into CUDA graphs without other API calls in between
+  static bool opted_in[64] = {};
+  int dev = 0;
+  cudaError_t err = cudaGetDevice(&dev);
   if (err != cudaSuccess) return err;
+  if (dev < 0 || dev >= 64 || !opted_in[dev]) {
+    err = cudaFuncSetAttribute(grouped_dgemm_kernel<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)Cfg::SMEM_BYTES);
+    if (err != cudaSuccess) return err;
+    if (dev >= 0 && dev < 64) opted_in[dev] = true;
+  }
   const int64_t slots = (int64_t)num_sms * Cfg::MINB;
   const int64_t grid = total_tiles < slots ? total_tiles : slots;
   grouped_dgemm_kernel<Cfg><<<(unsigned)grid, Cfg::THREADS, Cfg::SMEM_BYTES, stream>>>(d_descs, n, (int)total_tiles);

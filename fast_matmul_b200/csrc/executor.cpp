@@ -23,10 +23,10 @@ Profiler::~Profiler() {
   for (cudaEvent_t e : pool) cudaEventDestroy(e);
 }
 
-cudaError_t run_program(int alg, const Program& prog, const CoefSlots& cf, const void* h_desc_pinned, void* d_desc,
-                        int num_sms, cudaStream_t stream, int64_t* launches, Profiler* prof) {
+cudaError_t run_program(const Program& prog, const void* h_desc, void* d_desc, int num_sms, cudaStream_t stream,
+                        int64_t* launches, Profiler* prof) {
   if (!prog.desc.empty()) {
-    cudaError_t e = cudaMemcpyAsync(d_desc, h_desc_pinned, prog.desc.size(), cudaMemcpyHostToDevice, stream);
+    cudaError_t e = cudaMemcpyAsync(d_desc, h_desc, prog.desc.size(), cudaMemcpyHostToDevice, stream);
     if (e != cudaSuccess) return e;
   }
   const unsigned char* base = static_cast<const unsigned char*>(d_desc);
@@ -47,11 +47,8 @@ cudaError_t run_program(int alg, const Program& prog, const CoefSlots& cf, const
         L.t_desc = L.s_desc + op.n_s;
         L.n_s = op.n_s;
         L.n_t = op.n_t;
-        L.a_rows = op.a_rows;
-        L.a_cols = op.a_cols;
-        L.b_rows = op.b_rows;
-        L.b_cols = op.b_cols;
-        e = form_launch(alg, L, cf, op.vec2, num_sms, stream);
+        L.max_items = op.max_items;
+        e = form_launch(op.alg, L, prog.coefs[(size_t)op.cf], op.vec2, num_sms, stream);
         break;
       }
       case OpKind::kGemm:
@@ -62,10 +59,8 @@ cudaError_t run_program(int alg, const Program& prog, const CoefSlots& cf, const
         CombineLaunch L;
         L.desc = reinterpret_cast<const CombineDesc*>(base + op.desc_off);
         L.n = op.n;
-        L.rows = op.rows;
-        L.cols = op.cols;
-        L.beta = op.beta;
-        e = combine_launch(alg, L, cf, op.vec2, num_sms, stream);
+        L.max_items = op.max_items;
+        e = combine_launch(op.alg, L, prog.coefs[(size_t)op.cf], op.vec2, num_sms, stream);
         break;
       }
     }

@@ -12,10 +12,12 @@
 #include <new>
 #include <string>
 
+#include "api_internal.h"
 #include "fmm_internal.h"
 #include "plan.h"
 
-namespace {
+namespace fmm {
+namespace api {
 
 thread_local std::string g_last_error;
 
@@ -28,63 +30,16 @@ fmm_status cuda_fail(cudaError_t e, const char* where) {
   return fail(FMM_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
 }
 
-#define FMM_CUDA_TRY(expr, where)            \
-  do {                                       \
-    cudaError_t e__ = (expr);                \
-    if (e__ != cudaSuccess) {                \
-      return cuda_fail(e__, where);          \
-    }                                        \
-  } while (0)
+}  // namespace api
 
-// Restores the caller's current device on scope exit.
-class DeviceGuard {
- public:
-  explicit DeviceGuard(int dev) {
-    if (cudaGetDevice(&prev_) != cudaSuccess) prev_ = -1;
-    ok_ = cudaSetDevice(dev) == cudaSuccess;
-  }
-  ~DeviceGuard() {
-    if (prev_ >= 0) cudaSetDevice(prev_);
-  }
-  bool ok() const { return ok_; }
+void set_last_error(const std::string& msg) { api::g_last_error = msg; }
 
- private:
-  int prev_ = -1;
-  bool ok_ = false;
-};
-
-}  // namespace
-
-namespace fmm {
-void set_last_error(const std::string& msg) { g_last_error = msg; }
 }  // namespace fmm
 
-struct fmm_handle_s {
-  int device = 0;
-  int num_sms = 148;
-  cudaStream_t stream = nullptr;
-  size_t ws_limit = 0;
-  // device workspace pool (S/T/M temporaries), grown on demand
-  void* ws = nullptr;
-  size_t ws_cap = 0;
-  // launch descriptors: pinned host staging + device copy
-  void* h_desc = nullptr;
-  size_t h_desc_cap = 0;
-  void* d_desc = nullptr;
-  size_t d_desc_cap = 0;
-  cudaEvent_t desc_done = nullptr;  // staging buffer may be rewritten after this
-  bool desc_pending = false;
-  // device copies of host operands for fmm_fast_matmul_host
-  double* io = nullptr;
-  size_t io_cap = 0;
-  double* d_small = nullptr;  // two doubles for reductions
-  int64_t launches = 0;
-  fmm::Program prog;
-  bool profiling = false;
-  fmm::Profiler prof;
-};
+using namespace fmm::api;
 
-namespace {
+namespace fmm {
+namespace api {
 
 fmm_status ensure_device_buffer(fmm_handle h, void** buf, size_t* cap, size_t need, const char* what) {
   if (need <= *cap) return FMM_OK;
@@ -132,8 +87,8 @@ fmm_status stage_descriptors(fmm_handle h, const fmm::Program& prog) {
   return FMM_OK;
 }
 
-fmm_status run_staged(fmm_handle h, int alg, const fmm::Program& prog, const fmm::CoefSlots& cf) {
-  cudaError_t e = fmm::run_program(alg, prog, cf, h->h_desc, h->d_desc, h->num_sms, h->stream, &h->launches,
+fmm_status run_staged(fmm_handle h, const fmm::Program& prog) {
+  cudaError_t e = fmm::run_program(prog, h->h_desc, h->d_desc, h->num_sms, h->stream, &h->launches,
                                    h->profiling ? &h->prof : nullptr);
   if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
   if (!prog.desc.empty()) {
@@ -212,7 +167,8 @@ fmm_status choose_dfs_levels(fmm_handle h, int alg, int64_t m, int64_t k, int64_
   return FMM_OK;
 }
 
-}  // namespace
+}  // namespace api
+}  // namespace fmm
 
 extern "C" {
 
@@ -225,7 +181,7 @@ void fmm_options_init(fmm_options* opts) {
   opts->workspace_limit = 0;
 }
 
-const char* fmm_last_error(void) { return g_last_error.c_str(); }
+const char* fmm_last_error(void) { return fmm::api::g_last_error.c_str(); }
 
 fmm_status fmm_handle_create(fmm_handle* out, int device) {
   if (!out) return fail(FMM_ERR_INVALID_ARGUMENT, "null handle pointer");
@@ -369,9 +325,7 @@ fmm_status fmm_fast_matmul(fmm_handle h, int alg, const double* A, int64_t lda, 
     return fail(FMM_ERR_OUT_OF_MEMORY, std::string("planning failed: ") + ex.what());
   }
   if ((s = stage_descriptors(h, h->prog)) != FMM_OK) return s;
-  fmm::CoefSlots cf;
-  fmm_algorithms[alg].eval(x, cf.v);
-  return run_staged(h, alg, h->prog, cf);
+  return run_staged(h, h->prog);
 }
 
 fmm_status fmm_fast_matmul_host(fmm_handle h, int alg, const double* A, int64_t lda, const double* B, int64_t ldb,
@@ -432,8 +386,7 @@ fmm_status fmm_dgemm(fmm_handle h, const double* A, int64_t lda, const double* B
   DeviceGuard g(h->device);
   if (!g.ok()) return fail(FMM_ERR_CUDA, "cudaSetDevice failed");
   fmm::Program& prog = h->prog;
-  prog.ops.clear();
-  prog.desc.clear();
+  prog.clear();
   fmm::GemmDesc d{};
   d.A = A;
   d.B = B;
@@ -457,8 +410,7 @@ fmm_status fmm_dgemm(fmm_handle h, const double* A, int64_t lda, const double* B
   op.flops = 2.0 * (double)m * (double)n * (double)k;
   prog.ops.push_back(op);
   if ((s = stage_descriptors(h, prog)) != FMM_OK) return s;
-  fmm::CoefSlots cf{};
-  return run_staged(h, 0, prog, cf);
+  return run_staged(h, prog);
 }
 
 fmm_status fmm_dgemm_host(fmm_handle h, const double* A, int64_t lda, const double* B, int64_t ldb, double* C,

@@ -45,6 +45,7 @@ struct FormDesc {
   double* out;        // first materialised output block
   int64_t ld_out;
   int64_t out_stride; // distance between consecutive output blocks (doubles)
+  int64_t rows, cols; // dims of one block of this operand (= of one output)
 };
 
 // Combine: for each sub-problem, read its R product blocks once and write the
@@ -55,6 +56,8 @@ struct CombineDesc {
   int64_t m_stride;   // distance between consecutive product blocks (doubles)
   double* c;          // sub-problem's C operand
   int64_t ld_c;
+  int64_t rows, cols; // dims of one C block (= of one product block)
+  double beta;        // C blocks = sum (+ beta * C); 0 never reads C
 };
 
 struct CoefSlots {
@@ -65,16 +68,21 @@ struct FormLaunch {
   const FormDesc* s_desc;  // A side
   const FormDesc* t_desc;  // B side
   int n_s, n_t;            // number of sub-problems on each side
-  int64_t a_rows, a_cols;  // dims of one A block (output S has the same dims)
-  int64_t b_rows, b_cols;  // dims of one B block
+  int64_t max_items;       // largest per-problem work-item count (grid sizing)
 };
 
 struct CombineLaunch {
   const CombineDesc* desc;
   int n;
-  int64_t rows, cols;  // dims of one C block (= one product block)
-  double beta;
+  int64_t max_items;       // largest per-problem work-item count (grid sizing)
 };
+
+// Work items of one block of rows x cols for a kernel of 128-thread chunks
+// of `vec` rows.
+inline int64_t add_work_items(int64_t rows, int64_t cols, int vec) {
+  const int64_t rv = rows / vec;
+  return ((rv + 127) / 128) * cols;
+}
 
 cudaError_t form_launch(int alg, const FormLaunch& L, const CoefSlots& cf, bool vec2, int num_sms,
                         cudaStream_t stream);

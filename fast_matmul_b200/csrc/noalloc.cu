@@ -109,10 +109,8 @@ extern "C" fmm_status fmm_fast_matmul_noalloc(int alg, const double* A, int64_t 
     return fail(FMM_ERR_WORKSPACE_TOO_SMALL, "allocation-free call needs " + std::to_string(prog.desc.size()) +
                                                  " bytes of launch descriptors; the scratch reserves " +
                                                  std::to_string(kDescBytes));
-  fmm::CoefSlots cf;
-  t.eval(x, cf.v);
   // descriptors go from ordinary host memory into the front of the scratch
-  e = fmm::run_program(alg, prog, cf, prog.desc.data(), scratch, sms, static_cast<cudaStream_t>(stream), nullptr);
+  e = fmm::run_program(prog, prog.desc.data(), scratch, sms, static_cast<cudaStream_t>(stream), nullptr);
   if (e != cudaSuccess) return fail(FMM_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
   return FMM_OK;
 }

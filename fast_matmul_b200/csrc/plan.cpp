@@ -1,4 +1,4 @@
-// Recursion planner and program runner.
+// Recursion planner.
 //
 // The reference recursion (FastMatmulRecursive, algorithms/strassen.hpp:377-659)
 // visits sub-problems one at a time on the host.  Every sub-problem at one
@@ -18,12 +18,19 @@
 // the breadth-first levels scale with R^l.  Leading dimensions are padded to
 // even and blocks to 256-byte multiples so every workspace block allows
 // 16-byte vector access.
+//
+// A batch of independent products is planned breadth-first per item, with
+// the launches of all items merged: one formation launch per (algorithm,
+// level), one GEMM launch for every leaf of every item, then the
+// combinations and fringe products level by level upwards.
 
 #include "plan.h"
 
 #include <algorithm>
 #include <cstring>
+#include <map>
 #include <stdexcept>
+#include <utility>
 
 namespace fmm {
 
@@ -34,12 +41,11 @@ constexpr int64_t kAlignDoubles = 32;  // 256 bytes
 int64_t round_up(int64_t v, int64_t a) { return (v + a - 1) / a * a; }
 
 struct LevelLayout {
-  int64_t cm, ck, cn;         // child block dims (level l+1)
-  int64_t ldS, ldT, ldM;      // padded leading dimensions
+  int64_t cm, ck, cn;           // child block dims (level l+1)
+  int64_t ldS, ldT, ldM;        // padded leading dimensions
   int64_t sizeS, sizeT, sizeM;  // doubles per block
-  int64_t unit;               // sub-problems per unit at this level
+  int64_t unit;                 // sub-problems per unit at this level
   size_t off_S, off_T, off_M;   // byte offsets
-  size_t bytes;
 };
 
 int64_t unit_size(int l, int dfs_levels, int R) {
@@ -51,9 +57,9 @@ int64_t unit_size(int l, int dfs_levels, int R) {
 }
 
 std::vector<LevelLayout> layout(const fmm_alg_table& t, const std::vector<LevelDims>& dims, int steps,
-                                int dfs_levels, size_t* total) {
+                                int dfs_levels, size_t base, size_t* end) {
   std::vector<LevelLayout> lay(steps);
-  size_t off = 0;
+  size_t off = base;
   for (int l = 0; l < steps; ++l) {
     LevelLayout& L = lay[l];
     L.cm = dims[l + 1].m;
@@ -72,9 +78,8 @@ std::vector<LevelLayout> layout(const fmm_alg_table& t, const std::vector<LevelD
     off += (size_t)(L.unit * t.n_b_out * L.sizeT) * sizeof(double);
     L.off_M = off;
     off += (size_t)(L.unit * t.rank * L.sizeM) * sizeof(double);
-    L.bytes = off - L.off_S;
   }
-  *total = off;
+  *end = off;
   return lay;
 }
 
@@ -86,17 +91,227 @@ struct SubProblem {
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 
+template <class D>
+size_t append_desc(Program* prog, const std::vector<D>& v) {
+  std::vector<unsigned char>& b = prog->desc;
+  const size_t off = (size_t)round_up((int64_t)b.size(), 64);
+  b.resize(off + v.size() * sizeof(D));
+  std::memcpy(b.data() + off, v.data(), v.size() * sizeof(D));
+  return off;
+}
+
+// ---- per-level building blocks shared by the single and batched builders
+
+// Formation descriptors of one sub-problem (A side into sd, B side into td).
+void add_form_descs(const fmm_alg_table& t, const LevelLayout& L, const SubProblem& p, double* S, double* T,
+                    std::vector<FormDesc>* sd, std::vector<FormDesc>* td, bool* vec2, int64_t* max_items,
+                    double* bytes) {
+  if (t.n_a_out > 0 && L.cm > 0 && L.ck > 0) {
+    FormDesc d{p.A.ptr, p.A.ld, S, L.ldS, L.sizeS, L.cm, L.ck};
+    *vec2 = *vec2 && aligned16(d.in) && d.ld_in % 2 == 0 && L.cm % 2 == 0;
+    sd->push_back(d);
+    *max_items = std::max(*max_items, add_work_items(L.cm, L.ck, 1));
+    *bytes += 8.0 * (double)L.cm * L.ck * (t.m0 * t.k0 + t.n_a_out);
+  }
+  if (t.n_b_out > 0 && L.ck > 0 && L.cn > 0) {
+    FormDesc d{p.B.ptr, p.B.ld, T, L.ldT, L.sizeT, L.ck, L.cn};
+    *vec2 = *vec2 && aligned16(d.in) && d.ld_in % 2 == 0 && L.ck % 2 == 0;
+    td->push_back(d);
+    *max_items = std::max(*max_items, add_work_items(L.ck, L.cn, 1));
+    *bytes += 8.0 * (double)L.ck * L.cn * (t.k0 * t.n0 + t.n_b_out);
+  }
+}
+
+Operand block_of(const Operand& X, int64_t rows, int64_t cols, int nbc, int b) {
+  const int bi = b / nbc, bj = b % nbc;
+  return Operand{X.ptr + bi * rows + bj * cols * X.ld, X.ld};
+}
+
+// The R children of p (codegen/gen.py:574-657): operands are materialised
+// outputs or views; single coefficients fold into the multiplier.
+void add_children(const fmm_alg_table& t, const double* slots, const LevelLayout& L, const SubProblem& p, double* S,
+                  double* T, double* M, std::vector<SubProblem>* out) {
+  const int R = t.rank;
+  for (int r = 0; r < R; ++r) {
+    SubProblem c;
+    const short* as = t.a_src + 3 * r;
+    const short* bs = t.b_src + 3 * r;
+    c.mult = p.mult;
+    if (as[0] == 0)
+      c.A = block_of(p.A, L.cm, L.ck, t.k0, as[1]);
+    else
+      c.A = Operand{S + as[1] * L.sizeS, L.ldS};
+    if (as[2]) c.mult *= slots[as[2] - 1];
+    if (bs[0] == 0)
+      c.B = block_of(p.B, L.ck, L.cn, t.n0, bs[1]);
+    else
+      c.B = Operand{T + bs[1] * L.sizeT, L.ldT};
+    if (bs[2]) c.mult *= slots[bs[2] - 1];
+    c.C = Operand{M + r * L.sizeM, L.ldM};
+    c.beta = 0.0;
+    out->push_back(c);
+  }
+}
+
+// C blocks = sum of gamma * M (+ beta * C)  (strassen.hpp:646-649)
+void add_combine_desc(const fmm_alg_table& t, const LevelLayout& L, const SubProblem& p, double* M,
+                      std::vector<CombineDesc>* cd, bool* vec2, int64_t* max_items, double* bytes) {
+  if (L.cm <= 0 || L.cn <= 0) return;
+  CombineDesc d{M, L.ldM, L.sizeM, p.C.ptr, p.C.ld, L.cm, L.cn, p.beta};
+  *vec2 = *vec2 && L.cm % 2 == 0 && aligned16(d.c) && d.ld_c % 2 == 0;
+  cd->push_back(d);
+  *max_items = std::max(*max_items, add_work_items(L.cm, L.cn, 1));
+  *bytes += 8.0 * (double)L.cm * L.cn * (t.rank + t.m0 * t.n0 * (p.beta != 0.0 ? 2 : 1));
+}
+
+// Dynamic peeling of the fringes of p (linalg/linalg.hpp:201-244).
+void add_peel_descs(const fmm_alg_table& t, const LevelDims& D, const SubProblem& p, std::vector<GemmDesc>* g) {
+  const int64_t xr = D.m - (D.m / t.m0) * t.m0;
+  const int64_t xk = D.k - (D.k / t.k0) * t.k0;
+  const int64_t xc = D.n - (D.n / t.n0) * t.n0;
+  if (xk > 0) {  // C(core, core) += A(core, kx) * B(kx, core)
+    const int64_t rd = D.m - xr, cdim = D.n - xc, inner = D.k - xk;
+    GemmDesc d{};
+    d.A = p.A.ptr + inner * p.A.ld;
+    d.lda = p.A.ld;
+    d.B = p.B.ptr + inner;
+    d.ldb = p.B.ld;
+    d.C = p.C.ptr;
+    d.ldc = p.C.ld;
+    d.m = (int)rd;
+    d.n = (int)cdim;
+    d.k = (int)xk;
+    d.alpha = p.mult;
+    d.beta = 1.0;
+    g->push_back(d);
+  }
+  if (xc > 0) {  // C(:, nx) = A * B(:, nx) + beta * C(:, nx)
+    const int64_t s = D.n - xc;
+    GemmDesc d{};
+    d.A = p.A.ptr;
+    d.lda = p.A.ld;
+    d.B = p.B.ptr + s * p.B.ld;
+    d.ldb = p.B.ld;
+    d.C = p.C.ptr + s * p.C.ld;
+    d.ldc = p.C.ld;
+    d.m = (int)D.m;
+    d.n = (int)xc;
+    d.k = (int)D.k;
+    d.alpha = p.mult;
+    d.beta = p.beta;
+    g->push_back(d);
+  }
+  if (xr > 0) {  // C(mx, core) = A(mx, :) * B(:, core) + beta * C(mx, core)
+    const int64_t s = D.m - xr, nc = D.n - xc;
+    GemmDesc d{};
+    d.A = p.A.ptr + s;
+    d.lda = p.A.ld;
+    d.B = p.B.ptr;
+    d.ldb = p.B.ld;
+    d.C = p.C.ptr + s;
+    d.ldc = p.C.ld;
+    d.m = (int)xr;
+    d.n = (int)nc;
+    d.k = (int)D.k;
+    d.alpha = p.mult;
+    d.beta = p.beta;
+    g->push_back(d);
+  }
+}
+
+GemmDesc leaf_desc(const LevelDims& D, const SubProblem& p) {
+  GemmDesc d{};
+  d.A = p.A.ptr;
+  d.B = p.B.ptr;
+  d.C = p.C.ptr;
+  d.lda = p.A.ld;
+  d.ldb = p.B.ld;
+  d.ldc = p.C.ld;
+  d.m = (int)D.m;
+  d.n = (int)D.n;
+  d.k = (int)D.k;
+  d.alpha = p.mult;
+  d.beta = 0.0;  // the base case calls MatMul(A, B, C) with its default beta
+  return d;
+}
+
+// ---- op emission
+
+void emit_form(Program* prog, int alg, int cf, int level, const std::vector<FormDesc>& sd,
+               const std::vector<FormDesc>& td, bool vec2, int64_t max_items, double bytes) {
+  if (sd.empty() && td.empty()) return;
+  std::vector<FormDesc> all(sd);
+  all.insert(all.end(), td.begin(), td.end());
+  Op op;
+  op.kind = OpKind::kForm;
+  op.alg = alg;
+  op.cf = cf;
+  op.n = (int)all.size();
+  op.n_s = (int)sd.size();
+  op.n_t = (int)td.size();
+  op.max_items = vec2 ? (max_items + 1) / 2 : max_items;
+  op.vec2 = vec2;
+  op.level = level;
+  op.bytes = bytes;
+  op.desc_off = append_desc(prog, all);
+  prog->ops.push_back(op);
+}
+
+void emit_combine(Program* prog, int alg, int cf, int level, const std::vector<CombineDesc>& cd, bool vec2,
+                  int64_t max_items, double bytes) {
+  if (cd.empty()) return;
+  Op op;
+  op.kind = OpKind::kCombine;
+  op.alg = alg;
+  op.cf = cf;
+  op.n = (int)cd.size();
+  op.max_items = vec2 ? (max_items + 1) / 2 : max_items;
+  op.vec2 = vec2;
+  op.level = level;
+  op.bytes = bytes;
+  op.desc_off = append_desc(prog, cd);
+  prog->ops.push_back(op);
+}
+
+void emit_gemm(Program* prog, int level, std::vector<GemmDesc>& g, bool leaves) {
+  if (g.empty()) return;
+  const int64_t tiles = gemm_prepare(g.data(), (int)g.size());
+  double flops = 0.0;
+  for (const GemmDesc& d : g) flops += 2.0 * d.m * d.n * (double)d.k;
+  if (leaves) {
+    prog->leaf_flops += flops;
+    prog->leaf_count += (int64_t)g.size();
+  } else {
+    prog->peel_flops += flops;
+  }
+  if (tiles == 0) return;
+  Op op;
+  op.kind = OpKind::kGemm;
+  op.n = (int)g.size();
+  op.total_tiles = tiles;
+  op.level = level;
+  op.peel = !leaves;
+  op.flops = flops;
+  op.desc_off = append_desc(prog, g);
+  prog->ops.push_back(op);
+}
+
+// ---- single call, any schedule
+
 class Builder {
  public:
   Builder(int alg, int steps, int dfs_levels, const std::vector<LevelDims>& dims, const std::vector<LevelLayout>& lay,
           const double* slots, char* ws, Program* prog)
-      : t_(fmm_algorithms[alg]), steps_(steps), d_(dfs_levels), dims_(dims), lay_(lay), slots_(slots), ws_(ws),
-        prog_(prog) {}
+      : alg_(alg), t_(fmm_algorithms[alg]), steps_(steps), d_(dfs_levels), dims_(dims), lay_(lay), slots_(slots),
+        ws_(ws), prog_(prog) {}
 
   void level(int l, const std::vector<SubProblem>& F) {
     if (F.empty()) return;
     if (l == steps_) {
-      emit_leaves(l, F);
+      std::vector<GemmDesc> g;
+      g.reserve(F.size());
+      for (const SubProblem& p : F) g.push_back(leaf_desc(dims_[l], p));
+      emit_gemm(prog_, l, g, true);
       return;
     }
     if (l < d_) {
@@ -107,223 +322,42 @@ class Builder {
   }
 
  private:
-  template <class D>
-  size_t append(const std::vector<D>& v) {
-    std::vector<unsigned char>& b = prog_->desc;
-    size_t off = round_up((int64_t)b.size(), 64);
-    b.resize(off + v.size() * sizeof(D));
-    std::memcpy(b.data() + off, v.data(), v.size() * sizeof(D));
-    return off;
-  }
-
-  void emit_gemm(int l, std::vector<GemmDesc>& g, bool leaves) {
-    // (tile counts and copy widths are filled in by gemm_prepare)
-    if (g.empty()) return;
-    const int64_t tiles = gemm_prepare(g.data(), (int)g.size());
-    double flops = 0.0;
-    for (const GemmDesc& d : g) flops += 2.0 * d.m * d.n * (double)d.k;
-    if (leaves) {
-      prog_->leaf_flops += flops;
-      prog_->leaf_count += (int64_t)g.size();
-    } else {
-      prog_->peel_flops += flops;
-    }
-    if (tiles == 0) return;
-    Op op;
-    op.kind = OpKind::kGemm;
-    op.n = (int)g.size();
-    op.total_tiles = tiles;
-    op.level = l;
-    op.peel = !leaves;
-    op.flops = flops;
-    op.desc_off = append(g);
-    prog_->ops.push_back(op);
-  }
-
-  void emit_leaves(int l, const std::vector<SubProblem>& F) {
-    const LevelDims& D = dims_[l];
-    std::vector<GemmDesc> g;
-    g.reserve(F.size());
-    for (const SubProblem& p : F) {
-      GemmDesc d{};
-      d.A = p.A.ptr;
-      d.B = p.B.ptr;
-      d.C = p.C.ptr;
-      d.lda = p.A.ld;
-      d.ldb = p.B.ld;
-      d.ldc = p.C.ld;
-      d.m = (int)D.m;
-      d.n = (int)D.n;
-      d.k = (int)D.k;
-      d.alpha = p.mult;
-      d.beta = 0.0;  // the base case calls MatMul(A, B, C) with its default beta
-      g.push_back(d);
-    }
-    emit_gemm(l, g, true);
-  }
-
-  Operand block(const Operand& X, int64_t rows, int64_t cols, int nbc, int b) const {
-    const int bi = b / nbc, bj = b % nbc;
-    return Operand{X.ptr + bi * rows + bj * cols * X.ld, X.ld};
-  }
-
   void unit(int l, const SubProblem* F, int64_t nf) {
     const LevelLayout& L = lay_[l];
     const int R = t_.rank;
     double* S = reinterpret_cast<double*>(ws_ + L.off_S);
     double* T = reinterpret_cast<double*>(ws_ + L.off_T);
     double* M = reinterpret_cast<double*>(ws_ + L.off_M);
-
-    // 1. form the materialised S and T operands of every product
-    const bool s_work = t_.n_a_out > 0 && L.cm > 0 && L.ck > 0;
-    const bool t_work = t_.n_b_out > 0 && L.ck > 0 && L.cn > 0;
-    if (s_work || t_work) {
-      std::vector<FormDesc> fd;
+    {
+      std::vector<FormDesc> sd, td;
       bool vec2 = true;
-      if (s_work) {
-        for (int64_t q = 0; q < nf; ++q) {
-          FormDesc d{F[q].A.ptr, F[q].A.ld, S + q * t_.n_a_out * L.sizeS, L.ldS, L.sizeS};
-          vec2 = vec2 && aligned16(d.in) && d.ld_in % 2 == 0 && L.cm % 2 == 0;
-          fd.push_back(d);
-        }
-      }
-      if (t_work) {
-        for (int64_t q = 0; q < nf; ++q) {
-          FormDesc d{F[q].B.ptr, F[q].B.ld, T + q * t_.n_b_out * L.sizeT, L.ldT, L.sizeT};
-          vec2 = vec2 && aligned16(d.in) && d.ld_in % 2 == 0 && L.ck % 2 == 0;
-          fd.push_back(d);
-        }
-      }
-      Op op;
-      op.kind = OpKind::kForm;
-      op.n = (int)fd.size();
-      op.n_s = s_work ? (int)nf : 0;
-      op.n_t = t_work ? (int)nf : 0;
-      op.a_rows = L.cm;
-      op.a_cols = L.ck;
-      op.b_rows = L.ck;
-      op.b_cols = L.cn;
-      op.vec2 = vec2;
-      op.level = l;
-      op.bytes = 8.0 * nf *
-                 ((s_work ? (double)L.cm * L.ck * (t_.m0 * t_.k0 + t_.n_a_out) : 0.0) +
-                  (t_work ? (double)L.ck * L.cn * (t_.k0 * t_.n0 + t_.n_b_out) : 0.0));
-      op.desc_off = append(fd);
-      prog_->ops.push_back(op);
+      int64_t items = 0;
+      double bytes = 0.0;
+      for (int64_t q = 0; q < nf; ++q)
+        add_form_descs(t_, L, F[q], S + q * t_.n_a_out * L.sizeS, T + q * t_.n_b_out * L.sizeT, &sd, &td, &vec2,
+                       &items, &bytes);
+      emit_form(prog_, alg_, 0, l, sd, td, vec2, items, bytes);
     }
-
-    // 2. the children (codegen/gen.py:574-657): operands are materialised
-    //    outputs or views; single coefficients fold into the multiplier
-    std::vector<SubProblem> ch((size_t)(nf * R));
-    for (int64_t q = 0; q < nf; ++q) {
-      const SubProblem& p = F[q];
-      for (int r = 0; r < R; ++r) {
-        SubProblem& c = ch[(size_t)(q * R + r)];
-        const short* as = t_.a_src + 3 * r;
-        const short* bs = t_.b_src + 3 * r;
-        c.mult = p.mult;
-        if (as[0] == 0) {
-          c.A = block(p.A, L.cm, L.ck, t_.k0, as[1]);
-        } else {
-          c.A = Operand{S + (q * t_.n_a_out + as[1]) * L.sizeS, L.ldS};
-        }
-        if (as[2]) c.mult *= slots_[as[2] - 1];
-        if (bs[0] == 0) {
-          c.B = block(p.B, L.ck, L.cn, t_.n0, bs[1]);
-        } else {
-          c.B = Operand{T + (q * t_.n_b_out + bs[1]) * L.sizeT, L.ldT};
-        }
-        if (bs[2]) c.mult *= slots_[bs[2] - 1];
-        c.C = Operand{M + (q * R + r) * L.sizeM, L.ldM};
-        c.beta = 0.0;
-      }
-    }
+    std::vector<SubProblem> ch;
+    ch.reserve((size_t)(nf * R));
+    for (int64_t q = 0; q < nf; ++q)
+      add_children(t_, slots_, L, F[q], S + q * t_.n_a_out * L.sizeS, T + q * t_.n_b_out * L.sizeT,
+                   M + q * R * L.sizeM, &ch);
     level(l + 1, ch);
-
-    // 3. C blocks = sum of gamma * M (+ beta * C)  (strassen.hpp:646-649)
-    if (L.cm > 0 && L.cn > 0) {
+    {
       std::vector<CombineDesc> cd;
-      bool vec2 = (L.cm % 2 == 0);
-      for (int64_t q = 0; q < nf; ++q) {
-        CombineDesc d{M + q * R * L.sizeM, L.ldM, L.sizeM, F[q].C.ptr, F[q].C.ld};
-        vec2 = vec2 && aligned16(d.c) && d.ld_c % 2 == 0;
-        cd.push_back(d);
-      }
-      Op op;
-      op.kind = OpKind::kCombine;
-      op.n = (int)cd.size();
-      op.rows = L.cm;
-      op.cols = L.cn;
-      op.beta = F[0].beta;
-      op.vec2 = vec2;
-      op.level = l;
-      op.bytes = 8.0 * nf * (double)L.cm * L.cn * (R + t_.m0 * t_.n0 * (F[0].beta != 0.0 ? 2 : 1));
-      op.desc_off = append(cd);
-      prog_->ops.push_back(op);
+      bool vec2 = true;
+      int64_t items = 0;
+      double bytes = 0.0;
+      for (int64_t q = 0; q < nf; ++q) add_combine_desc(t_, L, F[q], M + q * R * L.sizeM, &cd, &vec2, &items, &bytes);
+      emit_combine(prog_, alg_, 0, l, cd, vec2, items, bytes);
     }
-
-    // 4. dynamic peeling of the fringes (linalg/linalg.hpp:201-244)
-    const LevelDims& D = dims_[l];
-    const int64_t xr = D.m - (D.m / t_.m0) * t_.m0;
-    const int64_t xk = D.k - (D.k / t_.k0) * t_.k0;
-    const int64_t xc = D.n - (D.n / t_.n0) * t_.n0;
-    if (xr || xk || xc) {
-      std::vector<GemmDesc> g;
-      for (int64_t q = 0; q < nf; ++q) {
-        const SubProblem& p = F[q];
-        if (xk > 0) {  // C(core, core) += A(core, kx) * B(kx, core)
-          const int64_t rd = D.m - xr, cdim = D.n - xc, inner = D.k - xk;
-          GemmDesc d{};
-          d.A = p.A.ptr + inner * p.A.ld;
-          d.lda = p.A.ld;
-          d.B = p.B.ptr + inner;
-          d.ldb = p.B.ld;
-          d.C = p.C.ptr;
-          d.ldc = p.C.ld;
-          d.m = (int)rd;
-          d.n = (int)cdim;
-          d.k = (int)xk;
-          d.alpha = p.mult;
-          d.beta = 1.0;
-          g.push_back(d);
-        }
-        if (xc > 0) {  // C(:, nx) = A * B(:, nx) + beta * C(:, nx)
-          const int64_t s = D.n - xc;
-          GemmDesc d{};
-          d.A = p.A.ptr;
-          d.lda = p.A.ld;
-          d.B = p.B.ptr + s * p.B.ld;
-          d.ldb = p.B.ld;
-          d.C = p.C.ptr + s * p.C.ld;
-          d.ldc = p.C.ld;
-          d.m = (int)D.m;
-          d.n = (int)xc;
-          d.k = (int)D.k;
-          d.alpha = p.mult;
-          d.beta = p.beta;
-          g.push_back(d);
-        }
-        if (xr > 0) {  // C(mx, core) = A(mx, :) * B(:, core) + beta * C(mx, core)
-          const int64_t s = D.m - xr, nc = D.n - xc;
-          GemmDesc d{};
-          d.A = p.A.ptr + s;
-          d.lda = p.A.ld;
-          d.B = p.B.ptr;
-          d.ldb = p.B.ld;
-          d.C = p.C.ptr + s;
-          d.ldc = p.C.ld;
-          d.m = (int)xr;
-          d.n = (int)nc;
-          d.k = (int)D.k;
-          d.alpha = p.mult;
-          d.beta = p.beta;
-          g.push_back(d);
-        }
-      }
-      emit_gemm(l, g, false);
-    }
+    std::vector<GemmDesc> g;
+    for (int64_t q = 0; q < nf; ++q) add_peel_descs(t_, dims_[l], F[q], &g);
+    emit_gemm(prog_, l, g, false);
   }
 
+  int alg_;
   const fmm_alg_table& t_;
   int steps_;
   int d_;
@@ -334,7 +368,32 @@ class Builder {
   Program* prog_;
 };
 
+struct ItemState {
+  std::vector<LevelDims> dims;
+  std::vector<LevelLayout> lay;
+  std::vector<std::vector<SubProblem>> frontier;  // sub-problems per level
+  int cf = 0;
+};
+
 }  // namespace
+
+void Program::clear() {
+  ops.clear();
+  desc.clear();
+  coefs.clear();
+  workspace_bytes = 0;
+  dfs_levels = 0;
+  leaf_flops = 0.0;
+  peel_flops = 0.0;
+  leaf_count = 0;
+}
+
+std::vector<LevelDims> level_dims(const fmm_alg_table& t, int64_t m, int64_t k, int64_t n, int steps) {
+  std::vector<LevelDims> d((size_t)steps + 1);
+  d[0] = LevelDims{m, k, n};
+  for (int l = 1; l <= steps; ++l) d[l] = LevelDims{d[l - 1].m / t.m0, d[l - 1].k / t.k0, d[l - 1].n / t.n0};
+  return d;
+}
 
 int64_t gemm_prepare(GemmDesc* descs, int n, int tile_n, int tile_m) {
   int64_t total = 0;
@@ -353,16 +412,9 @@ int64_t gemm_prepare(GemmDesc* descs, int n, int tile_n, int tile_m) {
   return total;
 }
 
-std::vector<LevelDims> level_dims(const fmm_alg_table& t, int64_t m, int64_t k, int64_t n, int steps) {
-  std::vector<LevelDims> d((size_t)steps + 1);
-  d[0] = LevelDims{m, k, n};
-  for (int l = 1; l <= steps; ++l) d[l] = LevelDims{d[l - 1].m / t.m0, d[l - 1].k / t.k0, d[l - 1].n / t.n0};
-  return d;
-}
-
 size_t workspace_bytes(const fmm_alg_table& t, int64_t m, int64_t k, int64_t n, int steps, int dfs_levels) {
   size_t total = 0;
-  layout(t, level_dims(t, m, k, n, steps), steps, dfs_levels, &total);
+  layout(t, level_dims(t, m, k, n, steps), steps, dfs_levels, 0, &total);
   return total;
 }
 
@@ -371,21 +423,143 @@ void build_program(int alg, int64_t m, int64_t k, int64_t n, int steps, double x
   const fmm_alg_table& t = fmm_algorithms[alg];
   const std::vector<LevelDims> dims = level_dims(t, m, k, n, steps);
   size_t total = 0;
-  const std::vector<LevelLayout> lay = layout(t, dims, steps, dfs_levels, &total);
-  double slots[FMM_MAX_SLOTS > 0 ? FMM_MAX_SLOTS : 1];
-  t.eval(x, slots);
-  out->ops.clear();
-  out->desc.clear();
+  const std::vector<LevelLayout> lay = layout(t, dims, steps, dfs_levels, 0, &total);
+  out->clear();
+  CoefSlots cf{};
+  t.eval(x, cf.v);
+  out->coefs.push_back(cf);
   out->workspace_bytes = total;
   out->dfs_levels = dfs_levels;
-  out->leaf_flops = 0.0;
-  out->peel_flops = 0.0;
-  out->leaf_count = 0;
   // FastMatmul (strassen.hpp:661-722): A's multiplier is alpha; the first
   // recursion folds it into C's (C.mult = 1 * alpha * 1).
   SubProblem root{A, B, C, 1.0 * alpha * 1.0, beta};
-  Builder b(alg, steps, dfs_levels, dims, lay, slots, static_cast<char*>(ws), out);
+  Builder b(alg, steps, dfs_levels, dims, lay, out->coefs[0].v, static_cast<char*>(ws), out);
   b.level(0, std::vector<SubProblem>{root});
+}
+
+size_t batch_workspace_bytes(const BatchItem* items, int count) {
+  size_t off = 0;
+  for (int i = 0; i < count; ++i) {
+    if (items[i].classical) continue;
+    const fmm_alg_table& t = fmm_algorithms[items[i].alg];
+    size_t end = 0;
+    layout(t, level_dims(t, items[i].m, items[i].k, items[i].n, items[i].steps), items[i].steps, 0, off, &end);
+    off = (size_t)round_up((int64_t)end, 256);
+  }
+  return off;
+}
+
+void build_batch_program(const BatchItem* items, int count, void* ws, Program* out) {
+  out->clear();
+  out->dfs_levels = 0;
+  char* base = static_cast<char*>(ws);
+  std::vector<ItemState> st((size_t)count);
+  std::map<std::pair<int, double>, int> coef_index;  // (alg, x) -> coefficient set
+  int max_steps = 0;
+  size_t off = 0;
+  for (int i = 0; i < count; ++i) {
+    const BatchItem& it = items[i];
+    const fmm_alg_table& t = fmm_algorithms[it.classical ? 0 : it.alg];
+    ItemState& s = st[(size_t)i];
+    const int isteps = it.classical ? 0 : it.steps;
+    s.dims = level_dims(t, it.m, it.k, it.n, isteps);
+    size_t end = 0;
+    s.lay = layout(t, s.dims, isteps, 0, off, &end);
+    off = (size_t)round_up((int64_t)end, 256);
+    const std::pair<int, double> key(it.alg, it.x);
+    auto found = coef_index.find(key);
+    if (found == coef_index.end()) {
+      CoefSlots cf{};
+      t.eval(it.x, cf.v);
+      out->coefs.push_back(cf);
+      found = coef_index.emplace(key, (int)out->coefs.size() - 1).first;
+    }
+    s.cf = found->second;
+    s.frontier.resize((size_t)isteps + 1);
+    s.frontier[0].push_back(SubProblem{it.A, it.B, it.C, 1.0 * it.alpha * 1.0, it.beta});
+    for (int l = 0; l < isteps; ++l) {
+      const LevelLayout& L = s.lay[(size_t)l];
+      double* S = reinterpret_cast<double*>(base + L.off_S);
+      double* T = reinterpret_cast<double*>(base + L.off_T);
+      double* M = reinterpret_cast<double*>(base + L.off_M);
+      const std::vector<SubProblem>& F = s.frontier[(size_t)l];
+      for (size_t q = 0; q < F.size(); ++q)
+        add_children(t, out->coefs[(size_t)s.cf].v, L, F[q], S + q * t.n_a_out * L.sizeS,
+                     T + q * t.n_b_out * L.sizeT, M + q * t.rank * L.sizeM, &s.frontier[(size_t)l + 1]);
+    }
+    max_steps = std::max(max_steps, isteps);
+  }
+  out->workspace_bytes = off;
+  auto steps_of = [&](int i) { return items[i].classical ? 0 : items[i].steps; };
+
+  // formations, top-down: one launch per (algorithm, coefficient set, level)
+  for (int l = 0; l < max_steps; ++l) {
+    std::map<std::pair<int, int>, std::vector<int>> groups;
+    for (int i = 0; i < count; ++i)
+      if (steps_of(i) > l) groups[{items[i].alg, st[(size_t)i].cf}].push_back(i);
+    for (const auto& g : groups) {
+      const fmm_alg_table& t = fmm_algorithms[g.first.first];
+      std::vector<FormDesc> sd, td;
+      bool vec2 = true;
+      int64_t mx = 0;
+      double bytes = 0.0;
+      for (int i : g.second) {
+        const ItemState& s = st[(size_t)i];
+        const LevelLayout& L = s.lay[(size_t)l];
+        double* S = reinterpret_cast<double*>(base + L.off_S);
+        double* T = reinterpret_cast<double*>(base + L.off_T);
+        const std::vector<SubProblem>& F = s.frontier[(size_t)l];
+        for (size_t q = 0; q < F.size(); ++q)
+          add_form_descs(t, L, F[q], S + q * t.n_a_out * L.sizeS, T + q * t.n_b_out * L.sizeT, &sd, &td, &vec2,
+                         &mx, &bytes);
+      }
+      emit_form(out, g.first.first, g.first.second, l, sd, td, vec2, mx, bytes);
+    }
+  }
+  // every leaf of every item: one grouped GEMM
+  {
+    std::vector<GemmDesc> g;
+    for (int i = 0; i < count; ++i) {
+      const ItemState& s = st[(size_t)i];
+      const size_t steps = (size_t)steps_of(i);
+      for (const SubProblem& p : s.frontier[steps]) {
+        GemmDesc d = leaf_desc(s.dims[steps], p);
+        if (items[i].classical) d.beta = items[i].beta;
+        g.push_back(d);
+      }
+    }
+    emit_gemm(out, max_steps, g, true);
+  }
+  // combinations and fringes, bottom-up
+  for (int l = max_steps - 1; l >= 0; --l) {
+    std::map<std::pair<int, int>, std::vector<int>> groups;
+    for (int i = 0; i < count; ++i)
+      if (steps_of(i) > l) groups[{items[i].alg, st[(size_t)i].cf}].push_back(i);
+    for (const auto& g : groups) {
+      const fmm_alg_table& t = fmm_algorithms[g.first.first];
+      std::vector<CombineDesc> cd;
+      bool vec2 = true;
+      int64_t mx = 0;
+      double bytes = 0.0;
+      for (int i : g.second) {
+        const ItemState& s = st[(size_t)i];
+        const LevelLayout& L = s.lay[(size_t)l];
+        double* M = reinterpret_cast<double*>(base + L.off_M);
+        const std::vector<SubProblem>& F = s.frontier[(size_t)l];
+        for (size_t q = 0; q < F.size(); ++q)
+          add_combine_desc(t, L, F[q], M + q * t.rank * L.sizeM, &cd, &vec2, &mx, &bytes);
+      }
+      emit_combine(out, g.first.first, g.first.second, l, cd, vec2, mx, bytes);
+    }
+    std::vector<GemmDesc> peel;
+    for (int i = 0; i < count; ++i) {
+      if (steps_of(i) <= l) continue;
+      const fmm_alg_table& t = fmm_algorithms[items[i].alg];
+      const ItemState& s = st[(size_t)i];
+      for (const SubProblem& p : s.frontier[(size_t)l]) add_peel_descs(t, s.dims[(size_t)l], p, &peel);
+    }
+    emit_gemm(out, l, peel, false);
+  }
 }
 
 }  // namespace fmm

@@ -1,6 +1,6 @@
-// Recursion planner: turns one FastMatmul call into a list of grouped
-// launches (operand formation, leaf products, combination, peeling) over a
-// device workspace laid out level by level.
+// Recursion planner: turns one FastMatmul call (or a batch of independent
+// calls) into a list of grouped launches (operand formation, leaf products,
+// combination, peeling) over a device workspace laid out level by level.
 #pragma once
 
 #include <cstddef>
@@ -20,16 +20,13 @@ enum class OpKind { kForm, kGemm, kCombine };
 
 struct Op {
   OpKind kind;
+  int alg = 0;          // form / combine: algorithm of the kernel
+  int cf = 0;           // form / combine: index into Program::coefs
   size_t desc_off = 0;  // byte offset of this launch's descriptors in Program::desc
   int n = 0;            // descriptors
-  // form
-  int n_s = 0, n_t = 0;
-  int64_t a_rows = 0, a_cols = 0, b_rows = 0, b_cols = 0;
-  // combine
-  int64_t rows = 0, cols = 0;
-  double beta = 0.0;
-  // gemm
-  int64_t total_tiles = 0;
+  int n_s = 0, n_t = 0; // form: sub-problems on the A and B side
+  int64_t max_items = 0;     // form / combine: largest per-problem work-item count
+  int64_t total_tiles = 0;   // gemm
   bool vec2 = false;
   bool peel = false;     // gemm: dynamic-peeling fringe products
   int level = 0;         // recursion level the launch belongs to (steps = leaves)
@@ -56,11 +53,13 @@ struct Profiler {
 struct Program {
   std::vector<Op> ops;
   std::vector<unsigned char> desc;
+  std::vector<CoefSlots> coefs;
   size_t workspace_bytes = 0;
   int dfs_levels = 0;
   double leaf_flops = 0.0;  // 2 * m * n * k summed over leaf products
   double peel_flops = 0.0;
   int64_t leaf_count = 0;
+  void clear();
 };
 
 struct LevelDims {
@@ -74,15 +73,36 @@ std::vector<LevelDims> level_dims(const fmm_alg_table& t, int64_t m, int64_t k, 
 // Workspace bytes for `dfs_levels` depth-first levels (0 = all breadth-first).
 size_t workspace_bytes(const fmm_alg_table& t, int64_t m, int64_t k, int64_t n, int steps, int dfs_levels);
 
-// Builds the launch program.  ws must hold workspace_bytes(...) bytes.
+// Builds the launch program of one call.  ws must hold workspace_bytes(...) bytes.
 void build_program(int alg, int64_t m, int64_t k, int64_t n, int steps, double x, double alpha, double beta,
                    int dfs_levels, Operand A, Operand B, Operand C, void* ws, Program* out);
 
+// One independent product of a batch.  A classical item is one GEMM
+// C = alpha * A * B + beta * C (beta honoured; alg and steps unused); the
+// others follow FastMatmul exactly (num_steps == 0 ignores beta).
+struct BatchItem {
+  int alg;
+  int steps;
+  int64_t m, k, n;
+  Operand A, B, C;
+  double x, alpha, beta;
+  bool classical;
+};
+
+// Workspace of a batch (every item planned breadth-first, regions back to back).
+size_t batch_workspace_bytes(const BatchItem* items, int count);
+
+// Builds one program for the whole batch: operand formations level by level
+// (one launch per algorithm and level over all items), ONE grouped GEMM over
+// every item's leaf products, then combinations and fringe products level by
+// level upwards.
+void build_batch_program(const BatchItem* items, int count, void* ws, Program* out);
+
 // Runs a built program: one host-to-device copy of all descriptors to
 // d_desc (which must hold prog.desc.size() bytes), then the launches in order.
-// Returns the number of kernels launched through *launches.
+// Adds the number of kernels launched to *launches (may be null).
 // When prof is non-null every launch is bracketed by CUDA events.
-cudaError_t run_program(int alg, const Program& prog, const CoefSlots& cf, const void* h_desc_pinned, void* d_desc,
-                        int num_sms, cudaStream_t stream, int64_t* launches, Profiler* prof = nullptr);
+cudaError_t run_program(const Program& prog, const void* h_desc, void* d_desc, int num_sms, cudaStream_t stream,
+                        int64_t* launches, Profiler* prof = nullptr);
 
 }  // namespace fmm

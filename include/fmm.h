@@ -167,6 +167,71 @@ fmm_status fmm_profile_enable(fmm_handle h, int enable);
 fmm_status fmm_profile_reset(fmm_handle h);
 fmm_status fmm_profile_read(fmm_handle h, fmm_profile* out);
 
+/* ---- Batches, autotuning and CUDA-graph plans.  No counterpart in the
+ * reference, which multiplies one pair per call and fixes the algorithm and
+ * depth at compile time. */
+
+/* Algorithm value of a batch item: -1 lets the autotuner choose the
+ * algorithm and depth; FMM_ALG_CLASSICAL is one GEMM
+ * C = alpha * A * B + beta * C (beta honoured). */
+#define FMM_ALG_AUTO (-1)
+#define FMM_ALG_CLASSICAL (-2)
+
+typedef struct fmm_batch_item {
+  int alg;        /* algorithm index, FMM_ALG_AUTO or FMM_ALG_CLASSICAL */
+  int num_steps;  /* recursive levels (ignored for FMM_ALG_AUTO / FMM_ALG_CLASSICAL) */
+  const double* A;
+  int64_t lda;
+  const double* B;
+  int64_t ldb;
+  double* C;
+  int64_t ldc;
+  int64_t m, k, n;
+  double x, alpha, beta; /* as in fmm_fast_matmul */
+} fmm_batch_item;
+
+/* Independent products in one program: the operand formations of all items
+ * level by level (one launch per algorithm and level), the leaf products of
+ * ALL items in one persistent grouped GEMM launch, then the combinations and
+ * fringe products.  Each item's result equals the one fmm_fast_matmul gives
+ * for it alone (bit for bit).  Items whose combined workspace exceeds the
+ * handle's limit are run in several such programs.  Device pointers; queued
+ * on the handle's stream. */
+fmm_status fmm_fast_matmul_batched(fmm_handle h, const fmm_batch_item* items, int count);
+
+/* The (algorithm, num_steps) the handle uses for FMM_ALG_AUTO items of this
+ * shape: the autotuned choice of the shape's bucket (ceil(log2) of m, k and
+ * n) if fmm_autotune measured it, otherwise a size rule (classical below
+ * 4000; Strassen with 2 steps from 4000; fast424_26_206 with 2 steps from
+ * 12000 in every dimension).  *alg is FMM_ALG_CLASSICAL for a plain GEMM. */
+fmm_status fmm_autotune_choice(fmm_handle h, int64_t m, int64_t k, int64_t n, int* alg, int* num_steps);
+
+/* Times, for one representative shape per bucket of `shapes` (count x 3:
+ * m, k, n), the classical GEMM and every candidate algorithm with 1 ..
+ * max_steps levels (leaf blocks of at least 64), and records the fastest per
+ * bucket in the handle.  candidates may be NULL (Strassen, fast424_26_206,
+ * fast333_23_125, smirnov333_23_128).  Allocates scratch matrices. */
+fmm_status fmm_autotune(fmm_handle h, const int64_t* shapes, int count, const int* candidates, int n_candidates,
+                        int max_steps);
+
+/* The tuning table as text lines "mb kb nb alg steps" (buckets are
+ * ceil(log2(dim))), and loading it back. */
+fmm_status fmm_autotune_export(fmm_handle h, char* buf, size_t cap, size_t* len);
+fmm_status fmm_autotune_import(fmm_handle h, const char* text);
+
+/* A product or a batch planned once and captured as a CUDA graph; executing
+ * replays the graph on the handle's stream (same pointers, current data).
+ * The plan owns its workspace and descriptors. */
+typedef struct fmm_plan_s* fmm_plan;
+fmm_status fmm_plan_create(fmm_handle h, int alg, const double* A, int64_t lda, const double* B, int64_t ldb,
+                           double* C, int64_t ldc, int64_t m, int64_t k, int64_t n, int num_steps, double x,
+                           double alpha, double beta, const fmm_options* opts, fmm_plan* out);
+fmm_status fmm_plan_create_batched(fmm_handle h, const fmm_batch_item* items, int count, fmm_plan* out);
+fmm_status fmm_plan_execute(fmm_plan p);
+fmm_status fmm_plan_destroy(fmm_plan p);
+/* Kernels one execution launches. */
+int64_t fmm_plan_kernel_count(fmm_plan p);
+
 /* Allocation-free FastMatmul.  No counterpart in the reference.
  *
  * For callers that may not allocate device memory at all: code whose device

@@ -55,6 +55,10 @@ def emulator():
     L.emu_fast_matmul.restype = I
     L.emu_workspace_bytes.argtypes = [I, i64, i64, i64, I, I]
     L.emu_workspace_bytes.restype = ctypes.c_size_t
+    IP = ctypes.POINTER(ctypes.c_int)
+    LP = ctypes.POINTER(i64)
+    L.emu_fast_matmul_batch.argtypes = [I, IP, IP, LP, P, LP, P, LP, P, LP, D, D, D, LP]
+    L.emu_fast_matmul_batch.restype = I
     return L
 
 

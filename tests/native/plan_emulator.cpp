@@ -16,6 +16,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <limits>
+#include <string>
 #include <vector>
 
 #include "plan.h"
@@ -23,6 +24,7 @@
 namespace fmm {
 // The device launchers are not used by the interpreter.
 cudaError_t gemm_launch(const GemmDesc*, int, int64_t, int, cudaStream_t) { return cudaErrorNotSupported; }
+void set_last_error(const std::string&) {}
 cudaError_t form_launch(int, const FormLaunch&, const CoefSlots&, bool, int, cudaStream_t) {
   return cudaErrorNotSupported;
 }
@@ -56,8 +58,8 @@ void run_form(const fmm::Op& op, const unsigned char* desc, const double* cf) {
   for (int p = 0; p < op.n_s + op.n_t; ++p) {
     const bool s_side = p < op.n_s;
     const FormDesc& f = d[p];
-    const int64_t rows = s_side ? op.a_rows : op.b_rows;
-    const int64_t cols = s_side ? op.a_cols : op.b_cols;
+    const int64_t rows = f.rows;
+    const int64_t cols = f.cols;
     const int nbc = s_side ? ALG::kK0 : ALG::kN0;
     for (int64_t j = 0; j < cols; ++j)
       for (int64_t i = 0; i < rows; ++i) {
@@ -79,19 +81,19 @@ void run_combine(const fmm::Op& op, const unsigned char* desc, const double* cf)
   const CombineDesc* d = reinterpret_cast<const CombineDesc*>(desc + op.desc_off);
   for (int p = 0; p < op.n; ++p) {
     const CombineDesc& c = d[p];
-    for (int64_t j = 0; j < op.cols; ++j)
-      for (int64_t i = 0; i < op.rows; ++i) {
+    for (int64_t j = 0; j < c.cols; ++j)
+      for (int64_t i = 0; i < c.rows; ++i) {
         auto ld = [&](int r) -> double { return c.m[r * c.m_stride + i + j * c.ld_m]; };
         auto ptr = [&](int b) -> double* {
           const int bi = b / ALG::kN0, bj = b % ALG::kN0;
-          return c.c + (bi * op.rows + i) + (bj * op.cols + j) * c.ld_c;
+          return c.c + (bi * c.rows + i) + (bj * c.cols + j) * c.ld_c;
         };
         auto ldc = [&](int b) -> double { return *ptr(b); };
         auto st = [&](int b, double v) { *ptr(b) = v; };
-        if (op.beta != 0.0)
-          ALG::template combine<double, true>(cf, op.beta, ld, ldc, st);
+        if (c.beta != 0.0)
+          ALG::template combine<double, true>(cf, c.beta, ld, ldc, st);
         else
-          ALG::template combine<double, false>(cf, op.beta, ld, ldc, st);
+          ALG::template combine<double, false>(cf, 0.0, ld, ldc, st);
       }
   }
 }
@@ -119,15 +121,29 @@ void run_gemm(const fmm::Op& op, const unsigned char* desc) {
   }
 }
 
-template <class ALG>
-void run_ops(const fmm::Program& prog, const double* cf) {
+void run_ops(const fmm::Program& prog) {
   for (const fmm::Op& op : prog.ops) {
+    const double* cf = prog.coefs[(size_t)op.cf].v;
     switch (op.kind) {
       case fmm::OpKind::kForm:
-        run_form<ALG>(op, prog.desc.data(), cf);
+        switch (op.alg) {
+#define EMU_FORM(idx, ALG) \
+  case idx:                \
+    run_form<ALG>(op, prog.desc.data(), cf); \
+    break;
+          FMM_FOR_EACH_ALGORITHM(EMU_FORM)
+#undef EMU_FORM
+        }
         break;
       case fmm::OpKind::kCombine:
-        run_combine<ALG>(op, prog.desc.data(), cf);
+        switch (op.alg) {
+#define EMU_COMB(idx, ALG) \
+  case idx:                \
+    run_combine<ALG>(op, prog.desc.data(), cf); \
+    break;
+          FMM_FOR_EACH_ALGORITHM(EMU_COMB)
+#undef EMU_COMB
+        }
         break;
       case fmm::OpKind::kGemm:
         run_gemm(op, prog.desc.data());
@@ -157,21 +173,58 @@ int emu_fast_matmul(int alg, double* A, int64_t lda, double* B, int64_t ldb, dou
   fmm::Program prog;
   fmm::build_program(alg, m, k, n, steps, x, alpha, beta, dfs_levels, fmm::Operand{A, lda}, fmm::Operand{B, ldb},
                      fmm::Operand{C, ldc}, base, &prog);
-  double cf[FMM_MAX_SLOTS > 0 ? FMM_MAX_SLOTS : 1];
-  fmm_algorithms[alg].eval(x, cf);
-  switch (alg) {
-#define EMU_CASE(idx, ALG)             \
-  case idx:                            \
-    emu::run_ops<emu::ALG>(prog, cf);  \
-    break;
-    FMM_FOR_EACH_ALGORITHM(EMU_CASE)
-#undef EMU_CASE
-  }
+  emu::run_ops(prog);
   if (stats) {
     int64_t nf = 0, ng = 0, nc = 0;
     for (const fmm::Op& op : prog.ops) {
       nf += op.kind == fmm::OpKind::kForm;
       ng += op.kind == fmm::OpKind::kGemm;
+      nc += op.kind == fmm::OpKind::kCombine;
+    }
+    stats[0] = nf;
+    stats[1] = ng;
+    stats[2] = nc;
+    stats[3] = prog.leaf_count;
+    stats[4] = (int64_t)prog.workspace_bytes;
+  }
+  return 0;
+}
+
+// A batch through the planner + interpreter: item i is
+// (algs[i], steps[i], dims[3i..3i+2]) on A_i, B_i, C_i packed column-major
+// (lda = m, ...) at the given offsets into A, B, C.
+int emu_fast_matmul_batch(int count, const int* algs, const int* steps, const int64_t* dims, double* A,
+                          const int64_t* a_off, double* B, const int64_t* b_off, double* C, const int64_t* c_off,
+                          double x, double alpha, double beta, int64_t* stats) {
+  std::vector<fmm::BatchItem> items((size_t)count);
+  for (int i = 0; i < count; ++i) {
+    fmm::BatchItem& it = items[(size_t)i];
+    it.alg = algs[i];
+    it.steps = steps[i];
+    it.m = dims[3 * i];
+    it.k = dims[3 * i + 1];
+    it.n = dims[3 * i + 2];
+    it.A = fmm::Operand{A + a_off[i], it.m > 0 ? it.m : 1};
+    it.B = fmm::Operand{B + b_off[i], it.k > 0 ? it.k : 1};
+    it.C = fmm::Operand{C + c_off[i], it.m > 0 ? it.m : 1};
+    it.x = x;
+    it.alpha = alpha;
+    it.beta = beta;
+    it.classical = it.alg < 0;
+    if (it.classical) it.alg = 0;
+  }
+  const size_t bytes = fmm::batch_workspace_bytes(items.data(), count);
+  std::vector<double> ws(bytes / sizeof(double) + 64, std::numeric_limits<double>::quiet_NaN());
+  double* base = ws.data();
+  while (reinterpret_cast<uintptr_t>(base) % 256) ++base;
+  fmm::Program prog;
+  fmm::build_batch_program(items.data(), count, base, &prog);
+  emu::run_ops(prog);
+  if (stats) {
+    int64_t nf = 0, ng = 0, nc = 0;
+    for (const fmm::Op& op : prog.ops) {
+      nf += op.kind == fmm::OpKind::kForm;
+      ng += op.kind == fmm::OpKind::kGemm && !op.peel;
       nc += op.kind == fmm::OpKind::kCombine;
     }
     stats[0] = nf;

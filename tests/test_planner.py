@@ -80,3 +80,42 @@ def test_workspace_scales_with_breadth_first_levels():
     assert sizes[0] == sizes[1] > sizes[2] > sizes[3] > 0
     # the reference's MemoryManager needs ~209.7 GiB here; pure DFS needs a small fraction
     assert sizes[3] < 20 * 2**30
+
+
+def test_batch_program_matches_oracle_per_item():
+    """Mixed batch (algorithms, depths, odd shapes): every item equals its own
+    oracle call bit for bit, and all leaves share one GEMM launch."""
+    E = emulator()
+    rng = np.random.default_rng(3)
+    names = ["strassen", "grey424_26_206", "grey333_23_125", "classical222_8_24", "smirnov333_23_128"]
+    specs = []
+    for i in range(14):
+        alg = names[i % len(names)]
+        steps = [0, 1, 2][i % 3]
+        m, k, n = (int(v) for v in rng.integers(5, 70, size=3))
+        specs.append((alg, steps, m, k, n))
+    a_off, b_off, c_off, dims, algs, steps = [], [], [], [], [], []
+    ta = tb = tc = 0
+    for alg, s, m, k, n in specs:
+        a_off.append(ta); b_off.append(tb); c_off.append(tc)
+        ta += m * k; tb += k * n; tc += m * n
+        dims += [m, k, n]; algs.append(NAMES.index(alg)); steps.append(s)
+    A = oracle.uniform(ta, 1, 8, 1).ravel()
+    B = oracle.uniform(tb, 1, 8, 2).ravel()
+    C0 = oracle.uniform(tc, 1, 8, 3).ravel()
+    C = C0.copy()
+    i64 = ctypes.c_int64
+    arr = lambda t, v: (t * len(v))(*v)
+    stats = (i64 * 5)()
+    rc = E.emu_fast_matmul_batch(len(specs), arr(ctypes.c_int, algs), arr(ctypes.c_int, steps), arr(i64, dims),
+                                 A.ctypes.data_as(P), arr(i64, a_off), B.ctypes.data_as(P), arr(i64, b_off),
+                                 C.ctypes.data_as(P), arr(i64, c_off), 1e-8, 1.25, 0.5, stats)
+    assert rc == 0
+    assert stats[1] == 1  # one leaf GEMM launch for the whole batch
+    for i, (alg, s, m, k, n) in enumerate(specs):
+        Ai = np.asfortranarray(A[a_off[i]:a_off[i] + m * k].reshape(k, m).T)
+        Bi = np.asfortranarray(B[b_off[i]:b_off[i] + k * n].reshape(n, k).T)
+        want = np.asfortranarray(C0[c_off[i]:c_off[i] + m * n].reshape(n, m).T)
+        oracle.fast_matmul(alg, Ai, Bi, want, s, 1e-8, 1.25, 0.5)
+        got = np.asfortranarray(C[c_off[i]:c_off[i] + m * n].reshape(n, m).T)
+        assert np.array_equal(want, got), (i, alg, s, m, k, n)
