@@ -53,10 +53,12 @@ def parse_args(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=4096, help="edge of the CPU baseline sample")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU work budget of the baseline sample")
-    ap.add_argument("--workload", default="product", choices=["product", "batch"],
+    ap.add_argument("--workload", default="product", choices=["product", "batch", "serve"],
                     help="product: one large FastMatmul (the headline); batch: 4096 independent products "
                          "with log-uniform dimensions in [64, 1024] in one CUDA-graph plan")
     ap.add_argument("--batch-count", type=int, default=4096)
+    ap.add_argument("--serve-requests", type=int, default=300)
+    ap.add_argument("--serve-slots", type=int, default=6)
     ap.add_argument("--sweep", action="store_true",
                     help="time every configuration of the fast-vs-classical study (one JSON line each) "
                          "instead of the single headline line")
@@ -553,6 +555,113 @@ def run_batch_workload(a):
     return 0
 
 
+def run_serve_workload(a):
+    """Poisson stream of FP64 products, M, K, N each log-uniform in [256, 8192],
+    uniform [-1, 1) entries, operands resident in device memory, offered at
+    twice the rate that one-at-a-time launches sustain; the server admits
+    requests by workspace footprint into concurrent batches (--serve-slots).  Reports
+    throughput, p50/p99 latency (submission to completion) and the
+    one-at-a-time throughput on the same requests."""
+    import threading
+
+    import numpy as np
+    import torch
+
+    import fast_matmul_b200 as fmm
+
+    torch.cuda.set_device(0)
+    h = fmm.default_handle(0)
+    rng = np.random.default_rng(77)
+    N = a.serve_requests
+    dims = np.floor(np.exp(rng.uniform(np.log(256), np.log(8192), size=(N, 3)))).astype(int)
+    split_share = 0.3
+    wants_split = rng.uniform(size=N) < split_share
+    reqs = []
+    for i, (m, k, n) in enumerate(dims):
+        reqs.append((fmm.random_matrix(int(m), int(k), 9000 + i, 1, -1.0, 1.0, handle=h),
+                     fmm.random_matrix(int(k), int(n), 9000 + i, 2, -1.0, 1.0, handle=h),
+                     fmm.colmajor_empty(int(m), int(n))))
+    flops = float(sum(2.0 * m * n * k for m, k, n in dims))
+
+    def alone(i):
+        A, B, C = reqs[i]
+        alg, steps = fmm.autotune_choice(*(int(v) for v in dims[i]), handle=h)
+        if alg == fmm.CLASSICAL:
+            fmm.matmul(A, B, C, handle=h)
+        else:
+            fmm.fast_matmul(alg, A, B, C, steps, handle=h)
+
+    for i in range(min(N, 8)):  # warm
+        alone(i)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in range(N):
+        alone(i)
+        torch.cuda.synchronize()
+    t_single = time.perf_counter() - t0
+    reference = [reqs[i][2].clone() for i in range(0, N, max(1, N // 16))]
+    # one-at-a-time plain launches: the classical FP64 GEMM per request
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for A, B, C in reqs:
+        fmm.matmul(A, B, C, handle=h)
+        torch.cuda.synchronize()
+    t_plain = time.perf_counter() - t0
+    for _, _, C in reqs:
+        C.zero_()
+    torch.cuda.synchronize()
+
+    rate = 2.0 * N / t_single  # requests per second offered
+    gaps = rng.exponential(1.0 / rate, size=N)
+    srv = fmm.Server(0, workspace_bytes=0, max_inflight=a.serve_slots, max_batch=64)
+    tickets = [None] * N
+
+    def client():
+        t_next = time.perf_counter()
+        for i in range(N):
+            t_next += gaps[i]
+            d = t_next - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            A, B, C = reqs[i]
+            tickets[i] = srv.submit(A, B, C, fmm.AUTO)
+
+    th = threading.Thread(target=client)
+    th.start()
+    th.join()
+    srv.drain()
+    infos = [srv.wait(t) for t in tickets]
+    stats = srv.stats()
+    srv.close()
+    t_first = min(x["submit_ms"] for x in infos)
+    t_last = max(x["done_ms"] for x in infos)
+    t_serve = (t_last - t_first) * 1e-3
+    lat = np.array([x["done_ms"] - x["submit_ms"] for x in infos])
+    same = all(torch.equal(ref, reqs[i][2]) for ref, i in zip(reference, range(0, N, max(1, N // 16))))
+    out = {
+        "metric": METRIC, "value": flops / t_serve / 1e12, "unit": "TFLOP/s", "n_gpus": 1, "steps": N,
+        "warmup": 8, "ms_per_step": t_serve * 1e3 / N, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "serving: %d Poisson requests, M,K,N log-uniform in [256,8192], uniform[-1,1), "
+                               "offered at 2x the one-at-a-time rate (%.1f req/s), FP64 (the split-BF16 share "
+                               "of %.0f%% is served in FP64)" % (N, rate, 100 * split_share),
+                   "total_tflop": flops / 1e12, "requests_marked_split_bf16": int(wants_split.sum())},
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                       "max": float(lat.max())},
+        "one_at_a_time": {"value": flops / t_single / 1e12, "seconds": t_single,
+                          "throughput_ratio_of_server": t_single / t_serve,
+                          "what": "same algorithm choice per request, one launch set + synchronize each"},
+        "one_at_a_time_plain": {"value": flops / t_plain / 1e12, "seconds": t_plain,
+                                "throughput_ratio_of_server": t_plain / t_serve,
+                                "what": "classical FP64 GEMM per request, launch + synchronize each"},
+        "server": stats,
+        "results_identical_to_alone": bool(same),
+        "gpu_launches": stats["launches"],
+    }
+    print(json.dumps(out))
+    return 0
+
+
 def main(argv=None):
     a = parse_args(argv)
     if a.impl == "reference":
@@ -561,6 +670,8 @@ def main(argv=None):
         return run_sweep(a)
     if a.workload == "batch":
         return run_batch_workload(a)
+    if a.workload == "serve":
+        return run_serve_workload(a)
     return run_ours(a)
 
 

@@ -11,6 +11,7 @@ from .api import (  # noqa: F401
     CLASSICAL,
     Handle,
     Plan,
+    Server,
     autotune,
     autotune_choice,
     autotune_load,

@@ -80,6 +80,33 @@ class BatchItem(ctypes.Structure):
     ]
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("workspace_bytes", ctypes.c_size_t), ("max_inflight", ctypes.c_int),
+                ("max_batch", ctypes.c_int)]
+
+
+class Request(ctypes.Structure):
+    _fields_ = [
+        ("alg", ctypes.c_int), ("num_steps", ctypes.c_int), ("precision", ctypes.c_int),
+        ("A", ctypes.c_void_p), ("lda", ctypes.c_int64),
+        ("B", ctypes.c_void_p), ("ldb", ctypes.c_int64),
+        ("C", ctypes.c_void_p), ("ldc", ctypes.c_int64),
+        ("m", ctypes.c_int64), ("k", ctypes.c_int64), ("n", ctypes.c_int64),
+        ("x", ctypes.c_double), ("alpha", ctypes.c_double), ("beta", ctypes.c_double),
+    ]
+
+
+class RequestInfo(ctypes.Structure):
+    _fields_ = [("done", ctypes.c_int), ("status", ctypes.c_int), ("submit_ms", ctypes.c_double),
+                ("launch_ms", ctypes.c_double), ("done_ms", ctypes.c_double)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("launches", ctypes.c_int64),
+                ("batches", ctypes.c_int64), ("max_batch_seen", ctypes.c_int64),
+                ("workspace_peak", ctypes.c_size_t)]
+
+
 # name -> (restype, argtypes); every function declared in include/fmm.h
 SIGNATURES = {
     "fmm_options_init": (None, [ctypes.POINTER(Options)]),
@@ -142,6 +169,13 @@ SIGNATURES = {
     "fmm_plan_execute": (ctypes.c_int, [ctypes.c_void_p]),
     "fmm_plan_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "fmm_plan_kernel_count": (ctypes.c_int64, [ctypes.c_void_p]),
+    "fmm_server_create": (ctypes.c_int, [ctypes.POINTER(ServerConfig), ctypes.POINTER(ctypes.c_void_p)]),
+    "fmm_server_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_uint64)]),
+    "fmm_server_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_double,
+                                        ctypes.POINTER(RequestInfo)]),
+    "fmm_server_drain": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
+    "fmm_server_get_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ServerStats)]),
+    "fmm_server_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "fmm_profile_enable": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "fmm_profile_reset": (ctypes.c_int, [ctypes.c_void_p]),
     "fmm_profile_read": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Profile)]),

@@ -394,3 +394,61 @@ class Plan:
             self.close()
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------------------
+# serving: continuous-batching request loop (fmm_server_*)
+
+
+class Server:
+    """Requests are admitted in arrival order as launch slots and workspace
+    free up; results are written into each request's C in place."""
+
+    def __init__(self, device: int = 0, workspace_bytes: int = 0, max_inflight: int = 4, max_batch: int = 64):
+        cfg = _lib.ServerConfig(device, workspace_bytes, max_inflight, max_batch)
+        self._s = ctypes.c_void_p()
+        check(lib().fmm_server_create(ctypes.byref(cfg), ctypes.byref(self._s)))
+        self._keep = {}
+
+    def submit(self, A, B, C, alg=AUTO, num_steps: int = 1, precision: str = "fp64", x: float = 1e-8,
+               alpha: float = 1.0, beta: float = 0.0) -> int:
+        m, k = A.shape
+        n = B.shape[1]
+        pa, lda = _mat(A, m, k, "A")
+        pb, ldb = _mat(B, k, n, "B")
+        pc, ldc = _mat(C, m, n, "C")
+        if not (isinstance(alg, int) and alg < 0):
+            alg = algorithm_index(alg)
+        r = _lib.Request(alg, num_steps, _lib.PRECISIONS[precision], pa, lda, pb, ldb, pc, ldc, m, k, n, x, alpha,
+                         beta)
+        t = ctypes.c_uint64()
+        check(lib().fmm_server_submit(self._s, ctypes.byref(r), ctypes.byref(t)))
+        self._keep[t.value] = (A, B, C)  # operands stay alive until the request is done
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: float = -1.0) -> dict:
+        inf = _lib.RequestInfo()
+        check(lib().fmm_server_wait(self._s, ticket, timeout_ms, ctypes.byref(inf)))
+        self._keep.pop(ticket, None)
+        return {"done": bool(inf.done), "status": inf.status, "submit_ms": inf.submit_ms,
+                "launch_ms": inf.launch_ms, "done_ms": inf.done_ms}
+
+    def drain(self, timeout_ms: float = -1.0) -> None:
+        check(lib().fmm_server_drain(self._s, timeout_ms))
+
+    def stats(self) -> dict:
+        st = _lib.ServerStats()
+        check(lib().fmm_server_get_stats(self._s, ctypes.byref(st)))
+        return {name: getattr(st, name) for name, _ in st._fields_}
+
+    def close(self):
+        if self._s:
+            lib().fmm_server_destroy(self._s)
+            self._s = ctypes.c_void_p()
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

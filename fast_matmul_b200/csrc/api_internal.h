@@ -8,6 +8,7 @@
 #include <string>
 #include <tuple>
 #include <utility>
+#include <vector>
 
 #include "fmm.h"
 #include "fmm_internal.h"
@@ -79,6 +80,9 @@ fmm_status check_dims(int64_t m, int64_t k, int64_t n, int64_t lda, int64_t ldb,
 void resolve_options(const fmm_options* opts, fmm_options* out);
 fmm_status choose_dfs_levels(fmm_handle h, int alg, int64_t m, int64_t k, int64_t n, int steps,
                              const fmm_options& o, int* dfs_levels, size_t* bytes);
+// Batch items with FMM_ALG_AUTO / FMM_ALG_CLASSICAL resolved (batch.cpp);
+// items with an empty result are dropped.
+fmm_status resolve_items(fmm_handle h, const fmm_batch_item* items, int count, std::vector<fmm::BatchItem>* out);
 
 }  // namespace api
 }  // namespace fmm

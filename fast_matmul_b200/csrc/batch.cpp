@@ -57,6 +57,11 @@ void choice_for(fmm_handle h, int64_t m, int64_t k, int64_t n, int* alg, int* st
   rule_choice(m, k, n, alg, steps);
 }
 
+}  // namespace
+
+namespace fmm {
+namespace api {
+
 fmm_status resolve_items(fmm_handle h, const fmm_batch_item* items, int count, std::vector<fmm::BatchItem>* out) {
   out->clear();
   out->reserve((size_t)count);
@@ -95,6 +100,11 @@ fmm_status resolve_items(fmm_handle h, const fmm_batch_item* items, int count, s
   }
   return FMM_OK;
 }
+
+}  // namespace api
+}  // namespace fmm
+
+namespace {
 
 // Splits resolved items into consecutive groups whose workspace fits `limit`.
 std::vector<std::pair<int, int>> chunk_items(const std::vector<fmm::BatchItem>& items, size_t limit) {

@@ -232,6 +232,64 @@ fmm_status fmm_plan_destroy(fmm_plan p);
 /* Kernels one execution launches. */
 int64_t fmm_plan_kernel_count(fmm_plan p);
 
+/* ---- Serving: a continuous-batching request loop (no counterpart in the
+ * reference).  A background thread admits queued requests, in arrival
+ * order, whenever a launch slot (one stream each) is free and the S/T/M
+ * workspace of the request fits in the server's workspace pool; the
+ * requests admitted together go out as one batch program on that slot's
+ * stream, so work of different slots overlaps on the device.  Operands stay
+ * where the caller put them (device memory); C is written in place.  Each
+ * result equals the one fmm_fast_matmul (or the classical product) gives for
+ * the request alone, bit for bit. */
+typedef struct fmm_server_s* fmm_server;
+
+typedef struct fmm_server_config {
+  int device;
+  size_t workspace_bytes; /* pool for in-flight S/T/M temporaries (0 = 40% of free memory) */
+  int max_inflight;       /* launch slots / streams (0 = 4) */
+  int max_batch;          /* requests per launch (0 = 64) */
+} fmm_server_config;
+
+typedef struct fmm_request {
+  int alg;        /* algorithm index, FMM_ALG_AUTO or FMM_ALG_CLASSICAL */
+  int num_steps;
+  int precision;  /* fmm_precision */
+  const double* A;
+  int64_t lda;
+  const double* B;
+  int64_t ldb;
+  double* C;
+  int64_t ldc;
+  int64_t m, k, n;
+  double x, alpha, beta;
+} fmm_request;
+
+typedef struct fmm_request_info {
+  int done;          /* 1 once C holds the result */
+  fmm_status status; /* of the request's planning / launch */
+  double submit_ms;  /* host clock (ms since the server started) at submission */
+  double launch_ms;  /* ... when its batch was launched */
+  double done_ms;    /* ... when its batch was seen complete */
+} fmm_request_info;
+
+typedef struct fmm_server_stats {
+  int64_t submitted, completed, launches, batches;
+  int64_t max_batch_seen;
+  size_t workspace_peak;
+} fmm_server_stats;
+
+fmm_status fmm_server_create(const fmm_server_config* cfg, fmm_server* out);
+fmm_status fmm_server_submit(fmm_server s, const fmm_request* req, uint64_t* ticket);
+/* Waits up to timeout_ms (< 0: forever) for a request; FMM_ERR_TIMEOUT if it
+ * is not done by then. */
+fmm_status fmm_server_wait(fmm_server s, uint64_t ticket, double timeout_ms, fmm_request_info* info);
+/* Waits up to timeout_ms (< 0: forever) until every submitted request is done. */
+fmm_status fmm_server_drain(fmm_server s, double timeout_ms);
+fmm_status fmm_server_get_stats(fmm_server s, fmm_server_stats* out);
+/* Stops the loop after the in-flight work finishes; pending requests are
+ * dropped with FMM_ERR_TIMEOUT. */
+fmm_status fmm_server_destroy(fmm_server s);
+
 /* Allocation-free FastMatmul.  No counterpart in the reference.
  *
  * For callers that may not allocate device memory at all: code whose device
