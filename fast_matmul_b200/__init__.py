@@ -25,8 +25,10 @@ from .api import (  # noqa: F401
     fast_matmul,
     fast_matmul_host,
     matmul,
+    matmul_split_bf16,
     max_relative_diff,
     num_algorithms,
     random_matrix,
+    synchronize,
     workspace_bytes,
 )

@@ -77,6 +77,7 @@ class BatchItem(ctypes.Structure):
         ("C", ctypes.c_void_p), ("ldc", ctypes.c_int64),
         ("m", ctypes.c_int64), ("k", ctypes.c_int64), ("n", ctypes.c_int64),
         ("x", ctypes.c_double), ("alpha", ctypes.c_double), ("beta", ctypes.c_double),
+        ("precision", ctypes.c_int), ("split_slices", ctypes.c_int),
     ]
 
 
@@ -93,6 +94,7 @@ class Request(ctypes.Structure):
         ("C", ctypes.c_void_p), ("ldc", ctypes.c_int64),
         ("m", ctypes.c_int64), ("k", ctypes.c_int64), ("n", ctypes.c_int64),
         ("x", ctypes.c_double), ("alpha", ctypes.c_double), ("beta", ctypes.c_double),
+        ("split_slices", ctypes.c_int),
     ]
 
 
@@ -139,6 +141,10 @@ SIGNATURES = {
     "fmm_dgemm_host": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
                                        ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
                                        ctypes.c_int64, ctypes.c_int64, ctypes.c_double, ctypes.c_double]),
+    "fmm_dgemm_split_bf16": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+                                             ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
+                                             ctypes.c_int64, ctypes.c_int64, ctypes.c_double, ctypes.c_double,
+                                             ctypes.c_int]),
     "fmm_fill_uniform": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
                                          ctypes.c_int64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_double,
                                          ctypes.c_double]),
@@ -147,6 +153,7 @@ SIGNATURES = {
                                               c_double_p]),
     "fmm_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
     "fmm_kernel_launch_count": (ctypes.c_int64, [ctypes.c_void_p]),
+    "fmm_selftest_wait_timeout": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.POINTER(ctypes.c_int)]),
     "fmm_fast_matmul_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
                                                 ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
                                                 ctypes.c_int64, ctypes.c_int64, ctypes.c_int, ctypes.c_double,

@@ -176,10 +176,11 @@ def _options(schedule="auto", dfs_levels=-1, workspace_limit=0, precision="fp64"
 
 def fast_matmul(alg, A, B, C, num_steps: int, x: float = 1e-8, alpha: float = 1.0, beta: float = 0.0,
                 schedule: str = "auto", dfs_levels: int = -1, workspace_limit: int = 0,
-                handle: Optional[Handle] = None) -> None:
+                precision: str = "fp64", split_slices: int = 0, handle: Optional[Handle] = None) -> None:
     """C := alpha * A * B + beta * C with `num_steps` levels of algorithm
     `alg` -- <alg>::FastMatmul(A, B, C, num_steps, x, alpha, beta).
-    Queued on torch's current stream."""
+    precision "split_bf16" runs the leaf products on the BF16 tensor cores
+    over `split_slices` slices (0 = 5).  Queued on torch's current stream."""
     idx = algorithm_index(alg)
     m, k = A.shape
     k2, n = B.shape
@@ -189,15 +190,16 @@ def fast_matmul(alg, A, B, C, num_steps: int, x: float = 1e-8, alpha: float = 1.
     pb, ldb = _mat(B, k, n, "B")
     pc, ldc = _mat(C, m, n, "C")
     h = handle or default_handle(C.device.index)
-    o = _options(schedule, dfs_levels, workspace_limit)
+    o = _options(schedule, dfs_levels, workspace_limit, precision, split_slices)
     check(lib().fmm_fast_matmul(h.ptr, idx, pa, lda, pb, ldb, pc, ldc, m, k, n, num_steps, x, alpha, beta,
                                 ctypes.byref(o)))
 
 
 def workspace_bytes(alg, m: int, k: int, n: int, num_steps: int, schedule: str = "auto", dfs_levels: int = -1,
-                    workspace_limit: int = 0, handle: Optional[Handle] = None) -> int:
+                    workspace_limit: int = 0, precision: str = "fp64", split_slices: int = 0,
+                    handle: Optional[Handle] = None) -> int:
     h = handle or default_handle()
-    o = _options(schedule, dfs_levels, workspace_limit)
+    o = _options(schedule, dfs_levels, workspace_limit, precision, split_slices)
     out = ctypes.c_size_t()
     check(lib().fmm_workspace_query(h.ptr, algorithm_index(alg), m, k, n, num_steps, ctypes.byref(o),
                                     ctypes.byref(out)))
@@ -247,6 +249,26 @@ def matmul(A, B, C, alpha: float = 1.0, beta: float = 0.0, handle: Optional[Hand
     pc, ldc = _mat(C, m, n, "C")
     h = handle or default_handle(C.device.index)
     check(lib().fmm_dgemm(h.ptr, pa, lda, pb, ldb, pc, ldc, m, k, n, alpha, beta))
+
+
+def matmul_split_bf16(A, B, C, alpha: float = 1.0, beta: float = 0.0, slices: int = 0,
+                      handle: Optional[Handle] = None) -> None:
+    """Classical C := alpha * A * B + beta * C with split-BF16 tensor-core
+    products (fmm_dgemm_split_bf16; `slices` 0 = 5)."""
+    m, k = A.shape
+    n = B.shape[1]
+    pa, lda = _mat(A, m, k, "A")
+    pb, ldb = _mat(B, k, n, "B")
+    pc, ldc = _mat(C, m, n, "C")
+    h = handle or default_handle(C.device.index)
+    check(lib().fmm_dgemm_split_bf16(h.ptr, pa, lda, pb, ldb, pc, ldc, m, k, n, alpha, beta, slices))
+
+
+def synchronize(handle: Optional[Handle] = None) -> None:
+    """Waits for the handle's stream; raises if a split-BF16 kernel reported
+    a bounded wait that gave up."""
+    h = handle or default_handle()
+    check(lib().fmm_synchronize(h.ptr))
 
 
 def random_matrix(m: int, n: int, seed: int, stream: int = 0, lo: float = 0.0, hi: float = 1.0, device=None,
@@ -302,6 +324,8 @@ def _batch_items(problems):
         it.x = float(p.get("x", 1e-8))
         it.alpha = float(p.get("alpha", 1.0))
         it.beta = float(p.get("beta", 0.0))
+        it.precision = _lib.PRECISIONS[p.get("precision", "fp64")]
+        it.split_slices = int(p.get("split_slices", 0))
     return arr
 
 
@@ -355,7 +379,7 @@ class Plan:
 
     @classmethod
     def for_product(cls, alg, A, B, C, num_steps, x=1e-8, alpha=1.0, beta=0.0, schedule="auto",
-                    handle: Optional[Handle] = None):
+                    precision: str = "fp64", split_slices: int = 0, handle: Optional[Handle] = None):
         m, k = A.shape
         n = B.shape[1]
         pa, lda = _mat(A, m, k, "A")
@@ -363,7 +387,7 @@ class Plan:
         pc, ldc = _mat(C, m, n, "C")
         h = handle or default_handle(C.device.index)
         out = ctypes.c_void_p()
-        o = _options(schedule)
+        o = _options(schedule, precision=precision, split_slices=split_slices)
         check(lib().fmm_plan_create(h.ptr, algorithm_index(alg), pa, lda, pb, ldb, pc, ldc, m, k, n, num_steps, x,
                                     alpha, beta, ctypes.byref(o), ctypes.byref(out)))
         return cls(out, h)
@@ -411,7 +435,7 @@ class Server:
         self._keep = {}
 
     def submit(self, A, B, C, alg=AUTO, num_steps: int = 1, precision: str = "fp64", x: float = 1e-8,
-               alpha: float = 1.0, beta: float = 0.0) -> int:
+               alpha: float = 1.0, beta: float = 0.0, split_slices: int = 0) -> int:
         m, k = A.shape
         n = B.shape[1]
         pa, lda = _mat(A, m, k, "A")
@@ -420,7 +444,7 @@ class Server:
         if not (isinstance(alg, int) and alg < 0):
             alg = algorithm_index(alg)
         r = _lib.Request(alg, num_steps, _lib.PRECISIONS[precision], pa, lda, pb, ldb, pc, ldc, m, k, n, x, alpha,
-                         beta)
+                         beta, split_slices)
         t = ctypes.c_uint64()
         check(lib().fmm_server_submit(self._s, ctypes.byref(r), ctypes.byref(t)))
         self._keep[t.value] = (A, B, C)  # operands stay alive until the request is done

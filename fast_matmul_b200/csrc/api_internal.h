@@ -41,6 +41,7 @@ struct fmm_handle_s {
   double* io = nullptr;
   size_t io_cap = 0;
   double* d_small = nullptr;  // two doubles for reductions
+  int* d_err = nullptr;       // error codes of split-BF16 kernels (bounded waits that gave up)
   int64_t launches = 0;
   fmm::Program prog;
   bool profiling = false;
@@ -78,6 +79,10 @@ fmm_status run_staged(fmm_handle h, const fmm::Program& prog);
 fmm_status check_alg(int alg);
 fmm_status check_dims(int64_t m, int64_t k, int64_t n, int64_t lda, int64_t ldb, int64_t ldc);
 void resolve_options(const fmm_options* opts, fmm_options* out);
+// Slices of the leaf products for a precision (0 for FP64).
+fmm_status split_slices_for(int precision, int requested, int* slices);
+// Reads and clears the handle's device error word (synchronises the stream).
+fmm_status check_device_errors(fmm_handle h);
 fmm_status choose_dfs_levels(fmm_handle h, int alg, int64_t m, int64_t k, int64_t n, int steps,
                              const fmm_options& o, int* dfs_levels, size_t* bytes);
 // Batch items with FMM_ALG_AUTO / FMM_ALG_CLASSICAL resolved (batch.cpp);

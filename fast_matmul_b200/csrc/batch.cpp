@@ -96,6 +96,8 @@ fmm_status resolve_items(fmm_handle h, const fmm_batch_item* items, int count, s
     b.x = it.x;
     b.alpha = it.alpha;
     b.beta = it.beta;
+    if ((s = split_slices_for(it.precision, it.split_slices, &b.split_slices)) != FMM_OK)
+      return fail(s, "batch item " + std::to_string(i) + ": " + fmm_last_error());
     out->push_back(b);
   }
   return FMM_OK;
@@ -165,7 +167,7 @@ fmm_status plan_capture(fmm_plan p) {
   cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
     int64_t n = 0;
-    e = fmm::run_program(p->prog, p->h_desc, p->d_desc, h->num_sms, cap, &n, nullptr);
+    e = fmm::run_program(p->prog, p->h_desc, p->d_desc, h->num_sms, cap, &n, nullptr, h->d_err);
     cudaGraph_t g = nullptr;
     cudaError_t e2 = cudaStreamEndCapture(cap, &g);
     if (e == cudaSuccess) e = e2;
@@ -336,6 +338,8 @@ fmm_status fmm_plan_create(fmm_handle h, int alg, const double* A, int64_t lda, 
   if (!C || (k > 0 && (!A || !B))) return fail(FMM_ERR_INVALID_ARGUMENT, "null matrix pointer");
   fmm_options o;
   resolve_options(opts, &o);
+  int slices = 0;
+  if ((s = split_slices_for(o.precision, o.split_slices, &slices)) != FMM_OK) return s;
   DeviceGuard g(h->device);
   if (!g.ok()) return fail(FMM_ERR_CUDA, "cudaSetDevice failed");
   int d = 0;
@@ -349,7 +353,7 @@ fmm_status fmm_plan_create(fmm_handle h, int alg, const double* A, int64_t lda, 
     return fail(FMM_ERR_OUT_OF_MEMORY, "cannot allocate the plan's workspace");
   }
   fmm::build_program(alg, m, k, n, num_steps, x, alpha, beta, d, fmm::Operand{const_cast<double*>(A), lda},
-                     fmm::Operand{const_cast<double*>(B), ldb}, fmm::Operand{C, ldc}, p->ws, &p->prog);
+                     fmm::Operand{const_cast<double*>(B), ldb}, fmm::Operand{C, ldc}, p->ws, &p->prog, slices);
   if ((s = plan_capture(p)) != FMM_OK) {
     plan_free(p);
     return s;

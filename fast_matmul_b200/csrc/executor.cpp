@@ -24,7 +24,7 @@ Profiler::~Profiler() {
 }
 
 cudaError_t run_program(const Program& prog, const void* h_desc, void* d_desc, int num_sms, cudaStream_t stream,
-                        int64_t* launches, Profiler* prof) {
+                        int64_t* launches, Profiler* prof, int* d_err) {
   if (!prog.desc.empty()) {
     cudaError_t e = cudaMemcpyAsync(d_desc, h_desc, prog.desc.size(), cudaMemcpyHostToDevice, stream);
     if (e != cudaSuccess) return e;
@@ -55,6 +55,13 @@ cudaError_t run_program(const Program& prog, const void* h_desc, void* d_desc, i
         e = gemm_launch(reinterpret_cast<const GemmDesc*>(base + op.desc_off), op.n, op.total_tiles, num_sms,
                         stream);
         break;
+      case OpKind::kSplitGemm: {
+        int64_t n_launched = 0;
+        e = split_gemm_launch(reinterpret_cast<const SplitDesc*>(base + op.desc_off), op.n, op.split,
+                              prog.split_scratch, d_err, num_sms, stream, &n_launched);
+        count += n_launched - 1;  // the op itself is counted below
+        break;
+      }
       case OpKind::kCombine: {
         CombineLaunch L;
         L.desc = reinterpret_cast<const CombineDesc*>(base + op.desc_off);

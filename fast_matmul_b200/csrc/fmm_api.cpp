@@ -89,7 +89,7 @@ fmm_status stage_descriptors(fmm_handle h, const fmm::Program& prog) {
 
 fmm_status run_staged(fmm_handle h, const fmm::Program& prog) {
   cudaError_t e = fmm::run_program(prog, h->h_desc, h->d_desc, h->num_sms, h->stream, &h->launches,
-                                   h->profiling ? &h->prof : nullptr);
+                                   h->profiling ? &h->prof : nullptr, h->d_err);
   if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
   if (!prog.desc.empty()) {
     FMM_CUDA_TRY(cudaEventRecord(h->desc_done, h->stream), "cudaEventRecord");
@@ -118,23 +118,49 @@ void resolve_options(const fmm_options* opts, fmm_options* out) {
   if (opts) *out = *opts;
 }
 
+fmm_status split_slices_for(int precision, int requested, int* slices) {
+  *slices = 0;
+  if (precision == FMM_PRECISION_FP64) return FMM_OK;
+  if (precision != FMM_PRECISION_SPLIT_BF16) return fail(FMM_ERR_INVALID_ARGUMENT, "unknown precision");
+  const int s = requested == 0 ? FMM_SPLIT_DEFAULT_SLICES : requested;
+  if (s < FMM_SPLIT_MIN_SLICES || s > FMM_SPLIT_MAX_SLICES)
+    return fail(FMM_ERR_INVALID_ARGUMENT, "split_slices must be in [2, 6]");
+  *slices = s;
+  return FMM_OK;
+}
+
+fmm_status check_device_errors(fmm_handle h) {
+  FMM_CUDA_TRY(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+  int code = 0;
+  FMM_CUDA_TRY(cudaMemcpy(&code, h->d_err, sizeof(int), cudaMemcpyDeviceToHost), "read device error word");
+  if (code != 0) {
+    FMM_CUDA_TRY(cudaMemset(h->d_err, 0, sizeof(int)), "clear device error word");
+    return fail(FMM_ERR_TIMEOUT, "a split-BF16 tensor-core kernel gave up a bounded wait (code " +
+                                     std::to_string(code) + "); its results are not valid");
+  }
+  return FMM_OK;
+}
+
 // Depth-first levels for a schedule: the fewest that fit the limit.
 fmm_status choose_dfs_levels(fmm_handle h, int alg, int64_t m, int64_t k, int64_t n, int steps,
                              const fmm_options& o, int* dfs_levels, size_t* bytes) {
   const fmm_alg_table& t = fmm_algorithms[alg];
   const size_t limit = o.workspace_limit ? o.workspace_limit : h->ws_limit;
+  int slices = 0;
+  fmm_status ss = split_slices_for(o.precision, o.split_slices, &slices);
+  if (ss != FMM_OK) return ss;
   auto fits = [&](int d, size_t* b) {
-    *b = fmm::workspace_bytes(t, m, k, n, steps, d);
+    *b = fmm::workspace_bytes(t, m, k, n, steps, d, slices);
     return *b <= limit;
   };
   switch (o.schedule) {
     case FMM_SCHEDULE_BFS:
       *dfs_levels = 0;
-      *bytes = fmm::workspace_bytes(t, m, k, n, steps, 0);
+      *bytes = fmm::workspace_bytes(t, m, k, n, steps, 0, slices);
       break;
     case FMM_SCHEDULE_DFS:
       *dfs_levels = steps;
-      *bytes = fmm::workspace_bytes(t, m, k, n, steps, steps);
+      *bytes = fmm::workspace_bytes(t, m, k, n, steps, steps, slices);
       break;
     case FMM_SCHEDULE_HYBRID:
     case FMM_SCHEDULE_AUTO: {
@@ -143,7 +169,7 @@ fmm_status choose_dfs_levels(fmm_handle h, int alg, int64_t m, int64_t k, int64_
         if (o.dfs_levels >= 0) {
           if (o.dfs_levels > steps) return fail(FMM_ERR_INVALID_ARGUMENT, "dfs_levels exceeds num_steps");
           *dfs_levels = o.dfs_levels;
-          *bytes = fmm::workspace_bytes(t, m, k, n, steps, o.dfs_levels);
+          *bytes = fmm::workspace_bytes(t, m, k, n, steps, o.dfs_levels, slices);
           break;
         }
         // dfs_levels 0 and 1 plan identically (the root level has a single
@@ -207,9 +233,12 @@ fmm_status fmm_handle_create(fmm_handle* out, int device) {
   if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = (size_t)8 << 30;
   h->ws_limit = (size_t)(0.6 * (double)free_b);
   if (cudaEventCreateWithFlags(&h->desc_done, cudaEventDisableTiming) != cudaSuccess ||
-      cudaMalloc(&h->d_small, 2 * sizeof(double)) != cudaSuccess) {
+      cudaMalloc(&h->d_small, 2 * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&h->d_err, 256) != cudaSuccess || cudaMemset(h->d_err, 0, 256) != cudaSuccess) {
     cudaGetLastError();
     if (h->desc_done) cudaEventDestroy(h->desc_done);
+    if (h->d_small) cudaFree(h->d_small);
+    if (h->d_err) cudaFree(h->d_err);
     delete h;
     return fail(FMM_ERR_CUDA, "handle setup failed");
   }
@@ -226,6 +255,7 @@ fmm_status fmm_handle_destroy(fmm_handle h) {
   if (h->h_desc) cudaFreeHost(h->h_desc);
   if (h->io) cudaFree(h->io);
   if (h->d_small) cudaFree(h->d_small);
+  if (h->d_err) cudaFree(h->d_err);
   if (h->desc_done) cudaEventDestroy(h->desc_done);
   delete h;
   return FMM_OK;
@@ -310,8 +340,8 @@ fmm_status fmm_fast_matmul(fmm_handle h, int alg, const double* A, int64_t lda, 
   if (!C || (k > 0 && (!A || !B))) return fail(FMM_ERR_INVALID_ARGUMENT, "null matrix pointer");
   fmm_options o;
   resolve_options(opts, &o);
-  if (o.precision != FMM_PRECISION_FP64)
-    return fail(FMM_ERR_NOT_SUPPORTED, "only FMM_PRECISION_FP64 is available in this build");
+  int slices = 0;
+  if ((s = split_slices_for(o.precision, o.split_slices, &slices)) != FMM_OK) return s;
   DeviceGuard g(h->device);
   if (!g.ok()) return fail(FMM_ERR_CUDA, "cudaSetDevice failed");
   int d = 0;
@@ -320,7 +350,7 @@ fmm_status fmm_fast_matmul(fmm_handle h, int alg, const double* A, int64_t lda, 
   if ((s = ensure_device_buffer(h, &h->ws, &h->ws_cap, bytes ? bytes : 256, "workspace")) != FMM_OK) return s;
   try {
     fmm::build_program(alg, m, k, n, num_steps, x, alpha, beta, d, fmm::Operand{const_cast<double*>(A), lda},
-                       fmm::Operand{const_cast<double*>(B), ldb}, fmm::Operand{C, ldc}, h->ws, &h->prog);
+                       fmm::Operand{const_cast<double*>(B), ldb}, fmm::Operand{C, ldc}, h->ws, &h->prog, slices);
   } catch (const std::exception& ex) {
     return fail(FMM_ERR_OUT_OF_MEMORY, std::string("planning failed: ") + ex.what());
   }
@@ -370,7 +400,7 @@ fmm_status fmm_fast_matmul_host(fmm_handle h, int alg, const double* A, int64_t 
   FMM_CUDA_TRY(cudaMemcpy2DAsync(C, ldc * sizeof(double), dC, ldC * sizeof(double), m * sizeof(double), n,
                                  cudaMemcpyDeviceToHost, h->stream),
                "copy C to host");
-  FMM_CUDA_TRY(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+  if ((s = check_device_errors(h)) != FMM_OK) return s;
   if (elapsed_ms)
     *elapsed_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   return FMM_OK;
@@ -454,6 +484,52 @@ fmm_status fmm_dgemm_host(fmm_handle h, const double* A, int64_t lda, const doub
   return FMM_OK;
 }
 
+fmm_status fmm_dgemm_split_bf16(fmm_handle h, const double* A, int64_t lda, const double* B, int64_t ldb,
+                                double* C, int64_t ldc, int64_t m, int64_t k, int64_t n, double alpha, double beta,
+                                int slices) {
+  if (!h) return fail(FMM_ERR_INVALID_ARGUMENT, "null handle");
+  fmm_status s = check_dims(m, k, n, lda, ldb, ldc);
+  if (s != FMM_OK) return s;
+  int sl = 0;
+  if ((s = split_slices_for(FMM_PRECISION_SPLIT_BF16, slices, &sl)) != FMM_OK) return s;
+  if (m == 0 || n == 0) return FMM_OK;
+  if (!C || (k > 0 && (!A || !B))) return fail(FMM_ERR_INVALID_ARGUMENT, "null matrix pointer");
+  DeviceGuard g(h->device);
+  if (!g.ok()) return fail(FMM_ERR_CUDA, "cudaSetDevice failed");
+  fmm::Program& prog = h->prog;
+  prog.clear();
+  fmm::SplitDesc d{};
+  d.A = A;
+  d.B = B;
+  d.C = C;
+  d.lda = lda;
+  d.ldb = ldb;
+  d.ldc = ldc;
+  d.m = (int)m;
+  d.n = (int)n;
+  d.k = (int)k;
+  d.alpha = alpha;
+  d.beta = beta;
+  const fmm::SplitPlan plan = fmm::split_prepare(&d, 1, sl);
+  if ((s = ensure_device_buffer(h, &h->ws, &h->ws_cap, plan.bytes, "split scratch")) != FMM_OK) return s;
+  prog.desc.resize(sizeof(d));
+  std::memcpy(prog.desc.data(), &d, sizeof(d));
+  prog.split_slices = sl;
+  prog.split_scratch = static_cast<char*>(h->ws);
+  prog.split_bytes = plan.bytes;
+  prog.workspace_bytes = plan.bytes;
+  fmm::Op op;
+  op.kind = fmm::OpKind::kSplitGemm;
+  op.n = 1;
+  op.total_tiles = plan.tiles;
+  op.desc_off = 0;
+  op.flops = 2.0 * (double)m * (double)n * (double)k;
+  op.split = plan;
+  prog.ops.push_back(op);
+  if ((s = stage_descriptors(h, prog)) != FMM_OK) return s;
+  return run_staged(h, prog);
+}
+
 fmm_status fmm_fill_uniform(fmm_handle h, double* out, int64_t rows, int64_t cols, int64_t ld, uint64_t seed,
                             uint64_t stream, double lo, double hi) {
   if (!h) return fail(FMM_ERR_INVALID_ARGUMENT, "null handle");
@@ -485,7 +561,21 @@ fmm_status fmm_max_relative_diff(fmm_handle h, const double* a, int64_t lda, con
 fmm_status fmm_synchronize(fmm_handle h) {
   if (!h) return fail(FMM_ERR_INVALID_ARGUMENT, "null handle");
   DeviceGuard g(h->device);
+  return check_device_errors(h);
+}
+
+fmm_status fmm_selftest_wait_timeout(fmm_handle h, double limit_ms, int* code) {
+  if (!h || !code) return fail(FMM_ERR_INVALID_ARGUMENT, "null argument");
+  if (!(limit_ms > 0.0) || limit_ms > 1000.0) return fail(FMM_ERR_INVALID_ARGUMENT, "limit_ms must be in (0, 1000]");
+  DeviceGuard g(h->device);
+  if (!g.ok()) return fail(FMM_ERR_CUDA, "cudaSetDevice failed");
   FMM_CUDA_TRY(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+  FMM_CUDA_TRY(cudaMemsetAsync(h->d_err, 0, sizeof(int), h->stream), "clear device error word");
+  FMM_CUDA_TRY(fmm::wait_probe_launch(h->d_err, (uint64_t)(limit_ms * 1e6), 99, h->stream), "wait probe launch");
+  h->launches++;
+  FMM_CUDA_TRY(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+  FMM_CUDA_TRY(cudaMemcpy(code, h->d_err, sizeof(int), cudaMemcpyDeviceToHost), "read device error word");
+  FMM_CUDA_TRY(cudaMemset(h->d_err, 0, sizeof(int)), "clear device error word");
   return FMM_OK;
 }
 
@@ -524,6 +614,7 @@ fmm_status fmm_profile_read(fmm_handle h, fmm_profile* out) {
         out->combine_ms += ms;
         out->combine_bytes += r.bytes;
         break;
+      case fmm::OpKind::kSplitGemm:
       case fmm::OpKind::kGemm:
         if (r.peel) {
           out->peel_launches++;

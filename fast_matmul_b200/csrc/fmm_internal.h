@@ -35,6 +35,64 @@ int64_t gemm_prepare(GemmDesc* descs, int n, int tile_n = kGemmBN, int tile_m = 
 cudaError_t gemm_launch(const GemmDesc* d_descs, int n, int64_t total_tiles, int num_sms, cudaStream_t stream);
 
 // ---------------------------------------------------------------------------
+// Split-BF16 leaf products on the tensor cores (split_bf16.cu):
+// C_p = alpha_p * A_p * B_p + beta_p * C_p with A_p, B_p split into BF16
+// slices after per-row / per-column power-of-two scaling.
+constexpr int kSplitMinSlices = 2;
+constexpr int kSplitMaxSlices = 6;
+constexpr int kSplitDefaultSlices = 5;
+constexpr int kSplitTile = 128;   // output tile rows and columns
+constexpr int kSplitKBlock = 64;  // k-depth of one TMA box (128 bytes of BF16)
+constexpr int kSplitChunk = 128;  // k-depth accumulated exactly in FP32
+
+struct SplitDesc {
+  const double* A;
+  const double* B;
+  double* C;
+  int64_t lda, ldb, ldc;
+  double alpha, beta;
+  int m, n, k;
+  int kblocks;          // padded k / kSplitKBlock
+  int tiles_m, tiles_n; // padded m / kSplitTile, padded n / kSplitTile
+  int64_t tile_begin;   // first output tile of this problem
+  int64_t sa_begin;     // first A-splitting work tile (32 rows x one k-block)
+  int64_t a_row;        // first 128-byte row of this problem's A slices
+  int64_t b_row;        // first 128-byte row of this problem's B slices
+  int64_t e_off;        // first row exponent (tiles_m * 128 entries)
+  int64_t f_off;        // first column exponent (tiles_n * 128 entries)
+};
+
+// Scratch layout of one split launch (offsets from the scratch base).
+struct SplitPlan {
+  int slices = 0;
+  int64_t tiles = 0;     // output tiles over all problems
+  int64_t sa_work = 0;   // A-splitting work tiles
+  int64_t rows_a = 0, rows_b = 0;  // 128-byte slice rows
+  int64_t n_e = 0, n_f = 0;        // row / column exponents
+  size_t off_b = 0, off_e = 0, off_f = 0, bytes = 0;
+};
+
+// Fills the derived fields of descs[0..n) for `slices` slices and returns the
+// scratch layout.  Problems with m == 0 or n == 0 get no tiles.
+SplitPlan split_prepare(SplitDesc* descs, int n, int slices);
+// Adds `count` problems of m x k x n to the sizes of *plan (before
+// split_finish), the same arithmetic split_prepare applies per descriptor.
+void split_accumulate(SplitPlan* plan, int64_t m, int64_t k, int64_t n, int64_t count);
+// Computes the region offsets and total bytes of *plan from its sizes.
+void split_finish(SplitPlan* plan);
+// Scratch bytes split_prepare would report for `count` problems of m x k x n.
+size_t split_scratch_bytes(int64_t m, int64_t k, int64_t n, int64_t count, int slices);
+// Launches splitting and the tensor-core product.  `scratch` holds plan.bytes
+// bytes (256-byte aligned); *d_err (device) receives a nonzero code if a
+// bounded wait inside the product kernel gave up.  Returns the kernel count
+// launched through *launches.
+cudaError_t split_gemm_launch(const SplitDesc* d_descs, int n, const SplitPlan& plan, void* scratch, int* d_err,
+                              int num_sms, cudaStream_t stream, int64_t* launches);
+// A kernel whose single bounded mbarrier wait is never satisfied: it records
+// `code` in *d_err after limit_ns and returns.
+cudaError_t wait_probe_launch(int* d_err, uint64_t limit_ns, int code, cudaStream_t stream);
+
+// ---------------------------------------------------------------------------
 // Operand formation and product combination (block_adds.cu).
 //
 // Form: for each sub-problem, read the M0*K0 (K0*N0) blocks of its input

@@ -296,6 +296,54 @@ void emit_gemm(Program* prog, int level, std::vector<GemmDesc>& g, bool leaves) 
   prog->ops.push_back(op);
 }
 
+// Leaf products of one launch as split-BF16 products with `slices` slices.
+// All split launches of a program run in order on one stream, so they share
+// one scratch region sized for the largest (Program::split_bytes).
+void emit_split_gemm(Program* prog, int level, const std::vector<GemmDesc>& g, int slices) {
+  if (g.empty()) return;
+  std::vector<SplitDesc> sd;
+  sd.reserve(g.size());
+  double flops = 0.0;
+  for (const GemmDesc& d : g) {
+    SplitDesc s{};
+    s.A = d.A;
+    s.B = d.B;
+    s.C = d.C;
+    s.lda = d.lda;
+    s.ldb = d.ldb;
+    s.ldc = d.ldc;
+    s.alpha = d.alpha;
+    s.beta = d.beta;
+    s.m = d.m;
+    s.n = d.n;
+    s.k = d.k;
+    sd.push_back(s);
+    flops += 2.0 * d.m * d.n * (double)d.k;
+  }
+  prog->leaf_flops += flops;
+  prog->leaf_count += (int64_t)g.size();
+  const SplitPlan plan = split_prepare(sd.data(), (int)sd.size(), slices);
+  if (plan.tiles == 0) return;
+  Op op;
+  op.kind = OpKind::kSplitGemm;
+  op.n = (int)sd.size();
+  op.total_tiles = plan.tiles;
+  op.level = level;
+  op.flops = flops;
+  op.split = plan;
+  op.desc_off = append_desc(prog, sd);
+  prog->ops.push_back(op);
+  prog->split_bytes = std::max(prog->split_bytes, plan.bytes);
+}
+
+// Places the split scratch after the recursion's workspace.
+void place_split_scratch(Program* prog, char* ws) {
+  if (prog->split_bytes == 0) return;
+  const size_t off = (size_t)round_up((int64_t)prog->workspace_bytes, 1024);
+  prog->split_scratch = ws + off;
+  prog->workspace_bytes = off + prog->split_bytes;
+}
+
 // ---- single call, any schedule
 
 class Builder {
@@ -311,7 +359,10 @@ class Builder {
       std::vector<GemmDesc> g;
       g.reserve(F.size());
       for (const SubProblem& p : F) g.push_back(leaf_desc(dims_[l], p));
-      emit_gemm(prog_, l, g, true);
+      if (prog_->split_slices > 0)
+        emit_split_gemm(prog_, l, g, prog_->split_slices);
+      else
+        emit_gemm(prog_, l, g, true);
       return;
     }
     if (l < d_) {
@@ -386,6 +437,9 @@ void Program::clear() {
   leaf_flops = 0.0;
   peel_flops = 0.0;
   leaf_count = 0;
+  split_slices = 0;
+  split_scratch = nullptr;
+  split_bytes = 0;
 }
 
 std::vector<LevelDims> level_dims(const fmm_alg_table& t, int64_t m, int64_t k, int64_t n, int steps) {
@@ -412,14 +466,28 @@ int64_t gemm_prepare(GemmDesc* descs, int n, int tile_n, int tile_m) {
   return total;
 }
 
-size_t workspace_bytes(const fmm_alg_table& t, int64_t m, int64_t k, int64_t n, int steps, int dfs_levels) {
+size_t workspace_bytes(const fmm_alg_table& t, int64_t m, int64_t k, int64_t n, int steps, int dfs_levels,
+                       int split_slices) {
   size_t total = 0;
-  layout(t, level_dims(t, m, k, n, steps), steps, dfs_levels, 0, &total);
+  const std::vector<LevelDims> dims = level_dims(t, m, k, n, steps);
+  layout(t, dims, steps, dfs_levels, 0, &total);
+  if (split_slices > 0) {
+    // leaf products per launch: R^steps breadth-first; below depth-first
+    // levels, the R^(steps - d + 1) leaves of one unit at level d - 1
+    int64_t leaves = 1;
+    if (steps > 0) {
+      const int d = std::max(1, std::min(dfs_levels, steps));
+      for (int i = 0; i < steps - d + 1; ++i) leaves *= t.rank;
+    }
+    const LevelDims& L = dims[(size_t)steps];
+    const size_t sb = split_scratch_bytes(L.m, L.k, L.n, leaves, split_slices);
+    if (sb > 0) total = (size_t)round_up((int64_t)total, 1024) + sb;
+  }
   return total;
 }
 
 void build_program(int alg, int64_t m, int64_t k, int64_t n, int steps, double x, double alpha, double beta,
-                   int dfs_levels, Operand A, Operand B, Operand C, void* ws, Program* out) {
+                   int dfs_levels, Operand A, Operand B, Operand C, void* ws, Program* out, int split_slices) {
   const fmm_alg_table& t = fmm_algorithms[alg];
   const std::vector<LevelDims> dims = level_dims(t, m, k, n, steps);
   size_t total = 0;
@@ -430,12 +498,45 @@ void build_program(int alg, int64_t m, int64_t k, int64_t n, int steps, double x
   out->coefs.push_back(cf);
   out->workspace_bytes = total;
   out->dfs_levels = dfs_levels;
+  out->split_slices = split_slices;
   // FastMatmul (strassen.hpp:661-722): A's multiplier is alpha; the first
   // recursion folds it into C's (C.mult = 1 * alpha * 1).
   SubProblem root{A, B, C, 1.0 * alpha * 1.0, beta};
   Builder b(alg, steps, dfs_levels, dims, lay, out->coefs[0].v, static_cast<char*>(ws), out);
   b.level(0, std::vector<SubProblem>{root});
+  place_split_scratch(out, static_cast<char*>(ws));
 }
+
+namespace {
+
+// Split scratch of a batch: one split launch per distinct slice count, all
+// sharing one region.
+size_t batch_split_bytes(const BatchItem* items, int count) {
+  std::map<int, SplitPlan> plans;
+  for (int i = 0; i < count; ++i) {
+    const BatchItem& it = items[i];
+    if (it.split_slices <= 0) continue;
+    SplitPlan& p = plans[it.split_slices];
+    p.slices = it.split_slices;
+    if (it.classical) {
+      split_accumulate(&p, it.m, it.k, it.n, 1);
+      continue;
+    }
+    const fmm_alg_table& t = fmm_algorithms[it.alg];
+    const std::vector<LevelDims> dims = level_dims(t, it.m, it.k, it.n, it.steps);
+    int64_t leaves = 1;
+    for (int l = 0; l < it.steps; ++l) leaves *= t.rank;
+    split_accumulate(&p, dims[(size_t)it.steps].m, dims[(size_t)it.steps].k, dims[(size_t)it.steps].n, leaves);
+  }
+  size_t mx = 0;
+  for (auto& kv : plans) {
+    split_finish(&kv.second);
+    if (kv.second.tiles > 0) mx = std::max(mx, kv.second.bytes);
+  }
+  return mx;
+}
+
+}  // namespace
 
 size_t batch_workspace_bytes(const BatchItem* items, int count) {
   size_t off = 0;
@@ -446,6 +547,8 @@ size_t batch_workspace_bytes(const BatchItem* items, int count) {
     layout(t, level_dims(t, items[i].m, items[i].k, items[i].n, items[i].steps), items[i].steps, 0, off, &end);
     off = (size_t)round_up((int64_t)end, 256);
   }
+  const size_t sb = batch_split_bytes(items, count);
+  if (sb > 0) off = (size_t)round_up((int64_t)off, 1024) + sb;
   return off;
 }
 
@@ -516,19 +619,26 @@ void build_batch_program(const BatchItem* items, int count, void* ws, Program* o
       emit_form(out, g.first.first, g.first.second, l, sd, td, vec2, mx, bytes);
     }
   }
-  // every leaf of every item: one grouped GEMM
+  // every leaf of every item: one grouped GEMM (FP64), one split launch per
+  // distinct slice count
   {
-    std::vector<GemmDesc> g;
+    std::map<int, std::vector<GemmDesc>> g;
     for (int i = 0; i < count; ++i) {
       const ItemState& s = st[(size_t)i];
       const size_t steps = (size_t)steps_of(i);
+      std::vector<GemmDesc>& dst = g[std::max(0, items[i].split_slices)];
       for (const SubProblem& p : s.frontier[steps]) {
         GemmDesc d = leaf_desc(s.dims[steps], p);
         if (items[i].classical) d.beta = items[i].beta;
-        g.push_back(d);
+        dst.push_back(d);
       }
     }
-    emit_gemm(out, max_steps, g, true);
+    for (auto& kv : g) {
+      if (kv.first == 0)
+        emit_gemm(out, max_steps, kv.second, true);
+      else
+        emit_split_gemm(out, max_steps, kv.second, kv.first);
+    }
   }
   // combinations and fringes, bottom-up
   for (int l = max_steps - 1; l >= 0; --l) {
@@ -560,6 +670,7 @@ void build_batch_program(const BatchItem* items, int count, void* ws, Program* o
     }
     emit_gemm(out, l, peel, false);
   }
+  place_split_scratch(out, base);
 }
 
 }  // namespace fmm

@@ -16,7 +16,7 @@ struct Operand {
   int64_t ld;
 };
 
-enum class OpKind { kForm, kGemm, kCombine };
+enum class OpKind { kForm, kGemm, kCombine, kSplitGemm };
 
 struct Op {
   OpKind kind;
@@ -32,6 +32,7 @@ struct Op {
   int level = 0;         // recursion level the launch belongs to (steps = leaves)
   double flops = 0.0;    // gemm: 2 * m * n * k summed over the problems
   double bytes = 0.0;    // form / combine: algorithmic HBM bytes (each input read once, each output written once)
+  SplitPlan split;       // split gemm: scratch layout (offsets from Program::split_scratch)
 };
 
 // Per-launch timing with CUDA events (fmm_profile_* in include/fmm.h).
@@ -59,6 +60,9 @@ struct Program {
   double leaf_flops = 0.0;  // 2 * m * n * k summed over leaf products
   double peel_flops = 0.0;
   int64_t leaf_count = 0;
+  int split_slices = 0;         // > 0: leaf products run split-BF16 with this many slices
+  char* split_scratch = nullptr;  // scratch shared by the split launches (inside the workspace)
+  size_t split_bytes = 0;       // its size
   void clear();
 };
 
@@ -70,12 +74,16 @@ struct LevelDims {
 // linalg/linalg.hpp:179-184).
 std::vector<LevelDims> level_dims(const fmm_alg_table& t, int64_t m, int64_t k, int64_t n, int steps);
 
-// Workspace bytes for `dfs_levels` depth-first levels (0 = all breadth-first).
-size_t workspace_bytes(const fmm_alg_table& t, int64_t m, int64_t k, int64_t n, int steps, int dfs_levels);
+// Workspace bytes for `dfs_levels` depth-first levels (0 = all breadth-first);
+// split_slices > 0 adds the scratch of split-BF16 leaf products.
+size_t workspace_bytes(const fmm_alg_table& t, int64_t m, int64_t k, int64_t n, int steps, int dfs_levels,
+                       int split_slices = 0);
 
 // Builds the launch program of one call.  ws must hold workspace_bytes(...) bytes.
+// split_slices > 0 runs the leaf products (not the fringe products of
+// dynamic peeling) split-BF16 with that many slices.
 void build_program(int alg, int64_t m, int64_t k, int64_t n, int steps, double x, double alpha, double beta,
-                   int dfs_levels, Operand A, Operand B, Operand C, void* ws, Program* out);
+                   int dfs_levels, Operand A, Operand B, Operand C, void* ws, Program* out, int split_slices = 0);
 
 // One independent product of a batch.  A classical item is one GEMM
 // C = alpha * A * B + beta * C (beta honoured; alg and steps unused); the
@@ -87,6 +95,7 @@ struct BatchItem {
   Operand A, B, C;
   double x, alpha, beta;
   bool classical;
+  int split_slices = 0;  // > 0: this item's leaf products run split-BF16
 };
 
 // Workspace of a batch (every item planned breadth-first, regions back to back).
@@ -101,8 +110,9 @@ void build_batch_program(const BatchItem* items, int count, void* ws, Program* o
 // Runs a built program: one host-to-device copy of all descriptors to
 // d_desc (which must hold prog.desc.size() bytes), then the launches in order.
 // Adds the number of kernels launched to *launches (may be null).
-// When prof is non-null every launch is bracketed by CUDA events.
+// When prof is non-null every launch is bracketed by CUDA events.  d_err
+// (device int) collects the error codes of split-BF16 launches.
 cudaError_t run_program(const Program& prog, const void* h_desc, void* d_desc, int num_sms, cudaStream_t stream,
-                        int64_t* launches, Profiler* prof = nullptr);
+                        int64_t* launches, Profiler* prof = nullptr, int* d_err = nullptr);
 
 }  // namespace fmm

@@ -8,8 +8,9 @@
 //   2. for every idle slot, admits queued requests in arrival order while the
 //      summed S/T/M workspace of the requests fits one free block of the pool
 //      (and at most max_batch requests), plans them as one batch program
-//      (breadth-first per request, all leaf products in one grouped GEMM) and
-//      launches it on the slot's stream.
+//      (breadth-first per request, all FP64 leaf products in one grouped GEMM,
+//      all split-BF16 leaf products in one tensor-core launch per slice
+//      count) and launches it on the slot's stream.
 // Requests that arrive while earlier batches run are admitted as soon as a
 // slot and memory free up; batches of different slots overlap on the device.
 
@@ -43,6 +44,8 @@ struct Slot {
   std::vector<uint64_t> tickets;
   size_t ws_off = 0, ws_size = 0;
   fmm::Program prog;
+  int* d_err = nullptr;  // error word of the slot's split-BF16 kernels
+  int* h_err = nullptr;  // pinned copy, valid once `done` has completed
 };
 
 struct Pending {
@@ -136,6 +139,8 @@ fmm_batch_item as_item(const fmm_request& r) {
   it.x = r.x;
   it.alpha = r.alpha;
   it.beta = r.beta;
+  it.precision = r.precision;
+  it.split_slices = r.split_slices;
   return it;
 }
 
@@ -174,7 +179,8 @@ bool turn(fmm_server s) {
     if (!sl.busy) continue;
     const cudaError_t q = cudaEventQuery(sl.done);
     if (q == cudaErrorNotReady) continue;
-    const fmm_status st = q == cudaSuccess ? FMM_OK : FMM_ERR_CUDA;
+    fmm_status st = q == cudaSuccess ? FMM_OK : FMM_ERR_CUDA;
+    if (st == FMM_OK && *sl.h_err != 0) st = FMM_ERR_TIMEOUT;  // a bounded device wait gave up
     for (uint64_t t : sl.tickets) finish(s, t, st);
     sl.tickets.clear();
     pool_free(s, sl.ws_off, sl.ws_size);
@@ -191,12 +197,6 @@ bool turn(fmm_server s) {
     const size_t avail = largest_free(s);
     while (!s->pending.empty() && (int)batch.size() < s->max_batch) {
       const Pending& p = s->pending.front();
-      if (p.req.precision != FMM_PRECISION_FP64) {
-        finish(s, p.ticket, FMM_ERR_NOT_SUPPORTED);
-        s->pending.pop_front();
-        progressed = true;
-        continue;
-      }
       const fmm_batch_item it = as_item(p.req);
       std::vector<fmm::BatchItem> one;
       fmm_status st = resolve_items(s->h, &it, 1, &one);
@@ -234,11 +234,17 @@ bool turn(fmm_server s) {
       } catch (const std::exception&) {
         st = FMM_ERR_OUT_OF_MEMORY;
       }
+      // the batch's own layout never exceeds the summed per-request footprints
+      if (st == FMM_OK && sl.prog.workspace_bytes > need) st = FMM_ERR_OUT_OF_MEMORY;
       if (st == FMM_OK && !ensure_slot_buffers(sl, sl.prog.desc.size() + 64)) st = FMM_ERR_OUT_OF_MEMORY;
       if (st == FMM_OK) {
         std::memcpy(sl.h_desc, sl.prog.desc.data(), sl.prog.desc.size());
         int64_t n = 0;
-        const cudaError_t e = fmm::run_program(sl.prog, sl.h_desc, sl.d_desc, s->h->num_sms, sl.stream, &n, nullptr);
+        *sl.h_err = 0;
+        cudaError_t e = cudaMemsetAsync(sl.d_err, 0, sizeof(int), sl.stream);
+        if (e == cudaSuccess)
+          e = fmm::run_program(sl.prog, sl.h_desc, sl.d_desc, s->h->num_sms, sl.stream, &n, nullptr, sl.d_err);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(sl.h_err, sl.d_err, sizeof(int), cudaMemcpyDeviceToHost, sl.stream);
         if (e != cudaSuccess) st = FMM_ERR_CUDA;
         s->stats.launches += n;
       }
@@ -306,7 +312,8 @@ fmm_status fmm_server_create(const fmm_server_config* cfg, fmm_server* out) {
   s->slots.resize((size_t)nslots);
   for (Slot& sl : s->slots) {
     if (cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) != cudaSuccess || !ensure_slot_buffers(sl, 1 << 20)) {
+        cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) != cudaSuccess || !ensure_slot_buffers(sl, 1 << 20) ||
+        cudaMalloc(&sl.d_err, 256) != cudaSuccess || cudaMallocHost(&sl.h_err, sizeof(int)) != cudaSuccess) {
       cudaGetLastError();
       s->stop = true;
       fmm_server_destroy(s);
@@ -380,6 +387,8 @@ fmm_status fmm_server_destroy(fmm_server s) {
     if (sl.done) cudaEventDestroy(sl.done);
     if (sl.h_desc) cudaFreeHost(sl.h_desc);
     if (sl.d_desc) cudaFree(sl.d_desc);
+    if (sl.d_err) cudaFree(sl.d_err);
+    if (sl.h_err) cudaFreeHost(sl.h_err);
   }
   if (s->pool) cudaFree(s->pool);
   fmm_handle_destroy(s->h);

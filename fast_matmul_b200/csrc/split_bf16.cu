@@ -1,0 +1,479 @@
+// Split-BF16 leaf products on the sm_100a tensor cores (tcgen05, TMA, TMEM).
+//
+// An FP64 product C = alpha * A * B + beta * C is computed from BF16 slices:
+//   * every row i of A is scaled by 2^-e_i (e_i: the least exponent with
+//     max_p |a_ip| < 2^e_i), every column j of B by 2^-f_j; scaling by a
+//     power of two is exact;
+//   * each scaled value x in (-1, 1) is split into S integer digits
+//     d_1 = rint(256 x), d_t = rint(256 r_{t-1}) with r the running
+//     remainder, so x = sum_t d_t 2^-8t + r_S 2^-8S with |r_S| <= 1/2;
+//     |d_1| <= 256 and |d_t| <= 128 are exact BF16 values;
+//   * C_ij = alpha 2^(e_i + f_j) sum_{t+u <= S+1} 2^-8(t+u) (dA_t dB_u)_ij,
+//     S (S + 1) / 2 slice products.  The products of one diagonal t + u are
+//     accumulated by the tensor cores in FP32 over k chunks of 128: every
+//     partial sum is an integer of magnitude <= 2^24, so the accumulation is
+//     exact.  After each chunk the diagonal's sum is scaled by 2^-8(t+u) and
+//     added into an FP64 accumulator: all rounding happens in FP64, in a
+//     fixed order.
+// Error: |x - sum_t d_t 2^-8t| <= 2^-(8S+1) 2^e per operand entry plus the
+// dropped diagonals, so |C - AB| <~ 3 * 2^-8S * k * max|a_i.| * max|b_.j|.
+//
+// Product kernel: persistent CTAs over the 128 x 128 output tiles of every
+// problem.  Warp 0 issues TMA loads of (A_t, B_u) 64-deep k-blocks into a
+// 6-stage ring, warp 1 issues tcgen05.mma (M128 N128 K16) into one of two
+// TMEM accumulators of 128 FP32 columns, warps 2-9 (two warpgroups of 64
+// columns) drain each finished accumulator into FP64 registers.  Every
+// mbarrier wait is bounded; on a timeout the kernel records a code in *err,
+// lets its copies and MMAs in flight finish, frees its TMEM and returns.
+
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+
+#include "fmm_internal.h"
+#include "sm100_primitives.cuh"
+
+namespace fmm {
+namespace {
+
+using namespace sm100;
+
+constexpr int kBM = kSplitTile, kBN = kSplitTile, kBK = kSplitKBlock, kStages = 6;
+constexpr int kTileABytes = kBM * kBK * 2;  // 16 KB
+constexpr int kTileBBytes = kBN * kBK * 2;  // 16 KB
+constexpr int kStageBytes = kTileABytes + kTileBBytes;
+constexpr int kChunkBlocks = kSplitChunk / kBK;
+// TMA warp, MMA warp, 2 x 4 epilogue warps.  Registers are budgeted per
+// group of four warps, so the 10 warps are charged as 12: 168 per thread.
+constexpr int kGemmThreads = 320;
+constexpr size_t kGemmSmem = (size_t)kStages * kStageBytes + 1024;
+static_assert(kSplitChunk % kBK == 0, "chunks are whole k-blocks");
+static_assert(kBK * 2 == 128, "one k-block row is one 128-byte swizzle row");
+
+// Largest i in [0, n) with key(d[i]) <= x (keys non-decreasing).
+template <typename Key>
+__device__ __forceinline__ int find_desc(const SplitDesc* __restrict__ d, int n, int64_t x, Key key) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (key(d[mid]) <= x)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ int exponent_above(double maxabs) {
+  if (!(maxabs > 0.0)) return 0;
+  int e;
+  frexp(maxabs, &e);  // maxabs = f 2^e, f in [0.5, 1)
+  return e;
+}
+
+// ---------------------------------------------------------------------------
+// splitting
+
+// Row exponents of A: one thread per padded row (coalesced down each column).
+__global__ void __launch_bounds__(256) split_row_exponents(const SplitDesc* __restrict__ d, int nd, int64_t total,
+                                                           int* __restrict__ ea) {
+  for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < total; x += (int64_t)gridDim.x * blockDim.x) {
+    const int q = find_desc(d, nd, x, [](const SplitDesc& s) { return s.e_off; });
+    const SplitDesc& s = d[q];
+    const int64_t i = x - s.e_off;
+    double mx = 0.0;
+    if (i < s.m) {
+      const double* a = s.A + i;
+      const int64_t lda = s.lda;
+      int p = 0;
+      for (; p + 4 <= s.k; p += 4) {
+        const double v0 = a[p * lda], v1 = a[(p + 1) * lda], v2 = a[(p + 2) * lda], v3 = a[(p + 3) * lda];
+        mx = fmax(mx, fmax(fmax(fabs(v0), fabs(v1)), fmax(fabs(v2), fabs(v3))));
+      }
+      for (; p < s.k; ++p) mx = fmax(mx, fabs(a[p * lda]));
+    }
+    ea[x] = exponent_above(mx);
+  }
+}
+
+// A slices: one work tile = 32 rows x one 64-deep k-block, read column-major
+// (coalesced along rows), written as 128-byte k-block rows for every slice.
+__global__ void __launch_bounds__(256) split_a(const SplitDesc* __restrict__ d, int nd, int64_t total, int slices,
+                                               const int* __restrict__ ea, __nv_bfloat16* __restrict__ out) {
+  __shared__ double tile[64][33];
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int row = threadIdx.x >> 3, kc = (threadIdx.x & 7) * 8;
+  for (int64_t w = blockIdx.x; w < total; w += gridDim.x) {
+    const int q = find_desc(d, nd, w, [](const SplitDesc& s) { return s.sa_begin; });
+    const SplitDesc& s = d[q];
+    const int64_t mp = (int64_t)s.tiles_m * kBM;
+    const int64_t local = w - s.sa_begin;
+    const int64_t rt = local % (mp / 32), kb = local / (mp / 32);
+    const int64_t i0 = rt * 32, p0 = kb * kBK;
+    __syncthreads();  // previous tile's readers are done
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const int64_t p = p0 + ty + 8 * r, i = i0 + tx;
+      tile[ty + 8 * r][tx] = (i < s.m && p < s.k) ? s.A[i + p * s.lda] : 0.0;
+    }
+    __syncthreads();
+    const int e = ea[s.e_off + i0 + row];
+    double x[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) x[c] = ldexp(tile[kc + c][row], -e);
+    for (int t = 0; t < slices; ++t) {
+      __align__(16) __nv_bfloat16 v[8];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        const double y = x[c] * 256.0;
+        const double dg = rint(y);
+        x[c] = y - dg;
+        v[c] = __double2bfloat16(dg);
+      }
+      const int64_t orow = s.a_row + ((int64_t)t * s.kblocks + kb) * mp + i0 + row;
+      *reinterpret_cast<uint4*>(out + orow * kBK + kc) = *reinterpret_cast<const uint4*>(v);
+    }
+  }
+}
+
+// B: one block per padded column: the column maximum, then the slices (B's
+// columns are contiguous in k, so they are written as they are read).
+__global__ void __launch_bounds__(256) split_b(const SplitDesc* __restrict__ d, int nd, int64_t total, int slices,
+                                               int* __restrict__ fb, __nv_bfloat16* __restrict__ out) {
+  __shared__ double red[8];
+  __shared__ int e_sh;
+  for (int64_t x = blockIdx.x; x < total; x += gridDim.x) {
+    const int q = find_desc(d, nd, x, [](const SplitDesc& s) { return s.f_off; });
+    const SplitDesc& s = d[q];
+    const int64_t j = x - s.f_off;
+    const int64_t np = (int64_t)s.tiles_n * kBN;
+    const double* b = s.B + j * s.ldb;
+    const bool live = j < s.n;
+    double mx = 0.0;
+    if (live)
+      for (int p = threadIdx.x; p < s.k; p += blockDim.x) mx = fmax(mx, fabs(b[p]));
+    for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double v = 0.0;
+      for (int w = 0; w < 8; ++w) v = fmax(v, red[w]);
+      e_sh = exponent_above(v);
+      fb[x] = e_sh;
+    }
+    __syncthreads();
+    const int f = e_sh;
+    const int kp = s.kblocks * kBK;
+    for (int p = threadIdx.x; p < kp; p += blockDim.x) {
+      double v = (live && p < s.k) ? ldexp(b[p], -f) : 0.0;
+      const int64_t kb = p / kBK, pk = p % kBK;
+      for (int t = 0; t < slices; ++t) {
+        const double y = v * 256.0;
+        const double dg = rint(y);
+        v = y - dg;
+        const int64_t orow = s.b_row + ((int64_t)t * s.kblocks + kb) * np + j;
+        out[orow * kBK + pk] = __double2bfloat16(dg);
+      }
+    }
+    __syncthreads();  // e_sh and red are reused by the next column
+  }
+}
+
+// ---------------------------------------------------------------------------
+// tensor-core product of the slices
+
+struct GemmParams {
+  const SplitDesc* desc;
+  const int* ea;
+  const int* fb;
+  int* err;
+  int nd;
+  int slices;
+  int64_t tiles;
+};
+
+struct TileCoord {
+  int q, tm, tn;
+};
+
+__device__ __forceinline__ TileCoord tile_coord(const GemmParams& g, int64_t tile) {
+  TileCoord c;
+  c.q = find_desc(g.desc, g.nd, tile, [](const SplitDesc& s) { return s.tile_begin; });
+  const SplitDesc& s = g.desc[c.q];
+  const int64_t rem = tile - s.tile_begin;
+  c.tm = (int)(rem % s.tiles_m);
+  c.tn = (int)(rem / s.tiles_m);
+  return c;
+}
+
+__global__ void __launch_bounds__(kGemmThreads, 1)
+    split_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                      const GemmParams g) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  __shared__ __align__(8) uint64_t full[kStages], empty[kStages], acc_full[2], acc_empty[2], mma_done;
+  __shared__ uint32_t tmem_slot;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int S = g.slices;
+  if (tid == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&acc_full[b], 1);
+      mbar_init(&acc_empty[b], 8);
+    }
+    mbar_init(&mma_done, 1);
+    fence_barrier_init();
+  }
+  if (warp == 1) tmem_alloc(&tmem_slot, 256);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      prefetch_tensormap(&tmA);
+      prefetch_tensormap(&tmB);
+      uint32_t it = 0;
+      bool ok = true;
+      for (int64_t tile = blockIdx.x; tile < g.tiles && ok; tile += gridDim.x) {
+        const TileCoord tc = tile_coord(g, tile);
+        const SplitDesc& s = g.desc[tc.q];
+        const int64_t mp = (int64_t)s.tiles_m * kBM, np = (int64_t)s.tiles_n * kBN;
+        const int chunks = s.kblocks / kChunkBlocks;
+        for (int c = 0; c < chunks && ok; ++c)
+          for (int D = 0; D < S && ok; ++D)
+            for (int t = 0; t <= D && ok; ++t)
+              for (int kb = 0; kb < kChunkBlocks; ++kb, ++it) {
+                const int st = it % kStages;
+                if (it >= kStages && !mbar_wait(&empty[st], ((it / kStages) & 1) ^ 1, g.err, 1)) {
+                  ok = false;
+                  break;
+                }
+                const int64_t blk = (int64_t)c * kChunkBlocks + kb;
+                const int ya = (int)(s.a_row + ((int64_t)t * s.kblocks + blk) * mp + (int64_t)tc.tm * kBM);
+                const int yb = (int)(s.b_row + ((int64_t)(D - t) * s.kblocks + blk) * np + (int64_t)tc.tn * kBN);
+                uint8_t* dst = base + st * kStageBytes;
+                mbar_arrive_expect_tx(&full[st], kStageBytes);
+                tma_load_2d(dst, &tmA, &full[st], 0, ya);
+                tma_load_2d(dst + kTileABytes, &tmB, &full[st], 0, yb);
+              }
+      }
+      // let every copy in flight land before the CTA can exit
+      for (uint32_t st = 0; st < (uint32_t)kStages && st < it; ++st) {
+        const uint32_t last = st + ((it - 1 - st) / kStages) * kStages;
+        mbar_wait(&full[st], (last / kStages) & 1, g.err, 5);
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      const uint32_t idesc = idesc_bf16_f32(kBM, kBN);
+      uint32_t it = 0, ai = 0;
+      bool ok = true;
+      for (int64_t tile = blockIdx.x; tile < g.tiles && ok; tile += gridDim.x) {
+        const TileCoord tc = tile_coord(g, tile);
+        const int chunks = g.desc[tc.q].kblocks / kChunkBlocks;
+        for (int c = 0; c < chunks && ok; ++c)
+          for (int D = 0; D < S && ok; ++D, ++ai) {
+            const int buf = ai & 1;
+            if (ai >= 2 && !mbar_wait(&acc_empty[buf], ((ai >> 1) & 1) ^ 1, g.err, 2)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint32_t d_tmem = tmem + buf * kBN;
+            bool acc = false;
+            for (int t = 0; t <= D && ok; ++t)
+              for (int kb = 0; kb < kChunkBlocks; ++kb, ++it) {
+                const int st = it % kStages;
+                if (!mbar_wait(&full[st], (it / kStages) & 1, g.err, 3)) {
+                  ok = false;
+                  break;
+                }
+                tc_fence_after();
+                const uint32_t a = smem_addr(base + st * kStageBytes);
+#pragma unroll
+                for (int kk = 0; kk < kBK / 16; ++kk) {
+                  mma_bf16(d_tmem, smem_desc_sw128(a + kk * 32), smem_desc_sw128(a + kTileABytes + kk * 32), idesc,
+                           acc);
+                  acc = true;
+                }
+                mma_commit(&empty[st]);
+              }
+            if (ok) mma_commit(&acc_full[buf]);
+          }
+      }
+      // every MMA issued by this thread completes before TMEM is freed
+      mma_commit(&mma_done);
+      mbar_wait(&mma_done, 0, g.err, 6);
+    }
+  } else {
+    // warpgroup wg owns columns [64 wg, 64 wg + 64) of the tile; warp
+    // quadrant qd owns TMEM lanes (tile rows) [32 qd, 32 qd + 32)
+    const int wg = (warp - 2) >> 2, qd = warp & 3;
+    const int row_in_tile = qd * 32 + lane;
+    uint32_t ai = 0;
+    bool ok = true;
+    for (int64_t tile = blockIdx.x; tile < g.tiles && ok; tile += gridDim.x) {
+      const TileCoord tc = tile_coord(g, tile);
+      const SplitDesc& s = g.desc[tc.q];
+      const int chunks = s.kblocks / kChunkBlocks;
+      double acc[64];
+#pragma unroll
+      for (int j = 0; j < 64; ++j) acc[j] = 0.0;
+      for (int c = 0; c < chunks && ok; ++c)
+        for (int D = 0; D < S; ++D, ++ai) {
+          const int buf = ai & 1;
+          if (!mbar_wait(&acc_full[buf], (ai >> 1) & 1, g.err, 4)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const double scale = ldexp(1.0, -8 * (D + 2));
+          const uint32_t taddr = tmem + ((uint32_t)(qd * 32) << 16) + buf * kBN + wg * 64;
+#pragma unroll
+          for (int g4 = 0; g4 < 4; ++g4) {
+            uint32_t r[16];
+            tmem_ld_32x32b_x16(taddr + g4 * 16, r);
+            tmem_ld_wait();
+            if (g4 == 3) {  // the accumulator is free once the last piece is in registers
+              tc_fence_before();
+              __syncwarp();
+              if (lane == 0) mbar_arrive(&acc_empty[buf]);
+            }
+#pragma unroll
+            for (int j = 0; j < 16; ++j)
+              acc[g4 * 16 + j] = fma((double)__uint_as_float(r[j]), scale, acc[g4 * 16 + j]);
+          }
+        }
+      if (!ok) break;
+      const int64_t row = (int64_t)tc.tm * kBM + row_in_tile;
+      if (row < s.m) {
+        const int er = g.ea[s.e_off + row];
+        const int64_t col0 = (int64_t)tc.tn * kBN + wg * 64;
+        const int* fcol = g.fb + s.f_off + col0;
+        double* cp = s.C + row;
+        const double alpha = s.alpha, beta = s.beta;
+#pragma unroll
+        for (int j = 0; j < 64; ++j) {
+          const int64_t col = col0 + j;
+          if (col < s.n) {
+            double v = __dmul_rn(alpha, ldexp(acc[j], er + fcol[j]));
+            if (beta != 0.0) v = __dadd_rn(v, __dmul_rn(beta, cp[col * s.ldc]));
+            cp[col * s.ldc] = v;
+          }
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 1) tmem_dealloc(tmem, 256);
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  });
+  return fn;
+}
+
+// {64 BF16, rows} view of a slice buffer; boxes of `box_rows` 128-byte rows.
+bool encode_slices(CUtensorMap* map, void* base, int64_t rows, int box_rows) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)kBK, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)kBK * 2};
+  const cuuint32_t box[2] = {(cuuint32_t)kBK, (cuuint32_t)box_rows};
+  const cuuint32_t es[2] = {1, 1};
+  return enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+unsigned grid_for(int64_t work, int64_t cap) { return (unsigned)(work < cap ? (work > 0 ? work : 1) : cap); }
+
+// One thread waits on an mbarrier that nothing arrives on: the bounded wait
+// must give up after limit_ns and record `code` (a check of the timeout path
+// that every kernel here relies on).
+__global__ void wait_probe_kernel(int* err, uint64_t limit_ns, int code) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x != 0) return;
+  mbar_init(&bar, 1);
+  fence_barrier_init();
+  mbar_wait(&bar, 0, err, code, limit_ns);
+}
+
+}  // namespace
+
+cudaError_t wait_probe_launch(int* d_err, uint64_t limit_ns, int code, cudaStream_t stream) {
+  wait_probe_kernel<<<1, 32, 0, stream>>>(d_err, limit_ns, code);
+  return cudaGetLastError();
+}
+
+cudaError_t split_gemm_launch(const SplitDesc* d_descs, int n, const SplitPlan& plan, void* scratch, int* d_err,
+                              int num_sms, cudaStream_t stream, int64_t* launches) {
+  if (plan.tiles == 0) return cudaSuccess;
+  if (plan.slices < kSplitMinSlices || plan.slices > kSplitMaxSlices || !d_err || !scratch ||
+      reinterpret_cast<uintptr_t>(scratch) % 256 != 0)
+    return cudaErrorInvalidValue;
+  // tensor-map row coordinates are 32-bit
+  if (plan.rows_a >= (int64_t(1) << 31) || plan.rows_b >= (int64_t(1) << 31)) return cudaErrorInvalidValue;
+  char* base = static_cast<char*>(scratch);
+  __nv_bfloat16* as = reinterpret_cast<__nv_bfloat16*>(base);
+  __nv_bfloat16* bs = reinterpret_cast<__nv_bfloat16*>(base + plan.off_b);
+  int* ea = reinterpret_cast<int*>(base + plan.off_e);
+  int* fb = reinterpret_cast<int*>(base + plan.off_f);
+  const int64_t cap = (int64_t)num_sms * 16;
+  split_row_exponents<<<grid_for((plan.n_e + 255) / 256, cap), 256, 0, stream>>>(d_descs, n, plan.n_e, ea);
+  split_a<<<grid_for(plan.sa_work, cap), 256, 0, stream>>>(d_descs, n, plan.sa_work, plan.slices, ea, as);
+  split_b<<<grid_for(plan.n_f, cap), 256, 0, stream>>>(d_descs, n, plan.n_f, plan.slices, fb, bs);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  CUtensorMap tA, tB;
+  if (!encode_slices(&tA, as, plan.rows_a, kBM) || !encode_slices(&tB, bs, plan.rows_b, kBN))
+    return cudaErrorInvalidValue;
+  GemmParams gp;
+  gp.desc = d_descs;
+  gp.ea = ea;
+  gp.fb = fb;
+  gp.err = d_err;
+  gp.nd = n;
+  gp.slices = plan.slices;
+  gp.tiles = plan.tiles;
+  static bool opted_in[64] = {};
+  static std::mutex mu;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev < 0 || dev >= 64 || !opted_in[dev]) {
+      e = cudaFuncSetAttribute(split_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem);
+      if (e != cudaSuccess) return e;
+      if (dev >= 0 && dev < 64) opted_in[dev] = true;
+    }
+  }
+  split_gemm_kernel<<<grid_for(plan.tiles, num_sms), kGemmThreads, kGemmSmem, stream>>>(tA, tB, gp);
+  e = cudaGetLastError();
+  if (e == cudaSuccess && launches) *launches += 4;
+  return e;
+}
+
+}  // namespace fmm

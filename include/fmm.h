@@ -56,17 +56,32 @@ typedef enum fmm_schedule {
   FMM_SCHEDULE_HYBRID = 3
 } fmm_schedule;
 
+/* Precision of the leaf products (no counterpart in the reference, which
+ * multiplies in the Scalar type of its Matrix).  The operand formations and
+ * the M -> C combinations are FP64 in both.
+ *   FP64        FP64 tensor-core GEMM (DMMA).
+ *   SPLIT_BF16  every leaf operand row (A) / column (B) is scaled by a power
+ *               of two and split into `split_slices` BF16 digit slices of 8
+ *               bits; the S(S+1)/2 leading slice products run on the BF16
+ *               tensor cores (tcgen05) with exact FP32 accumulation over
+ *               k-chunks of 128, recombined in FP64.  Error of one leaf
+ *               product: |C - AB|_ij <~ 3 * 2^-8S * k * max|A_i.| * max|B_.j|;
+ *               S = 5 stays near 1e-14 relative for well-scaled operands. */
 typedef enum fmm_precision {
-  FMM_PRECISION_FP64 = 0,      /* leaf products in FP64 (DMMA) */
-  FMM_PRECISION_SPLIT_BF16 = 1 /* leaf products on the BF16 tensor cores over split operands */
+  FMM_PRECISION_FP64 = 0,
+  FMM_PRECISION_SPLIT_BF16 = 1
 } fmm_precision;
+
+#define FMM_SPLIT_MIN_SLICES 2
+#define FMM_SPLIT_MAX_SLICES 6
+#define FMM_SPLIT_DEFAULT_SLICES 5
 
 typedef struct fmm_handle_s* fmm_handle;
 
 typedef struct fmm_options {
   fmm_schedule schedule;    /* default FMM_SCHEDULE_AUTO */
   fmm_precision precision;  /* default FMM_PRECISION_FP64 */
-  int split_slices;         /* BF16 slices per operand for SPLIT_BF16 (0 = default) */
+  int split_slices;         /* BF16 slices per operand for SPLIT_BF16, 2..6 (0 = default 5) */
   int dfs_levels;           /* HYBRID only: depth-first levels; -1 = choose */
   size_t workspace_limit;   /* bytes; 0 = the handle's limit */
 } fmm_options;
@@ -124,6 +139,13 @@ fmm_status fmm_workspace_query(fmm_handle h, int alg, int64_t m, int64_t k, int6
 fmm_status fmm_dgemm(fmm_handle h, const double* A, int64_t lda, const double* B, int64_t ldb, double* C,
                      int64_t ldc, int64_t m, int64_t k, int64_t n, double alpha, double beta);
 
+/* Classical product C := alpha * A * B + beta * C computed split-BF16 with
+ * `slices` slices (0 = default) on the BF16 tensor cores (no counterpart in
+ * the reference).  Device pointers; queued on the handle's stream. */
+fmm_status fmm_dgemm_split_bf16(fmm_handle h, const double* A, int64_t lda, const double* B, int64_t ldb,
+                                double* C, int64_t ldc, int64_t m, int64_t k, int64_t n, double alpha, double beta,
+                                int slices);
+
 /* Same with HOST matrices: A, B (and C when beta != 0) are copied in, the
  * product runs on the engine's GEMM, C is copied back; returns when C is on
  * the host.  MatMul(A, B, C, beta) of linalg/linalg.hpp:261-269 over host
@@ -142,8 +164,17 @@ fmm_status fmm_fill_uniform(fmm_handle h, double* out, int64_t rows, int64_t col
 fmm_status fmm_max_relative_diff(fmm_handle h, const double* a, int64_t lda, const double* b, int64_t ldb,
                                  int64_t m, int64_t n, double* max_rel, double* max_abs);
 
-/* Waits for all work queued on the handle's stream. */
+/* Waits for all work queued on the handle's stream.  FMM_ERR_TIMEOUT if a
+ * tensor-core kernel of a split-BF16 product gave up one of its bounded
+ * waits since the last check (its results are then not valid). */
 fmm_status fmm_synchronize(fmm_handle h);
+
+/* Diagnostic of the bounded device waits (no counterpart in the reference):
+ * launches one kernel whose mbarrier wait is never satisfied and must give
+ * up after limit_ms; *code receives the error code it recorded (nonzero
+ * when the timeout path works).  The handle's error word is cleared and the
+ * context stays usable. */
+fmm_status fmm_selftest_wait_timeout(fmm_handle h, double limit_ms, int* code);
 
 /* Number of kernels the handle has launched since it was created. */
 int64_t fmm_kernel_launch_count(fmm_handle h);
@@ -188,6 +219,8 @@ typedef struct fmm_batch_item {
   int64_t ldc;
   int64_t m, k, n;
   double x, alpha, beta; /* as in fmm_fast_matmul */
+  int precision;         /* fmm_precision of the item's leaf products (0 = FP64) */
+  int split_slices;      /* SPLIT_BF16 slices, 2..6 (0 = default) */
 } fmm_batch_item;
 
 /* Independent products in one program: the operand formations of all items
@@ -262,6 +295,7 @@ typedef struct fmm_request {
   int64_t ldc;
   int64_t m, k, n;
   double x, alpha, beta;
+  int split_slices; /* SPLIT_BF16 slices, 2..6 (0 = default) */
 } fmm_request;
 
 typedef struct fmm_request_info {

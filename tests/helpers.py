@@ -37,7 +37,7 @@ def decode_matrix(s, m, n):
 
 def emulator():
     """The planner interpreter (tests/native/plan_emulator.cpp), built on demand."""
-    srcs = [EMU_SRC, os.path.join(CSRC, "plan.cpp")]
+    srcs = [EMU_SRC, os.path.join(CSRC, "plan.cpp"), os.path.join(CSRC, "split_plan.cpp")]
     deps = srcs + [os.path.join(CSRC, f) for f in ("plan.h", "fmm_internal.h")] + \
         [os.path.join(CSRC, "generated", f) for f in os.listdir(os.path.join(CSRC, "generated"))]
     if not os.path.exists(EMU_LIB) or os.path.getmtime(EMU_LIB) < max(os.path.getmtime(d) for d in deps):
@@ -59,6 +59,14 @@ def emulator():
     LP = ctypes.POINTER(i64)
     L.emu_fast_matmul_batch.argtypes = [I, IP, IP, LP, P, LP, P, LP, P, LP, D, D, D, LP]
     L.emu_fast_matmul_batch.restype = I
+    L.emu_fast_matmul_split.argtypes = [I, P, i64, P, i64, P, i64, I, I, I, I, D, D, D, I, I, ctypes.POINTER(i64)]
+    L.emu_fast_matmul_split.restype = I
+    L.emu_workspace_bytes_split.argtypes = [I, i64, i64, i64, I, I, I]
+    L.emu_workspace_bytes_split.restype = ctypes.c_size_t
+    L.emu_split_gemm.argtypes = [I, I, I, P, i64, P, i64, P, i64, D, D, I]
+    L.emu_split_gemm.restype = None
+    L.emu_fast_matmul_batch_split.argtypes = [I, IP, IP, LP, P, LP, P, LP, P, LP, D, D, D, IP, LP]
+    L.emu_fast_matmul_batch_split.restype = I
     return L
 
 

@@ -10,7 +10,13 @@
 // matches the CPU oracle's.  The result must equal the oracle bit for bit,
 // which checks the planner's views, multipliers, workspace layout,
 // schedules and peeling on machines without a GPU.
+//
+// Split-BF16 leaf products are executed by a model of the device arithmetic
+// (power-of-two scaling, 8-bit digit slices, exact integer sums per
+// diagonal and 128-deep k-chunk, FP64 recombination in the device's order),
+// so the device result must equal the model's bit for bit.
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstdlib>
@@ -29,6 +35,9 @@ cudaError_t form_launch(int, const FormLaunch&, const CoefSlots&, bool, int, cud
   return cudaErrorNotSupported;
 }
 cudaError_t combine_launch(int, const CombineLaunch&, const CoefSlots&, bool, int, cudaStream_t) {
+  return cudaErrorNotSupported;
+}
+cudaError_t split_gemm_launch(const SplitDesc*, int, const SplitPlan&, void*, int*, int, cudaStream_t, int64_t*) {
   return cudaErrorNotSupported;
 }
 }  // namespace fmm
@@ -121,6 +130,86 @@ void run_gemm(const fmm::Op& op, const unsigned char* desc) {
   }
 }
 
+int exponent_above(double maxabs) {
+  if (!(maxabs > 0.0)) return 0;
+  int e;
+  std::frexp(maxabs, &e);
+  return e;
+}
+
+// Digits of x (|x| < 1): d_t = rint(256 r_{t-1}), r_t = 256 r_{t-1} - d_t.
+void digits(double x, int slices, double* out) {
+  for (int t = 0; t < slices; ++t) {
+    const double y = x * 256.0;
+    const double dg = std::rint(y);
+    x = y - dg;
+    out[t] = dg;
+  }
+}
+
+// One split-BF16 product C = alpha * A * B + beta * C, in the device's order.
+void split_product(const fmm::SplitDesc& d, int slices) {
+  const int m = d.m, n = d.n, k = d.k;
+  if (m <= 0 || n <= 0) return;
+  const int S = slices;
+  std::vector<int> ea((size_t)m), fb((size_t)n);
+  for (int i = 0; i < m; ++i) {
+    double mx = 0.0;
+    for (int p = 0; p < k; ++p) mx = std::fmax(mx, std::fabs(d.A[i + (int64_t)p * d.lda]));
+    ea[(size_t)i] = exponent_above(mx);
+  }
+  for (int j = 0; j < n; ++j) {
+    double mx = 0.0;
+    for (int p = 0; p < k; ++p) mx = std::fmax(mx, std::fabs(d.B[p + (int64_t)j * d.ldb]));
+    fb[(size_t)j] = exponent_above(mx);
+  }
+  // dA[(t * k + p) * m + i], dB[(t * k + p) * n + j]
+  std::vector<double> dA((size_t)S * k * m), dB((size_t)S * k * n);
+  double dg[8];
+  for (int p = 0; p < k; ++p) {
+    for (int i = 0; i < m; ++i) {
+      digits(std::ldexp(d.A[i + (int64_t)p * d.lda], -ea[(size_t)i]), S, dg);
+      for (int t = 0; t < S; ++t) dA[((size_t)t * k + p) * m + i] = dg[t];
+    }
+    for (int j = 0; j < n; ++j) {
+      digits(std::ldexp(d.B[p + (int64_t)j * d.ldb], -fb[(size_t)j]), S, dg);
+      for (int t = 0; t < S; ++t) dB[((size_t)t * k + p) * n + j] = dg[t];
+    }
+  }
+  std::vector<double> acc((size_t)m * n, 0.0), part((size_t)m * n);
+  const int chunks = std::max(1, (k + fmm::kSplitChunk - 1) / fmm::kSplitChunk);
+  for (int c = 0; c < chunks; ++c) {
+    const int p0 = c * fmm::kSplitChunk, p1 = std::min(k, p0 + fmm::kSplitChunk);
+    for (int D = 0; D < S; ++D) {
+      std::fill(part.begin(), part.end(), 0.0);
+      for (int t = 0; t <= D; ++t)
+        for (int p = p0; p < p1; ++p) {
+          const double* a = &dA[((size_t)t * k + p) * m];
+          const double* b = &dB[((size_t)(D - t) * k + p) * n];
+          for (int j = 0; j < n; ++j)
+            for (int i = 0; i < m; ++i) part[(size_t)j * m + i] += a[i] * b[j];  // exact integers
+        }
+      const double scale = std::ldexp(1.0, -8 * (D + 2));
+      for (size_t x = 0; x < part.size(); ++x) {
+        const float f = (float)part[x];  // the FP32 accumulator (exact)
+        acc[x] = std::fma((double)f, scale, acc[x]);
+      }
+    }
+  }
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < m; ++i) {
+      double* c = &d.C[i + (int64_t)j * d.ldc];
+      double v = d.alpha * std::ldexp(acc[(size_t)j * m + i], ea[(size_t)i] + fb[(size_t)j]);
+      if (d.beta != 0.0) v = v + d.beta * *c;
+      *c = v;
+    }
+}
+
+void run_split(const fmm::Op& op, const unsigned char* desc) {
+  const fmm::SplitDesc* g = reinterpret_cast<const fmm::SplitDesc*>(desc + op.desc_off);
+  for (int p = 0; p < op.n; ++p) split_product(g[p], op.split.slices);
+}
+
 void run_ops(const fmm::Program& prog) {
   for (const fmm::Op& op : prog.ops) {
     const double* cf = prog.coefs[(size_t)op.cf].v;
@@ -148,6 +237,9 @@ void run_ops(const fmm::Program& prog) {
       case fmm::OpKind::kGemm:
         run_gemm(op, prog.desc.data());
         break;
+      case fmm::OpKind::kSplitGemm:
+        run_split(op, prog.desc.data());
+        break;
     }
   }
 }
@@ -160,25 +252,50 @@ size_t emu_workspace_bytes(int alg, int64_t m, int64_t k, int64_t n, int steps, 
   return fmm::workspace_bytes(fmm_algorithms[alg], m, k, n, steps, dfs_levels);
 }
 
-// Runs FastMatmul through the planner + interpreter.  stats (may be NULL)
-// receives {#form, #gemm, #combine launches, leaf products, workspace bytes}.
-int emu_fast_matmul(int alg, double* A, int64_t lda, double* B, int64_t ldb, double* C, int64_t ldc, int m, int k,
-                    int n, int steps, double x, double alpha, double beta, int dfs_levels, int64_t* stats) {
+size_t emu_workspace_bytes_split(int alg, int64_t m, int64_t k, int64_t n, int steps, int dfs_levels, int slices) {
+  return fmm::workspace_bytes(fmm_algorithms[alg], m, k, n, steps, dfs_levels, slices);
+}
+
+// The split-BF16 model for one classical product.
+void emu_split_gemm(int m, int k, int n, const double* A, int64_t lda, const double* B, int64_t ldb, double* C,
+                    int64_t ldc, double alpha, double beta, int slices) {
+  fmm::SplitDesc d{};
+  d.A = A;
+  d.B = B;
+  d.C = C;
+  d.lda = lda;
+  d.ldb = ldb;
+  d.ldc = ldc;
+  d.m = m;
+  d.n = n;
+  d.k = k;
+  d.alpha = alpha;
+  d.beta = beta;
+  emu::split_product(d, slices);
+}
+
+// Runs FastMatmul through the planner + interpreter (split_slices > 0: leaf
+// products split-BF16).  stats (may be NULL) receives {#form, #gemm
+// (FP64 or split), #combine launches, leaf products, workspace bytes}.
+int emu_fast_matmul_split(int alg, double* A, int64_t lda, double* B, int64_t ldb, double* C, int64_t ldc, int m,
+                          int k, int n, int steps, double x, double alpha, double beta, int dfs_levels, int slices,
+                          int64_t* stats) {
   if (alg < 0 || alg >= FMM_NUM_ALGORITHMS) return -1;
-  const size_t bytes = emu_workspace_bytes(alg, m, k, n, steps, dfs_levels);
+  const size_t bytes = emu_workspace_bytes_split(alg, m, k, n, steps, dfs_levels, slices);
   std::vector<double> ws(bytes / sizeof(double) + 64, std::numeric_limits<double>::quiet_NaN());
   // 256-byte alignment like a device allocation
   double* base = ws.data();
   while (reinterpret_cast<uintptr_t>(base) % 256) ++base;
   fmm::Program prog;
   fmm::build_program(alg, m, k, n, steps, x, alpha, beta, dfs_levels, fmm::Operand{A, lda}, fmm::Operand{B, ldb},
-                     fmm::Operand{C, ldc}, base, &prog);
+                     fmm::Operand{C, ldc}, base, &prog, slices);
+  if (prog.workspace_bytes > bytes) return -2;  // the query must cover the program
   emu::run_ops(prog);
   if (stats) {
     int64_t nf = 0, ng = 0, nc = 0;
     for (const fmm::Op& op : prog.ops) {
       nf += op.kind == fmm::OpKind::kForm;
-      ng += op.kind == fmm::OpKind::kGemm;
+      ng += op.kind == fmm::OpKind::kGemm || op.kind == fmm::OpKind::kSplitGemm;
       nc += op.kind == fmm::OpKind::kCombine;
     }
     stats[0] = nf;
@@ -190,12 +307,18 @@ int emu_fast_matmul(int alg, double* A, int64_t lda, double* B, int64_t ldb, dou
   return 0;
 }
 
+int emu_fast_matmul(int alg, double* A, int64_t lda, double* B, int64_t ldb, double* C, int64_t ldc, int m, int k,
+                    int n, int steps, double x, double alpha, double beta, int dfs_levels, int64_t* stats) {
+  return emu_fast_matmul_split(alg, A, lda, B, ldb, C, ldc, m, k, n, steps, x, alpha, beta, dfs_levels, 0, stats);
+}
+
 // A batch through the planner + interpreter: item i is
 // (algs[i], steps[i], dims[3i..3i+2]) on A_i, B_i, C_i packed column-major
 // (lda = m, ...) at the given offsets into A, B, C.
-int emu_fast_matmul_batch(int count, const int* algs, const int* steps, const int64_t* dims, double* A,
-                          const int64_t* a_off, double* B, const int64_t* b_off, double* C, const int64_t* c_off,
-                          double x, double alpha, double beta, int64_t* stats) {
+int emu_fast_matmul_batch_split(int count, const int* algs, const int* steps, const int64_t* dims, double* A,
+                                const int64_t* a_off, double* B, const int64_t* b_off, double* C,
+                                const int64_t* c_off, double x, double alpha, double beta, const int* slices,
+                                int64_t* stats) {
   std::vector<fmm::BatchItem> items((size_t)count);
   for (int i = 0; i < count; ++i) {
     fmm::BatchItem& it = items[(size_t)i];
@@ -212,6 +335,7 @@ int emu_fast_matmul_batch(int count, const int* algs, const int* steps, const in
     it.beta = beta;
     it.classical = it.alg < 0;
     if (it.classical) it.alg = 0;
+    it.split_slices = slices ? slices[i] : 0;
   }
   const size_t bytes = fmm::batch_workspace_bytes(items.data(), count);
   std::vector<double> ws(bytes / sizeof(double) + 64, std::numeric_limits<double>::quiet_NaN());
@@ -219,12 +343,13 @@ int emu_fast_matmul_batch(int count, const int* algs, const int* steps, const in
   while (reinterpret_cast<uintptr_t>(base) % 256) ++base;
   fmm::Program prog;
   fmm::build_batch_program(items.data(), count, base, &prog);
+  if (prog.workspace_bytes > bytes) return -2;
   emu::run_ops(prog);
   if (stats) {
     int64_t nf = 0, ng = 0, nc = 0;
     for (const fmm::Op& op : prog.ops) {
       nf += op.kind == fmm::OpKind::kForm;
-      ng += op.kind == fmm::OpKind::kGemm && !op.peel;
+      ng += (op.kind == fmm::OpKind::kGemm && !op.peel) || op.kind == fmm::OpKind::kSplitGemm;
       nc += op.kind == fmm::OpKind::kCombine;
     }
     stats[0] = nf;
@@ -234,6 +359,13 @@ int emu_fast_matmul_batch(int count, const int* algs, const int* steps, const in
     stats[4] = (int64_t)prog.workspace_bytes;
   }
   return 0;
+}
+
+int emu_fast_matmul_batch(int count, const int* algs, const int* steps, const int64_t* dims, double* A,
+                          const int64_t* a_off, double* B, const int64_t* b_off, double* C, const int64_t* c_off,
+                          double x, double alpha, double beta, int64_t* stats) {
+  return emu_fast_matmul_batch_split(count, algs, steps, dims, A, a_off, B, b_off, C, c_off, x, alpha, beta, nullptr,
+                                     stats);
 }
 
 }  // extern "C"
