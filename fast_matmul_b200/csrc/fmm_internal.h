@@ -43,7 +43,7 @@ constexpr int kSplitMaxSlices = 6;
 constexpr int kSplitDefaultSlices = 5;
 constexpr int kSplitTile = 128;   // output tile rows and columns
 constexpr int kSplitKBlock = 64;  // k-depth of one TMA box (128 bytes of BF16)
-constexpr int kSplitChunk = 128;  // k-depth accumulated exactly in FP32
+constexpr int kSplitChunk = 128;  // k-depth accumulated exactly in FP32 (two k-blocks)
 
 struct SplitDesc {
   const double* A;

@@ -20,8 +20,8 @@
 //
 // Product kernel: persistent CTAs over the 128 x 128 output tiles of every
 // problem.  Warp 0 issues TMA loads of (A_t, B_u) 64-deep k-blocks into a
-// 6-stage ring, warp 1 issues tcgen05.mma (M128 N128 K16) into one of two
-// TMEM accumulators of 128 FP32 columns, warps 2-9 (two warpgroups of 64
+// 6-stage ring, warp 1 issues tcgen05.mma (M128 N128 K16) into one of four TMEM
+// accumulators of 128 FP32 columns, warps 2-9 (two warpgroups of 64
 // columns) drain each finished accumulator into FP64 registers.  Every
 // mbarrier wait is bounded; on a timeout the kernel records a code in *err,
 // lets its copies and MMAs in flight finish, frees its TMEM and returns.
@@ -42,6 +42,7 @@ namespace {
 using namespace sm100;
 
 constexpr int kBM = kSplitTile, kBN = kSplitTile, kBK = kSplitKBlock, kStages = 6;
+constexpr int kAccBufs = 4;  // TMEM accumulators of 128 FP32 columns
 constexpr int kTileABytes = kBM * kBK * 2;  // 16 KB
 constexpr int kTileBBytes = kBN * kBK * 2;  // 16 KB
 constexpr int kStageBytes = kTileABytes + kTileBBytes;
@@ -214,7 +215,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
                       const GemmParams g) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  __shared__ __align__(8) uint64_t full[kStages], empty[kStages], acc_full[2], acc_empty[2], mma_done;
+  __shared__ __align__(8) uint64_t full[kStages], empty[kStages], acc_full[kAccBufs], acc_empty[kAccBufs], mma_done;
   __shared__ uint32_t tmem_slot;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int S = g.slices;
@@ -223,14 +224,14 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    for (int b = 0; b < 2; ++b) {
+    for (int b = 0; b < kAccBufs; ++b) {
       mbar_init(&acc_full[b], 1);
       mbar_init(&acc_empty[b], 8);
     }
     mbar_init(&mma_done, 1);
     fence_barrier_init();
   }
-  if (warp == 1) tmem_alloc(&tmem_slot, 256);
+  if (warp == 1) tmem_alloc(&tmem_slot, kAccBufs * kBN);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -281,8 +282,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         const int chunks = g.desc[tc.q].kblocks / kChunkBlocks;
         for (int c = 0; c < chunks && ok; ++c)
           for (int D = 0; D < S && ok; ++D, ++ai) {
-            const int buf = ai & 1;
-            if (ai >= 2 && !mbar_wait(&acc_empty[buf], ((ai >> 1) & 1) ^ 1, g.err, 2)) {
+            const int buf = ai % kAccBufs;
+            if (ai >= kAccBufs && !mbar_wait(&acc_empty[buf], ((ai / kAccBufs) - 1) & 1, g.err, 2)) {
               ok = false;
               break;
             }
@@ -329,8 +330,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
       for (int j = 0; j < 64; ++j) acc[j] = 0.0;
       for (int c = 0; c < chunks && ok; ++c)
         for (int D = 0; D < S; ++D, ++ai) {
-          const int buf = ai & 1;
-          if (!mbar_wait(&acc_full[buf], (ai >> 1) & 1, g.err, 4)) {
+          const int buf = ai % kAccBufs;
+          if (!mbar_wait(&acc_full[buf], (ai / kAccBufs) & 1, g.err, 4)) {
             ok = false;
             break;
           }
@@ -375,7 +376,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  if (warp == 1) tmem_dealloc(tmem, 256);
+  if (warp == 1) tmem_dealloc(tmem, kAccBufs * kBN);
 }
 
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
