@@ -100,13 +100,32 @@ __global__ void __launch_bounds__(256) split_row_exponents(const SplitDesc* __re
   }
 }
 
+// Digits of 8 scaled values as 8 BF16 per slice, one 16-byte store each.
+__device__ __forceinline__ void store_digits(double (&x)[8], int slices, __nv_bfloat16* dst, int64_t slice_stride) {
+  for (int t = 0; t < slices; ++t) {
+    __align__(16) __nv_bfloat16 v[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const double y = x[c] * 256.0;
+      const double dg = rint(y);
+      x[c] = y - dg;
+      v[c] = __double2bfloat16(dg);
+    }
+    *reinterpret_cast<uint4*>(dst + t * slice_stride) = *reinterpret_cast<const uint4*>(v);
+  }
+}
+
 // A slices: one work tile = 32 rows x one 64-deep k-block, read column-major
-// (coalesced along rows), written as 128-byte k-block rows for every slice.
+// (coalesced along rows) into shared memory, written as 128-byte k-block rows
+// for every slice (8 threads per row, 16 bytes each).  The tile's row index
+// is XOR-swizzled by k so that both the column-wise fill and the row-wise
+// read-out touch every bank pair at most twice per warp.
 __global__ void __launch_bounds__(256) split_a(const SplitDesc* __restrict__ d, int nd, int64_t total, int slices,
                                                const int* __restrict__ ea, __nv_bfloat16* __restrict__ out) {
-  __shared__ double tile[64][33];
+  __shared__ double tile[64 * 32];
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
   const int row = threadIdx.x >> 3, kc = (threadIdx.x & 7) * 8;
+  auto at = [](int k, int r) { return k * 32 + (r ^ (((k >> 3) & 3) << 2)); };
   for (int64_t w = blockIdx.x; w < total; w += gridDim.x) {
     const int q = find_desc(d, nd, w, [](const SplitDesc& s) { return s.sa_begin; });
     const SplitDesc& s = d[q];
@@ -117,31 +136,23 @@ __global__ void __launch_bounds__(256) split_a(const SplitDesc* __restrict__ d, 
     __syncthreads();  // previous tile's readers are done
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
-      const int64_t p = p0 + ty + 8 * r, i = i0 + tx;
-      tile[ty + 8 * r][tx] = (i < s.m && p < s.k) ? s.A[i + p * s.lda] : 0.0;
+      const int k = ty + 8 * r;
+      const int64_t p = p0 + k, i = i0 + tx;
+      tile[at(k, tx)] = (i < s.m && p < s.k) ? s.A[i + p * s.lda] : 0.0;
     }
     __syncthreads();
     const int e = ea[s.e_off + i0 + row];
     double x[8];
 #pragma unroll
-    for (int c = 0; c < 8; ++c) x[c] = ldexp(tile[kc + c][row], -e);
-    for (int t = 0; t < slices; ++t) {
-      __align__(16) __nv_bfloat16 v[8];
-#pragma unroll
-      for (int c = 0; c < 8; ++c) {
-        const double y = x[c] * 256.0;
-        const double dg = rint(y);
-        x[c] = y - dg;
-        v[c] = __double2bfloat16(dg);
-      }
-      const int64_t orow = s.a_row + ((int64_t)t * s.kblocks + kb) * mp + i0 + row;
-      *reinterpret_cast<uint4*>(out + orow * kBK + kc) = *reinterpret_cast<const uint4*>(v);
-    }
+    for (int c = 0; c < 8; ++c) x[c] = ldexp(tile[at(kc + c, row)], -e);
+    const int64_t orow = s.a_row + kb * mp + i0 + row;
+    store_digits(x, slices, out + orow * kBK + kc, (int64_t)s.kblocks * mp * kBK);
   }
 }
 
-// B: one block per padded column: the column maximum, then the slices (B's
-// columns are contiguous in k, so they are written as they are read).
+// B: one block per padded column: the column maximum, then the slices, 8
+// consecutive k per thread (B's columns are contiguous in k, so they are
+// written as they are read).
 __global__ void __launch_bounds__(256) split_b(const SplitDesc* __restrict__ d, int nd, int64_t total, int slices,
                                                int* __restrict__ fb, __nv_bfloat16* __restrict__ out) {
   __shared__ double red[8];
@@ -153,9 +164,29 @@ __global__ void __launch_bounds__(256) split_b(const SplitDesc* __restrict__ d, 
     const int64_t np = (int64_t)s.tiles_n * kBN;
     const double* b = s.B + j * s.ldb;
     const bool live = j < s.n;
+    const bool vec = (reinterpret_cast<uintptr_t>(b) & 15) == 0;
+    const int k = s.k, kp = s.kblocks * kBK;
+    auto load8 = [&](int p0, double (&v)[8]) {
+      if (vec && p0 + 8 <= k) {
+#pragma unroll
+        for (int c = 0; c < 8; c += 2) {
+          const double2 t2 = *reinterpret_cast<const double2*>(b + p0 + c);
+          v[c] = t2.x;
+          v[c + 1] = t2.y;
+        }
+      } else {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) v[c] = p0 + c < k ? b[p0 + c] : 0.0;
+      }
+    };
     double mx = 0.0;
     if (live)
-      for (int p = threadIdx.x; p < s.k; p += blockDim.x) mx = fmax(mx, fabs(b[p]));
+      for (int p0 = threadIdx.x * 8; p0 < k; p0 += blockDim.x * 8) {
+        double v[8];
+        load8(p0, v);
+#pragma unroll
+        for (int c = 0; c < 8; ++c) mx = fmax(mx, fabs(v[c]));
+      }
     for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
     __syncthreads();
@@ -167,17 +198,18 @@ __global__ void __launch_bounds__(256) split_b(const SplitDesc* __restrict__ d, 
     }
     __syncthreads();
     const int f = e_sh;
-    const int kp = s.kblocks * kBK;
-    for (int p = threadIdx.x; p < kp; p += blockDim.x) {
-      double v = (live && p < s.k) ? ldexp(b[p], -f) : 0.0;
-      const int64_t kb = p / kBK, pk = p % kBK;
-      for (int t = 0; t < slices; ++t) {
-        const double y = v * 256.0;
-        const double dg = rint(y);
-        v = y - dg;
-        const int64_t orow = s.b_row + ((int64_t)t * s.kblocks + kb) * np + j;
-        out[orow * kBK + pk] = __double2bfloat16(dg);
+    for (int p0 = threadIdx.x * 8; p0 < kp; p0 += blockDim.x * 8) {
+      double v[8];
+      if (live) {
+        load8(p0, v);
+      } else {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) v[c] = 0.0;
       }
+#pragma unroll
+      for (int c = 0; c < 8; ++c) v[c] = ldexp(v[c], -f);
+      const int64_t orow = s.b_row + (int64_t)(p0 / kBK) * np + j;
+      store_digits(v, slices, out + orow * kBK + (p0 % kBK), (int64_t)s.kblocks * np * kBK);
     }
     __syncthreads();  // e_sh and red are reused by the next column
   }
