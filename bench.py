@@ -53,9 +53,14 @@ def parse_args(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=4096, help="edge of the CPU baseline sample")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU work budget of the baseline sample")
-    ap.add_argument("--workload", default="product", choices=["product", "batch", "serve"],
+    ap.add_argument("--workload", default="product", choices=["product", "batch", "serve", "precision"],
                     help="product: one large FastMatmul (the headline); batch: 4096 independent products "
-                         "with log-uniform dimensions in [64, 1024] in one CUDA-graph plan")
+                         "with log-uniform dimensions in [64, 1024] in one CUDA-graph plan; serve: a Poisson "
+                         "request stream through the continuous-batching server; precision: split-BF16 leaf "
+                         "products (Strassen, Bini) against the FP64 oracle")
+    ap.add_argument("--precision-sizes", default="8192,16384",
+                    help="square sizes of the precision workload")
+    ap.add_argument("--batch-precision", default="fp64", choices=["fp64", "split_bf16"])
     ap.add_argument("--batch-count", type=int, default=4096)
     ap.add_argument("--serve-requests", type=int, default=300)
     ap.add_argument("--serve-slots", type=int, default=6)
@@ -499,7 +504,8 @@ def run_batch_workload(a):
     for i, (m, k, n) in enumerate(dims):
         probs.append({"A": fmm.random_matrix(int(m), int(k), 7000 + i, 1, -1.0, 1.0, handle=h),
                       "B": fmm.random_matrix(int(k), int(n), 7000 + i, 2, -1.0, 1.0, handle=h),
-                      "C": fmm.colmajor_empty(int(m), int(n)), "alg": fmm.AUTO})
+                      "C": fmm.colmajor_empty(int(m), int(n)), "alg": fmm.AUTO,
+                      "precision": a.batch_precision, "split_slices": 6})
     flops = float(sum(2.0 * m * n * k for m, k, n in dims))
     t0 = time.perf_counter()
     fmm.autotune([tuple(int(v) for v in d) for d in dims], max_steps=1, handle=h)
@@ -531,18 +537,23 @@ def run_batch_workload(a):
         for p, (m, k, n) in zip(probs, dims):
             alg, steps = fmm.autotune_choice(int(m), int(k), int(n), handle=h)
             if alg == fmm.CLASSICAL:
-                fmm.matmul(p["A"], p["B"], p["C"], handle=h)
+                if a.batch_precision == "split_bf16":
+                    fmm.matmul_split_bf16(p["A"], p["B"], p["C"], slices=6, handle=h)
+                else:
+                    fmm.matmul(p["A"], p["B"], p["C"], handle=h)
             else:
-                fmm.fast_matmul(alg, p["A"], p["B"], p["C"], steps, handle=h)
+                fmm.fast_matmul(alg, p["A"], p["B"], p["C"], steps, precision=a.batch_precision, split_slices=6,
+                                handle=h)
 
     one_at_a_time()
     ms_single = timed(one_at_a_time, 1)
     out = {
         "metric": METRIC, "value": flops / (ms * 1e-3) / 1e12, "unit": "TFLOP/s", "n_gpus": 1, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "batch of %d independent FP64 products, M,K,N log-uniform in [64,1024], "
-                               "uniform[-1,1), autotuned per shape bucket, one CUDA-graph plan" % a.batch_count,
+        "dtype": "f64" if a.batch_precision == "fp64" else "bf16 slices (FP64 in and out)", "data": "synthetic",
+        "config": {"workload": "batch of %d independent %s products, M,K,N log-uniform in [64,1024], "
+                               "uniform[-1,1), autotuned per shape bucket, one CUDA-graph plan"
+                               % (a.batch_count, "FP64" if a.batch_precision == "fp64" else "split-BF16 (6 slices)"),
                    "total_gflop": flops / 1e9, "autotune_seconds": tune_s,
                    "choices": {("classical" if k[0] == fmm.CLASSICAL else "%s/%d" % (fmm.algorithm_names()[k[0]], k[1])): v
                                for k, v in choices.items()}},
@@ -556,8 +567,9 @@ def run_batch_workload(a):
 
 
 def run_serve_workload(a):
-    """Poisson stream of FP64 products, M, K, N each log-uniform in [256, 8192],
-    uniform [-1, 1) entries, operands resident in device memory, offered at
+    """Poisson stream of products (70% FP64, 30% split-BF16 with 6 slices),
+    M, K, N each log-uniform in [256, 8192], uniform [-1, 1) entries, operands
+    resident in device memory, offered at
     twice the rate that one-at-a-time launches sustain; the server admits
     requests by workspace footprint into concurrent batches (--serve-slots).  Reports
     throughput, p50/p99 latency (submission to completion) and the
@@ -583,13 +595,19 @@ def run_serve_workload(a):
                      fmm.colmajor_empty(int(m), int(n))))
     flops = float(sum(2.0 * m * n * k for m, k, n in dims))
 
+    split_slices = 6  # the 1e-12 target of the split-BF16 share
+
     def alone(i):
         A, B, C = reqs[i]
         alg, steps = fmm.autotune_choice(*(int(v) for v in dims[i]), handle=h)
         if alg == fmm.CLASSICAL:
-            fmm.matmul(A, B, C, handle=h)
+            if wants_split[i]:
+                fmm.matmul_split_bf16(A, B, C, slices=split_slices, handle=h)
+            else:
+                fmm.matmul(A, B, C, handle=h)
         else:
-            fmm.fast_matmul(alg, A, B, C, steps, handle=h)
+            fmm.fast_matmul(alg, A, B, C, steps, precision="split_bf16" if wants_split[i] else "fp64",
+                            split_slices=split_slices, handle=h)
 
     for i in range(min(N, 8)):  # warm
         alone(i)
@@ -624,7 +642,8 @@ def run_serve_workload(a):
             if d > 0:
                 time.sleep(d)
             A, B, C = reqs[i]
-            tickets[i] = srv.submit(A, B, C, fmm.AUTO)
+            tickets[i] = srv.submit(A, B, C, fmm.AUTO, precision="split_bf16" if wants_split[i] else "fp64",
+                                    split_slices=split_slices)
 
     th = threading.Thread(target=client)
     th.start()
@@ -643,20 +662,178 @@ def run_serve_workload(a):
         "warmup": 8, "ms_per_step": t_serve * 1e3 / N, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": "serving: %d Poisson requests, M,K,N log-uniform in [256,8192], uniform[-1,1), "
-                               "offered at 2x the one-at-a-time rate (%.1f req/s), FP64 (the split-BF16 share "
-                               "of %.0f%% is served in FP64)" % (N, rate, 100 * split_share),
-                   "total_tflop": flops / 1e12, "requests_marked_split_bf16": int(wants_split.sum())},
+                               "offered at 2x the one-at-a-time rate (%.1f req/s), %.0f%% FP64 / %.0f%% split-BF16 "
+                               "(%d slices)" % (N, rate, 100 - 100 * split_share, 100 * split_share, split_slices),
+                   "total_tflop": flops / 1e12, "requests_split_bf16": int(wants_split.sum())},
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                        "max": float(lat.max())},
         "one_at_a_time": {"value": flops / t_single / 1e12, "seconds": t_single,
                           "throughput_ratio_of_server": t_single / t_serve,
-                          "what": "same algorithm choice per request, one launch set + synchronize each"},
+                          "what": "same algorithm and precision per request, one launch set + synchronize each"},
         "one_at_a_time_plain": {"value": flops / t_plain / 1e12, "seconds": t_plain,
                                 "throughput_ratio_of_server": t_plain / t_serve,
                                 "what": "classical FP64 GEMM per request, launch + synchronize each"},
         "server": stats,
         "results_identical_to_alone": bool(same),
         "gpu_launches": stats["launches"],
+    }
+    print(json.dumps(out))
+    return 0
+
+
+def scaled_normal(m, n, seed, per, device):
+    """Column-major m x n FP64 matrix: N(0, 1) entries times 2^e, e an integer
+    uniform in [-16, 16] drawn per row (per="row") or per column."""
+    import torch
+
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    X = torch.randn((n, m), generator=g, device=device, dtype=torch.float64).t()
+    cnt = m if per == "row" else n
+    e = torch.randint(-16, 17, (cnt,), generator=g, device=device).to(torch.float64)
+    s = torch.exp2(e)
+    if per == "row":
+        X.mul_(s[:, None])
+    else:
+        X.mul_(s[None, :])
+    return X
+
+
+def precision_errors(fmm, A, B, C, ref, absAB, h):
+    """Errors of C against the FP64 classical product ref: elementwise
+    max |C - D| / |D| (the reference's MaxRelativeDiff), normwise
+    max |C - D| / max |D|, and max |C - D| / (|A| |B|)."""
+    import torch
+
+    rel, absd = fmm.max_relative_diff(ref, C, handle=h)
+    norm = absd / float(ref.abs().max())
+    d = (C - ref).abs_().div_(absAB.clamp_min(1e-300))
+    scaled = float(d.max())
+    del d
+    return {"max_rel_elementwise": rel, "max_rel_normwise": norm, "max_abs_over_absAB": scaled}
+
+
+def run_precision_workload(a):
+    """Split-BF16 leaf products against the FP64 oracle.  For each size and
+    input distribution (uniform [0, 1); N(0, 1) with per-row (A) / per-column
+    (B) scales 2^U{-16..16}): Strassen with 2 and 3 steps and bini322 with
+    lambda swept over 2^-10 .. 2^-26 (1 step), leaf products split into 3..6
+    BF16 slices, each timed (CUDA events, inputs resident) and checked
+    against the engine's FP64 classical product of the same inputs.  The
+    headline is the fastest Strassen configuration at 16384^3 whose
+    elementwise error on uniform inputs stays within 1e-12."""
+    import numpy as np
+    import torch
+
+    import fast_matmul_b200 as fmm
+
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    h = fmm.default_handle(0)
+    sizes = [int(x) for x in a.precision_sizes.split(",") if x]
+
+    def timed(fn, reps=2):
+        fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    rows = []
+    classical = {}
+    head = None
+    for n in sizes:
+        flops = 2.0 * n ** 3
+        for dist in ("uniform[0,1)", "N(0,1)*2^U(-16,16)"):
+            if dist.startswith("uniform"):
+                A = fmm.random_matrix(n, n, 31, 1, handle=h)
+                B = fmm.random_matrix(n, n, 31, 2, handle=h)
+            else:
+                A = scaled_normal(n, n, 41, "row", dev)
+                B = scaled_normal(n, n, 42, "col", dev)
+            ref = fmm.colmajor_empty(n, n, dev)
+            ms = timed(lambda: fmm.matmul(A, B, ref, handle=h))
+            if dist.startswith("uniform"):
+                classical[n] = {"engine_dgemm_tflops": flops / (ms * 1e-3) / 1e12}
+                Ct = torch.matmul(A, B)
+                msb = timed(lambda: torch.matmul(A, B, out=Ct))
+                classical[n]["cublas_dgemm_tflops"] = flops / (msb * 1e-3) / 1e12
+                del Ct
+            absAB = fmm.colmajor_empty(n, n, dev)
+            fmm.matmul(A.abs(), B.abs(), absAB, handle=h)
+            C = fmm.colmajor_empty(n, n, dev)
+            runs = [("strassen", s, 1e-8, sl) for s in (2, 3) for sl in (4, 5, 6)]
+            runs += [("fp64 strassen", s, 1e-8, 0) for s in (2,)]
+            if n == sizes[0]:
+                runs += [("split classical", 0, 0.0, sl) for sl in (3, 4, 5, 6)]
+                runs += [("bini322_10_52_approx", 1, 2.0 ** -lg, sl) for lg in (10, 14, 18, 22, 26) for sl in (0, 6)]
+            for alg, steps, x, sl in runs:
+                if alg == "split classical":
+                    fn = lambda: fmm.matmul_split_bf16(A, B, C, slices=sl, handle=h)  # noqa: E731
+                    name = "classical"
+                elif alg == "fp64 strassen":
+                    fn = lambda: fmm.fast_matmul("strassen", A, B, C, steps, handle=h)  # noqa: E731
+                    name = "strassen"
+                else:
+                    prec = "split_bf16" if sl else "fp64"
+                    fn = lambda: fmm.fast_matmul(alg, A, B, C, steps, x, precision=prec, split_slices=sl,  # noqa: E731
+                                                 handle=h)
+                    name = alg
+                ms = timed(fn)
+                h.profile(True)
+                h.profile_reset()
+                fn()
+                prof = h.profile_read()
+                h.profile(False)
+                fmm.synchronize(h)
+                err = precision_errors(fmm, A, B, C, ref, absAB, h)
+                leaf_ms = prof["gemm_ms"] - prof["split_ms"]
+                row = {"n": n, "inputs": dist, "algorithm": name, "num_steps": steps,
+                       "lambda": x if "approx" in name else None,
+                       "precision": "split_bf16 x%d" % sl if sl else "fp64", "ms": ms,
+                       "effective_tflops": flops / (ms * 1e-3) / 1e12, "error": err,
+                       "split_kernel_ms": prof["split_ms"] if sl else None,
+                       "slice_product_bf16_tflops": (prof["split_bf16_flops"] / (leaf_ms * 1e-3) / 1e12
+                                                     if sl and leaf_ms > 0 else None)}
+                rows.append(row)
+                print(json.dumps({"precision_row": row}), file=sys.stderr, flush=True)
+                if (n == max(sizes) and dist.startswith("uniform") and name == "strassen" and sl
+                        and err["max_rel_elementwise"] <= 1e-12
+                        and (head is None or row["effective_tflops"] > head["effective_tflops"])):
+                    head = row
+            del A, B, C, ref, absAB
+            torch.cuda.empty_cache()
+
+    peaks, peak_src = measured_peaks()
+    n_head = max(sizes)
+    base = classical[n_head]
+    value = head["effective_tflops"] if head else None
+    roofline = None
+    if head and head["slice_product_bf16_tflops"]:
+        pk = peaks.get("bf16_tflops", 1590.0)
+        roofline = {"kernel": "split_gemm_kernel (tcgen05 BF16 slice products)", "bound": "tensor",
+                    "achieved": head["slice_product_bf16_tflops"], "peak": pk, "unit": "TFLOP/s",
+                    "frac": head["slice_product_bf16_tflops"] / pk,
+                    "peak_source": "bf16_tflops of MEASURED_PEAKS.json (%s, cuBLAS bf16 8192^3 burst)" % peak_src,
+                    "traffic": None}
+    out = {
+        "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": 1, "steps": 2, "warmup": 1,
+        "ms_per_step": head["ms"] if head else None, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "bf16 slices (FP64 in and out)", "data": "synthetic",
+        "config": {"workload": "precision: split-BF16 leaf products; headline = fastest Strassen at %d^3 "
+                               "within 1e-12 (elementwise, uniform inputs) of the FP64 classical product"
+                               % n_head,
+                   "headline": head, "l2": "inputs larger than L2"},
+        "classical": {str(k): v for k, v in classical.items()},
+        "speedup_vs_engine_classical": value / base["engine_dgemm_tflops"] if value else None,
+        "speedup_vs_cublas": value / base["cublas_dgemm_tflops"] if value else None,
+        "roofline": roofline,
+        "rows": rows,
     }
     print(json.dumps(out))
     return 0
@@ -672,6 +849,8 @@ def main(argv=None):
         return run_batch_workload(a)
     if a.workload == "serve":
         return run_serve_workload(a)
+    if a.workload == "precision":
+        return run_precision_workload(a)
     return run_ours(a)
 
 

@@ -59,6 +59,7 @@ class Profile(ctypes.Structure):
         ("peel_ms", ctypes.c_double), ("combine_ms", ctypes.c_double),
         ("form_bytes", ctypes.c_double), ("combine_bytes", ctypes.c_double),
         ("gemm_flops", ctypes.c_double), ("peel_flops", ctypes.c_double),
+        ("split_ms", ctypes.c_double), ("split_bf16_flops", ctypes.c_double),
     ]
 
     def as_dict(self):

@@ -57,8 +57,14 @@ cudaError_t run_program(const Program& prog, const void* h_desc, void* d_desc, i
         break;
       case OpKind::kSplitGemm: {
         int64_t n_launched = 0;
+        if (prof) {
+          rec.mid = prof->get();
+          if (!rec.mid) return cudaErrorMemoryAllocation;
+          const double products = op.split.slices * (op.split.slices + 1) / 2.0;
+          rec.bf16_flops = op.flops * products;
+        }
         e = split_gemm_launch(reinterpret_cast<const SplitDesc*>(base + op.desc_off), op.n, op.split,
-                              prog.split_scratch, d_err, num_sms, stream, &n_launched);
+                              prog.split_scratch, d_err, num_sms, stream, &n_launched, rec.mid);
         count += n_launched - 1;  // the op itself is counted below
         break;
       }

@@ -615,6 +615,16 @@ fmm_status fmm_profile_read(fmm_handle h, fmm_profile* out) {
         out->combine_bytes += r.bytes;
         break;
       case fmm::OpKind::kSplitGemm:
+        if (r.mid) {
+          float sms = 0.f;
+          FMM_CUDA_TRY(cudaEventElapsedTime(&sms, r.start, r.mid), "cudaEventElapsedTime");
+          out->split_ms += sms;
+        }
+        out->split_bf16_flops += r.bf16_flops;
+        out->gemm_launches++;
+        out->gemm_ms += ms;
+        out->gemm_flops += r.flops;
+        break;
       case fmm::OpKind::kGemm:
         if (r.peel) {
           out->peel_launches++;

@@ -87,7 +87,7 @@ size_t split_scratch_bytes(int64_t m, int64_t k, int64_t n, int64_t count, int s
 // bounded wait inside the product kernel gave up.  Returns the kernel count
 // launched through *launches.
 cudaError_t split_gemm_launch(const SplitDesc* d_descs, int n, const SplitPlan& plan, void* scratch, int* d_err,
-                              int num_sms, cudaStream_t stream, int64_t* launches);
+                              int num_sms, cudaStream_t stream, int64_t* launches, cudaEvent_t split_done = nullptr);
 // A kernel whose single bounded mbarrier wait is never satisfied: it records
 // `code` in *d_err after limit_ns and returns.
 cudaError_t wait_probe_launch(int* d_err, uint64_t limit_ns, int code, cudaStream_t stream);

@@ -42,6 +42,8 @@ struct Profiler {
     bool peel;
     double flops, bytes;
     cudaEvent_t start, stop;
+    cudaEvent_t mid = nullptr;  // split gemm: after the splitting kernels
+    double bf16_flops = 0.0;    // split gemm: tensor-core FLOPs of the slice products
   };
   std::vector<Rec> recs;
   std::vector<cudaEvent_t> pool;

@@ -370,19 +370,28 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
           tc_fence_after();
           const double scale = ldexp(1.0, -8 * (D + 2));
           const uint32_t taddr = tmem + ((uint32_t)(qd * 32) << 16) + buf * kBN + wg * 64;
+          // eight pieces of 8 columns, software-pipelined: the load of piece
+          // g + 1 is in flight while piece g is converted and accumulated
+          uint32_t r0[8], r1[8];
+          tmem_ld_32x32b_x8(taddr, r0);
+          tmem_ld_wait();
 #pragma unroll
-          for (int g4 = 0; g4 < 4; ++g4) {
-            uint32_t r[16];
-            tmem_ld_32x32b_x16(taddr + g4 * 16, r);
+          for (int g8 = 0; g8 < 8; g8 += 2) {
+            tmem_ld_32x32b_x8(taddr + (g8 + 1) * 8, r1);
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+              acc[g8 * 8 + j] = fma((double)__uint_as_float(r0[j]), scale, acc[g8 * 8 + j]);
             tmem_ld_wait();
-            if (g4 == 3) {  // the accumulator is free once the last piece is in registers
+            if (g8 + 2 < 8) tmem_ld_32x32b_x8(taddr + (g8 + 2) * 8, r0);
+            if (g8 + 2 == 8) {  // the accumulator is free once the last piece is in registers
               tc_fence_before();
               __syncwarp();
               if (lane == 0) mbar_arrive(&acc_empty[buf]);
             }
 #pragma unroll
-            for (int j = 0; j < 16; ++j)
-              acc[g4 * 16 + j] = fma((double)__uint_as_float(r[j]), scale, acc[g4 * 16 + j]);
+            for (int j = 0; j < 8; ++j)
+              acc[(g8 + 1) * 8 + j] = fma((double)__uint_as_float(r1[j]), scale, acc[(g8 + 1) * 8 + j]);
+            if (g8 + 2 < 8) tmem_ld_wait();
           }
         }
       if (!ok) break;
@@ -462,7 +471,7 @@ cudaError_t wait_probe_launch(int* d_err, uint64_t limit_ns, int code, cudaStrea
 }
 
 cudaError_t split_gemm_launch(const SplitDesc* d_descs, int n, const SplitPlan& plan, void* scratch, int* d_err,
-                              int num_sms, cudaStream_t stream, int64_t* launches) {
+                              int num_sms, cudaStream_t stream, int64_t* launches, cudaEvent_t split_done) {
   if (plan.tiles == 0) return cudaSuccess;
   if (plan.slices < kSplitMinSlices || plan.slices > kSplitMaxSlices || !d_err || !scratch ||
       reinterpret_cast<uintptr_t>(scratch) % 256 != 0)
@@ -480,6 +489,7 @@ cudaError_t split_gemm_launch(const SplitDesc* d_descs, int n, const SplitPlan& 
   split_b<<<grid_for(plan.n_f, cap), 256, 0, stream>>>(d_descs, n, plan.n_f, plan.slices, fb, bs);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
+  if (split_done && (e = cudaEventRecord(split_done, stream)) != cudaSuccess) return e;
   CUtensorMap tA, tB;
   if (!encode_slices(&tA, as, plan.rows_a, kBM) || !encode_slices(&tB, bs, plan.rows_b, kBN))
     return cudaErrorInvalidValue;

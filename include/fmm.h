@@ -192,6 +192,11 @@ typedef struct fmm_profile {
   double form_ms, gemm_ms, peel_ms, combine_ms;
   double form_bytes, combine_bytes;
   double gemm_flops, peel_flops;
+  /* split-BF16 leaf products (counted in gemm_* above as well): time of the
+   * scale / split kernels within gemm_ms, and the BF16 tensor-core FLOPs of
+   * the slice products (2 m n k per product, S(S+1)/2 products per leaf) */
+  double split_ms;
+  double split_bf16_flops;
 } fmm_profile;
 
 fmm_status fmm_profile_enable(fmm_handle h, int enable);
