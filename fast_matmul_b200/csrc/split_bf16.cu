@@ -19,9 +19,11 @@
 // dropped diagonals, so |C - AB| <~ 3 * 2^-8S * k * max|a_i.| * max|b_.j|.
 //
 // Product kernel: persistent CTAs over the 128 x 128 output tiles of every
-// problem.  Warp 0 issues TMA loads of (A_t, B_u) 64-deep k-blocks into a
-// 6-stage ring, warp 1 issues tcgen05.mma (M128 N128 K16) into one of four TMEM
-// accumulators of 128 FP32 columns, warps 2-9 (two warpgroups of 64
+// problem.  Warp 0 issues TMA loads of (A_t, B_u) over one 128-deep chunk
+// (64 KB) into a 3-stage ring, warp 1 issues 8 tcgen05.mma (M128 N128 K16)
+// per stage -- few waits and commits per MMA keep the single issuing thread
+// ahead of the tensor pipe -- into one of four TMEM accumulators of 128 FP32
+// columns, warps 2-9 (two warpgroups of 64
 // columns) drain each finished accumulator into FP64 registers.  Every
 // mbarrier wait is bounded; on a timeout the kernel records a code in *err,
 // lets its copies and MMAs in flight finish, frees its TMEM and returns.
@@ -41,17 +43,18 @@ namespace {
 
 using namespace sm100;
 
-constexpr int kBM = kSplitTile, kBN = kSplitTile, kBK = kSplitKBlock, kStages = 6;
+constexpr int kBM = kSplitTile, kBN = kSplitTile, kBK = kSplitKBlock;
+constexpr int kChunkBlocks = kSplitChunk / kBK;    // 64-deep k-blocks per chunk (2)
+constexpr int kTileBytes = kBM * kBK * 2;          // one 128 x 64 BF16 box: 16 KB
+constexpr int kStageBytes = 2 * kChunkBlocks * kTileBytes;  // A and B over one chunk: 64 KB
+constexpr int kStages = 3;
 constexpr int kAccBufs = 4;  // TMEM accumulators of 128 FP32 columns
-constexpr int kTileABytes = kBM * kBK * 2;  // 16 KB
-constexpr int kTileBBytes = kBN * kBK * 2;  // 16 KB
-constexpr int kStageBytes = kTileABytes + kTileBBytes;
-constexpr int kChunkBlocks = kSplitChunk / kBK;
 // TMA warp, MMA warp, 2 x 4 epilogue warps.  Registers are budgeted per
 // group of four warps, so the 10 warps are charged as 12: 168 per thread.
 constexpr int kGemmThreads = 320;
 constexpr size_t kGemmSmem = (size_t)kStages * kStageBytes + 1024;
-static_assert(kSplitChunk % kBK == 0, "chunks are whole k-blocks");
+static_assert(kChunkBlocks == 2, "a stage holds two k-blocks of A and of B");
+static_assert(kBM == kBN, "A and B boxes share the box size");
 static_assert(kBK * 2 == 128, "one k-block row is one 128-byte swizzle row");
 
 // Largest i in [0, n) with key(d[i]) <= x (keys non-decreasing).
@@ -271,74 +274,84 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
 
   if (warp == 0) {
     if (lane == 0) {
+      // one stage = one slice product over one 128-deep chunk: A_t and B_u,
+      // two 64-deep k-blocks each (four 16 KB boxes)
       prefetch_tensormap(&tmA);
       prefetch_tensormap(&tmB);
-      uint32_t it = 0;
+      uint32_t n = 0, st = 0, ph = 0;  // stages filled, current stage, its round parity
       bool ok = true;
       for (int64_t tile = blockIdx.x; tile < g.tiles && ok; tile += gridDim.x) {
         const TileCoord tc = tile_coord(g, tile);
         const SplitDesc& s = g.desc[tc.q];
         const int64_t mp = (int64_t)s.tiles_m * kBM, np = (int64_t)s.tiles_n * kBN;
+        const int64_t ya_tile = s.a_row + (int64_t)tc.tm * kBM, yb_tile = s.b_row + (int64_t)tc.tn * kBN;
         const int chunks = s.kblocks / kChunkBlocks;
         for (int c = 0; c < chunks && ok; ++c)
           for (int D = 0; D < S && ok; ++D)
-            for (int t = 0; t <= D && ok; ++t)
-              for (int kb = 0; kb < kChunkBlocks; ++kb, ++it) {
-                const int st = it % kStages;
-                if (it >= kStages && !mbar_wait(&empty[st], ((it / kStages) & 1) ^ 1, g.err, 1)) {
-                  ok = false;
-                  break;
-                }
-                const int64_t blk = (int64_t)c * kChunkBlocks + kb;
-                const int ya = (int)(s.a_row + ((int64_t)t * s.kblocks + blk) * mp + (int64_t)tc.tm * kBM);
-                const int yb = (int)(s.b_row + ((int64_t)(D - t) * s.kblocks + blk) * np + (int64_t)tc.tn * kBN);
-                uint8_t* dst = base + st * kStageBytes;
-                mbar_arrive_expect_tx(&full[st], kStageBytes);
-                tma_load_2d(dst, &tmA, &full[st], 0, ya);
-                tma_load_2d(dst + kTileABytes, &tmB, &full[st], 0, yb);
+            for (int t = 0; t <= D; ++t) {
+              if (n >= (uint32_t)kStages && !mbar_wait(&empty[st], ph ^ 1u, g.err, 1)) {
+                ok = false;
+                break;
               }
+              const int64_t blk = (int64_t)c * kChunkBlocks;
+              const int64_t ya = ya_tile + ((int64_t)t * s.kblocks + blk) * mp;
+              const int64_t yb = yb_tile + ((int64_t)(D - t) * s.kblocks + blk) * np;
+              uint8_t* dst = base + st * kStageBytes;
+              uint64_t* bar = &full[st];
+              mbar_arrive_expect_tx(bar, kStageBytes);
+              tma_load_2d(dst, &tmA, bar, 0, (int)ya);
+              tma_load_2d(dst + kTileBytes, &tmA, bar, 0, (int)(ya + mp));
+              tma_load_2d(dst + 2 * kTileBytes, &tmB, bar, 0, (int)yb);
+              tma_load_2d(dst + 3 * kTileBytes, &tmB, bar, 0, (int)(yb + np));
+              ++n;
+              if (++st == (uint32_t)kStages) {
+                st = 0;
+                ph ^= 1u;
+              }
+            }
       }
       // let every copy in flight land before the CTA can exit
-      for (uint32_t st = 0; st < (uint32_t)kStages && st < it; ++st) {
-        const uint32_t last = st + ((it - 1 - st) / kStages) * kStages;
-        mbar_wait(&full[st], (last / kStages) & 1, g.err, 5);
+      for (uint32_t sx = 0; sx < (uint32_t)kStages && sx < n; ++sx) {
+        const uint32_t last = sx + ((n - 1 - sx) / kStages) * kStages;
+        mbar_wait(&full[sx], (last / kStages) & 1, g.err, 5);
       }
     }
   } else if (warp == 1) {
     if (lane == 0) {
       const uint32_t idesc = idesc_bf16_f32(kBM, kBN);
-      uint32_t it = 0, ai = 0;
+      uint32_t st = 0, ph = 0, ai = 0;
       bool ok = true;
       for (int64_t tile = blockIdx.x; tile < g.tiles && ok; tile += gridDim.x) {
         const TileCoord tc = tile_coord(g, tile);
         const int chunks = g.desc[tc.q].kblocks / kChunkBlocks;
         for (int c = 0; c < chunks && ok; ++c)
           for (int D = 0; D < S && ok; ++D, ++ai) {
-            const int buf = ai % kAccBufs;
-            if (ai >= kAccBufs && !mbar_wait(&acc_empty[buf], ((ai / kAccBufs) - 1) & 1, g.err, 2)) {
+            const uint32_t buf = ai % kAccBufs;
+            if (ai >= (uint32_t)kAccBufs && !mbar_wait(&acc_empty[buf], ((ai / kAccBufs) - 1) & 1, g.err, 2)) {
               ok = false;
               break;
             }
             tc_fence_after();
             const uint32_t d_tmem = tmem + buf * kBN;
-            bool acc = false;
-            for (int t = 0; t <= D && ok; ++t)
-              for (int kb = 0; kb < kChunkBlocks; ++kb, ++it) {
-                const int st = it % kStages;
-                if (!mbar_wait(&full[st], (it / kStages) & 1, g.err, 3)) {
-                  ok = false;
-                  break;
-                }
-                tc_fence_after();
-                const uint32_t a = smem_addr(base + st * kStageBytes);
-#pragma unroll
-                for (int kk = 0; kk < kBK / 16; ++kk) {
-                  mma_bf16(d_tmem, smem_desc_sw128(a + kk * 32), smem_desc_sw128(a + kTileABytes + kk * 32), idesc,
-                           acc);
-                  acc = true;
-                }
-                mma_commit(&empty[st]);
+            for (int t = 0; t <= D; ++t) {
+              if (!mbar_wait(&full[st], ph, g.err, 3)) {
+                ok = false;
+                break;
               }
+              tc_fence_after();
+              const uint32_t a = smem_addr(base + st * kStageBytes);
+              const uint32_t b = a + 2 * kTileBytes;
+#pragma unroll
+              for (int kk = 0; kk < 2 * kBK / 16; ++kk) {
+                const uint32_t off = (kk >> 2) * kTileBytes + (kk & 3) * 32;
+                mma_bf16(d_tmem, smem_desc_sw128(a + off), smem_desc_sw128(b + off), idesc, t > 0 || kk > 0);
+              }
+              mma_commit(&empty[st]);
+              if (++st == (uint32_t)kStages) {
+                st = 0;
+                ph ^= 1u;
+              }
+            }
             if (ok) mma_commit(&acc_full[buf]);
           }
       }
