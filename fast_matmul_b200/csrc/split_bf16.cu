@@ -46,14 +46,17 @@ using namespace sm100;
 constexpr int kBM = kSplitTile, kBN = kSplitTile, kBK = kSplitKBlock;
 constexpr int kChunkBlocks = kSplitChunk / kBK;    // 64-deep k-blocks per chunk (2)
 constexpr int kTileBytes = kBM * kBK * 2;          // one 128 x 64 BF16 box: 16 KB
-constexpr int kStageBytes = 2 * kChunkBlocks * kTileBytes;  // A and B over one chunk: 64 KB
+// Two k-blocks of A and of B per stage (64 KB), 3 stages: measured faster
+// than 7 stages of one k-block (fewer waits and commits per MMA).
+constexpr int kStageKBlocks = 2;
+constexpr int kStageBytes = 2 * kStageKBlocks * kTileBytes;
 constexpr int kStages = 3;
 constexpr int kAccBufs = 4;  // TMEM accumulators of 128 FP32 columns
 // TMA warp, MMA warp, 2 x 4 epilogue warps.  Registers are budgeted per
 // group of four warps, so the 10 warps are charged as 12: 168 per thread.
 constexpr int kGemmThreads = 320;
 constexpr size_t kGemmSmem = (size_t)kStages * kStageBytes + 1024;
-static_assert(kChunkBlocks == 2, "a stage holds two k-blocks of A and of B");
+static_assert(kChunkBlocks == 2 && kChunkBlocks % kStageKBlocks == 0, "stages tile the chunk");
 static_assert(kBM == kBN, "A and B boxes share the box size");
 static_assert(kBK * 2 == 128, "one k-block row is one 128-byte swizzle row");
 
@@ -81,6 +84,13 @@ __device__ __forceinline__ int exponent_above(double maxabs) {
 // ---------------------------------------------------------------------------
 // splitting
 
+// x * 2^-e, rounded like ldexp(x, -e): a multiplication by the exact power of
+// two when 2^-e is a normal double, ldexp otherwise.
+__device__ __forceinline__ double scale_pow2(double x, int e) {
+  if (e >= -1000 && e <= 1000) return x * __hiloint2double((1023 - e) << 20, 0);
+  return ldexp(x, -e);
+}
+
 // Row exponents of A: one thread per padded row (coalesced down each column).
 __global__ void __launch_bounds__(256) split_row_exponents(const SplitDesc* __restrict__ d, int nd, int64_t total,
                                                            int* __restrict__ ea) {
@@ -104,17 +114,28 @@ __global__ void __launch_bounds__(256) split_row_exponents(const SplitDesc* __re
 }
 
 // Digits of 8 scaled values as 8 BF16 per slice, one 16-byte store each.
+// d = rint(256 x) and the remainder 256 x - d come from the FP64 pipe:
+// 256 x is exact and |256 x| < 2^51, so fma(x, 256, 1.5 * 2^52) rounds it to
+// the nearest integer (ties to even, as rint does) and that integer is the
+// low word of the sum.  |d| <= 256, so its BF16 pattern is the top half of
+// the FP32 value (1.5 * 2^23 + d) - 1.5 * 2^23 (exact).  No conversion-unit
+// instruction is involved.
+__device__ __forceinline__ uint32_t bf16_bits_of_small_int(int d) {
+  return __float_as_uint(__int_as_float(0x4B400000 + d) - 12582912.0f) >> 16;
+}
+
 __device__ __forceinline__ void store_digits(double (&x)[8], int slices, __nv_bfloat16* dst, int64_t slice_stride) {
+  const double kRound = 6755399441055744.0;  // 1.5 * 2^52
   for (int t = 0; t < slices; ++t) {
-    __align__(16) __nv_bfloat16 v[8];
+    uint32_t w[4];
 #pragma unroll
-    for (int c = 0; c < 8; ++c) {
-      const double y = x[c] * 256.0;
-      const double dg = rint(y);
-      x[c] = y - dg;
-      v[c] = __double2bfloat16(dg);
+    for (int c = 0; c < 8; c += 2) {
+      const double y0 = fma(x[c], 256.0, kRound), y1 = fma(x[c + 1], 256.0, kRound);
+      x[c] = fma(x[c], 256.0, -(y0 - kRound));
+      x[c + 1] = fma(x[c + 1], 256.0, -(y1 - kRound));
+      w[c / 2] = bf16_bits_of_small_int(__double2loint(y0)) | (bf16_bits_of_small_int(__double2loint(y1)) << 16);
     }
-    *reinterpret_cast<uint4*>(dst + t * slice_stride) = *reinterpret_cast<const uint4*>(v);
+    *reinterpret_cast<uint4*>(dst + t * slice_stride) = make_uint4(w[0], w[1], w[2], w[3]);
   }
 }
 
@@ -147,7 +168,7 @@ __global__ void __launch_bounds__(256) split_a(const SplitDesc* __restrict__ d, 
     const int e = ea[s.e_off + i0 + row];
     double x[8];
 #pragma unroll
-    for (int c = 0; c < 8; ++c) x[c] = ldexp(tile[at(kc + c, row)], -e);
+    for (int c = 0; c < 8; ++c) x[c] = scale_pow2(tile[at(kc + c, row)], e);
     const int64_t orow = s.a_row + kb * mp + i0 + row;
     store_digits(x, slices, out + orow * kBK + kc, (int64_t)s.kblocks * mp * kBK);
   }
@@ -210,7 +231,7 @@ __global__ void __launch_bounds__(256) split_b(const SplitDesc* __restrict__ d, 
         for (int c = 0; c < 8; ++c) v[c] = 0.0;
       }
 #pragma unroll
-      for (int c = 0; c < 8; ++c) v[c] = ldexp(v[c], -f);
+      for (int c = 0; c < 8; ++c) v[c] = scale_pow2(v[c], f);
       const int64_t orow = s.b_row + (int64_t)(p0 / kBK) * np + j;
       store_digits(v, slices, out + orow * kBK + (p0 % kBK), (int64_t)s.kblocks * np * kBK);
     }
@@ -235,13 +256,23 @@ struct TileCoord {
   int q, tm, tn;
 };
 
+// Tiles of a problem are walked in groups of kRasterRows tile rows, row
+// index fastest within a group: the CTAs of one wave cover a compact block
+// of the output, so the A and B slices they read stay in L2 between them.
+constexpr int kRasterRows = 16;
+
 __device__ __forceinline__ TileCoord tile_coord(const GemmParams& g, int64_t tile) {
   TileCoord c;
   c.q = find_desc(g.desc, g.nd, tile, [](const SplitDesc& s) { return s.tile_begin; });
   const SplitDesc& s = g.desc[c.q];
   const int64_t rem = tile - s.tile_begin;
-  c.tm = (int)(rem % s.tiles_m);
-  c.tn = (int)(rem / s.tiles_m);
+  const int64_t per_group = (int64_t)kRasterRows * s.tiles_n;
+  const int64_t group = rem / per_group;
+  const int first = (int)(group * kRasterRows);
+  const int rows = s.tiles_m - first < kRasterRows ? s.tiles_m - first : kRasterRows;
+  const int64_t local = rem - group * per_group;
+  c.tm = first + (int)(local % rows);
+  c.tn = (int)(local / rows);
   return c;
 }
 
@@ -288,27 +319,29 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         const int chunks = s.kblocks / kChunkBlocks;
         for (int c = 0; c < chunks && ok; ++c)
           for (int D = 0; D < S && ok; ++D)
-            for (int t = 0; t <= D; ++t) {
-              if (n >= (uint32_t)kStages && !mbar_wait(&empty[st], ph ^ 1u, g.err, 1)) {
-                ok = false;
-                break;
+            for (int t = 0; t <= D && ok; ++t)
+              for (int h = 0; h < kChunkBlocks; h += kStageKBlocks) {
+                if (n >= (uint32_t)kStages && !mbar_wait(&empty[st], ph ^ 1u, g.err, 1)) {
+                  ok = false;
+                  break;
+                }
+                const int64_t blk = (int64_t)c * kChunkBlocks + h;
+                const int64_t ya = ya_tile + ((int64_t)t * s.kblocks + blk) * mp;
+                const int64_t yb = yb_tile + ((int64_t)(D - t) * s.kblocks + blk) * np;
+                uint8_t* dst = base + st * kStageBytes;
+                uint64_t* bar = &full[st];
+                mbar_arrive_expect_tx(bar, kStageBytes);
+#pragma unroll
+                for (int b = 0; b < kStageKBlocks; ++b) {
+                  tma_load_2d(dst + b * kTileBytes, &tmA, bar, 0, (int)(ya + b * mp));
+                  tma_load_2d(dst + (kStageKBlocks + b) * kTileBytes, &tmB, bar, 0, (int)(yb + b * np));
+                }
+                ++n;
+                if (++st == (uint32_t)kStages) {
+                  st = 0;
+                  ph ^= 1u;
+                }
               }
-              const int64_t blk = (int64_t)c * kChunkBlocks;
-              const int64_t ya = ya_tile + ((int64_t)t * s.kblocks + blk) * mp;
-              const int64_t yb = yb_tile + ((int64_t)(D - t) * s.kblocks + blk) * np;
-              uint8_t* dst = base + st * kStageBytes;
-              uint64_t* bar = &full[st];
-              mbar_arrive_expect_tx(bar, kStageBytes);
-              tma_load_2d(dst, &tmA, bar, 0, (int)ya);
-              tma_load_2d(dst + kTileBytes, &tmA, bar, 0, (int)(ya + mp));
-              tma_load_2d(dst + 2 * kTileBytes, &tmB, bar, 0, (int)yb);
-              tma_load_2d(dst + 3 * kTileBytes, &tmB, bar, 0, (int)(yb + np));
-              ++n;
-              if (++st == (uint32_t)kStages) {
-                st = 0;
-                ph ^= 1u;
-              }
-            }
       }
       // let every copy in flight land before the CTA can exit
       for (uint32_t sx = 0; sx < (uint32_t)kStages && sx < n; ++sx) {
@@ -333,25 +366,26 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
             }
             tc_fence_after();
             const uint32_t d_tmem = tmem + buf * kBN;
-            for (int t = 0; t <= D; ++t) {
-              if (!mbar_wait(&full[st], ph, g.err, 3)) {
-                ok = false;
-                break;
-              }
-              tc_fence_after();
-              const uint32_t a = smem_addr(base + st * kStageBytes);
-              const uint32_t b = a + 2 * kTileBytes;
+            for (int t = 0; t <= D && ok; ++t)
+              for (int h = 0; h < kChunkBlocks; h += kStageKBlocks) {
+                if (!mbar_wait(&full[st], ph, g.err, 3)) {
+                  ok = false;
+                  break;
+                }
+                tc_fence_after();
+                const uint32_t a = smem_addr(base + st * kStageBytes);
+                const uint32_t b = a + kStageKBlocks * kTileBytes;
 #pragma unroll
-              for (int kk = 0; kk < 2 * kBK / 16; ++kk) {
-                const uint32_t off = (kk >> 2) * kTileBytes + (kk & 3) * 32;
-                mma_bf16(d_tmem, smem_desc_sw128(a + off), smem_desc_sw128(b + off), idesc, t > 0 || kk > 0);
+                for (int kk = 0; kk < kStageKBlocks * kBK / 16; ++kk) {
+                  const uint32_t off = (kk >> 2) * kTileBytes + (kk & 3) * 32;
+                  mma_bf16(d_tmem, smem_desc_sw128(a + off), smem_desc_sw128(b + off), idesc, t > 0 || h > 0 || kk > 0);
+                }
+                mma_commit(&empty[st]);
+                if (++st == (uint32_t)kStages) {
+                  st = 0;
+                  ph ^= 1u;
+                }
               }
-              mma_commit(&empty[st]);
-              if (++st == (uint32_t)kStages) {
-                st = 0;
-                ph ^= 1u;
-              }
-            }
             if (ok) mma_commit(&acc_full[buf]);
           }
       }
