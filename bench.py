@@ -306,6 +306,7 @@ def run_ours(a):
     torch.cuda.synchronize()
     classical_tf = flops * reps / (e0.elapsed_time(e1) * 1e-3) / 1e12
     rel, absd = fmm.max_relative_diff(Cc, C, handle=h)
+    ex_rel, ex_scaled = exact_sample_errors(A, B, C, count=32)
     At, Bt = A, B
     Ct = torch.matmul(At, Bt)
     torch.cuda.synchronize()
@@ -397,7 +398,9 @@ def run_ours(a):
                        "precision": "fp64", "parallelism": "replicas" if world > 1 else "single GPU",
                        "l2": "inputs larger than L2 (each operand %.1f GiB > 126 MB)" % (8.0 * m * k / 2**30)},
             "error": {"max_rel_diff_vs_classical": rel, "max_abs_diff_vs_classical": absd,
-                      "max_rel_diff_vs_cublas": rel_cublas},
+                      "max_rel_diff_vs_cublas": rel_cublas,
+                      "max_rel_vs_exact_32_sampled_entries": ex_rel,
+                      "max_vs_exact_over_absAB_32_sampled_entries": ex_scaled},
             "classical": {"engine_dgemm_tflops": classical_tf, "cublas_dgemm_tflops": cublas_tf,
                           "speedup_vs_engine_classical": value / world / classical_tf,
                           "speedup_vs_cublas": value / world / cublas_tf},
@@ -699,6 +702,46 @@ def scaled_normal(m, n, seed, per, device):
     return X
 
 
+def exact_sample_errors(A, B, C, count=32, seed=0):
+    """Errors of C against the exact product on `count` sampled entries:
+    (max |c - q| / |q|, max |c - q| / (|A||B|)_ij) with q the exact rational
+    value of the dot product (every double is an integer times a power of two,
+    so the sum is formed in Python integers over a common power-of-two
+    denominator)."""
+    from fractions import Fraction
+
+    import numpy as np
+    import torch
+
+    m, k = A.shape
+    n = B.shape[1]
+    rng = np.random.default_rng(seed)
+    rows = rng.integers(0, m, count)
+    cols = rng.integers(0, n, count)
+    ri = torch.as_tensor(rows, device=A.device)
+    ci = torch.as_tensor(cols, device=B.device)
+    ar = A.index_select(0, ri).cpu().numpy()
+    bc = B.index_select(1, ci).t().cpu().numpy()
+    cv = C[ri, ci].cpu().numpy()
+    worst_rel = worst_scaled = 0.0
+    for s in range(count):
+        nums, dens, anums = [], [], []
+        for x, y in zip(ar[s].tolist(), bc[s].tolist()):
+            nx, dx = x.as_integer_ratio()
+            ny, dy = y.as_integer_ratio()
+            nums.append(nx * ny)
+            dens.append(dx * dy)
+        den = max(dens)
+        q_num = sum(nv * (den // dv) for nv, dv in zip(nums, dens))
+        aq_num = sum(abs(nv) * (den // dv) for nv, dv in zip(nums, dens))
+        diff = abs(Fraction(float(cv[s])) - Fraction(q_num, den))
+        if q_num:
+            worst_rel = max(worst_rel, float(diff / abs(Fraction(q_num, den))))
+        if aq_num:
+            worst_scaled = max(worst_scaled, float(diff / Fraction(aq_num, den)))
+    return worst_rel, worst_scaled
+
+
 def precision_errors(fmm, A, B, C, ref, absAB, h):
     """Errors of C against the FP64 classical product ref: elementwise
     max |C - D| / |D| (the reference's MaxRelativeDiff), normwise
@@ -710,7 +753,9 @@ def precision_errors(fmm, A, B, C, ref, absAB, h):
     d = (C - ref).abs_().div_(absAB.clamp_min(1e-300))
     scaled = float(d.max())
     del d
-    return {"max_rel_elementwise": rel, "max_rel_normwise": norm, "max_abs_over_absAB": scaled}
+    ex_rel, ex_scaled = exact_sample_errors(A, B, C, count=16)
+    return {"max_rel_elementwise": rel, "max_rel_normwise": norm, "max_abs_over_absAB": scaled,
+            "max_rel_vs_exact_16_sampled_entries": ex_rel, "max_vs_exact_over_absAB_16_sampled_entries": ex_scaled}
 
 
 def run_precision_workload(a):

@@ -368,3 +368,39 @@ void oracle_fill_uniform(double* out, long count, uint64_t seed, uint64_t stream
     out[e] = lo + (hi - lo) * u;
   }
 }
+
+/* Quad-precision check of sampled entries: the reference's QuadMatmul
+ * (linalg/quadmatmul.hpp:8-28, C(i,j) += (__float128)A(i,l) * (__float128)B(l,j))
+ * restricted to `count` (row, column) samples.  arows holds the sampled rows
+ * of A (count x k, row s contiguous), bcols the sampled columns of B (count x
+ * k, column s contiguous), values the computed C entries.  In __float128, q_s
+ * = sum_l a_l b_l and aq_s = sum_l |a_l| |b_l|; *max_rel receives
+ * max_s |values[s] - q_s| / |q_s| (q_s == 0 skipped) and *max_scaled
+ * max_s |values[s] - q_s| / aq_s (aq_s == 0 skipped). */
+void oracle_quad_errors(const double* arows, const double* bcols, long k, long count, const double* values,
+                        double* max_rel, double* max_scaled) {
+  double mr = 0.0, ms = 0.0;
+  long s, l;
+  for (s = 0; s < count; ++s) {
+    const double* a = arows + s * k;
+    const double* b = bcols + s * k;
+    __float128 q = 0, aq = 0, d;
+    for (l = 0; l < k; ++l) {
+      const __float128 p = (__float128)a[l] * (__float128)b[l];
+      q += p;
+      aq += p < 0 ? -p : p;
+    }
+    d = (__float128)values[s] - q;
+    if (d < 0) d = -d;
+    if (q != 0) {
+      const double r = (double)(d / (q < 0 ? -q : q));
+      if (r > mr) mr = r;
+    }
+    if (aq != 0) {
+      const double r = (double)(d / aq);
+      if (r > ms) ms = r;
+    }
+  }
+  *max_rel = mr;
+  *max_scaled = ms;
+}

@@ -57,6 +57,8 @@ def oracle_lib() -> ctypes.CDLL:
         L.oracle_algorithm_index.argtypes = [ctypes.c_char_p]
         L.oracle_algorithm_index.restype = _I
         L.oracle_fill_uniform.argtypes = [_P, _L, ctypes.c_uint64, ctypes.c_uint64, _D, _D]
+        L.oracle_quad_errors.argtypes = [_P, _P, _L, _L, _P, ctypes.POINTER(_D), ctypes.POINTER(_D)]
+        L.oracle_quad_errors.restype = None
         L.oracle_fill_uniform.restype = None
         L.oracle_set_leaf_gemm.argtypes = [ctypes.c_void_p]
         L.oracle_set_leaf_gemm.restype = None
@@ -169,6 +171,23 @@ def use_reference_leaf(enabled: bool) -> None:
         L.oracle_set_leaf_gemm(ctypes.cast(R.fmmref_matmul, ctypes.c_void_p))
     else:
         L.oracle_set_leaf_gemm(None)
+
+
+def quad_errors(A: np.ndarray, B: np.ndarray, rows, cols, values) -> tuple:
+    """Errors of computed entries values[s] = C[rows[s], cols[s]] against the
+    quad-precision product (oracle_quad_errors, after linalg/quadmatmul.hpp):
+    (max |v - q| / |q|, max |v - q| / (|A| |B|)_ij)."""
+    L = oracle_lib()
+    rows = np.asarray(rows, dtype=np.int64)
+    cols = np.asarray(cols, dtype=np.int64)
+    ar = np.ascontiguousarray(A[rows, :], dtype=np.float64)
+    bc = np.ascontiguousarray(B[:, cols].T, dtype=np.float64)
+    v = np.ascontiguousarray(values, dtype=np.float64)
+    mr = ctypes.c_double()
+    ms = ctypes.c_double()
+    L.oracle_quad_errors(ar.ctypes.data_as(_P), bc.ctypes.data_as(_P), A.shape[1], len(rows), v.ctypes.data_as(_P),
+                         ctypes.byref(mr), ctypes.byref(ms))
+    return mr.value, ms.value
 
 
 def max_relative_diff(a: np.ndarray, b: np.ndarray) -> float:

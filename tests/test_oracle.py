@@ -111,3 +111,37 @@ def test_restatement_is_bit_exact_with_reference_leaves():
                 assert np.array_equal(C1, C2, equal_nan=True), (alg, m, k, n, steps)
     finally:
         oracle.use_reference_leaf(False)
+
+
+def test_quad_oracle_is_exact_on_integer_products_and_sees_fp64_rounding():
+    """The quad-precision sampled-entry check (linalg/quadmatmul.hpp restated):
+    zero error on integer matrices (every product and sum exact), a small
+    nonzero error for an FP64 product, a planted 1e-10 error found as such,
+    and agreement with exact rational sums (fractions) on a few entries."""
+    from fractions import Fraction
+
+    rng = np.random.default_rng(5)
+    m, k, n = 40, 300, 30
+    Ai = np.asfortranarray(rng.integers(-1000, 1000, (m, k)).astype(np.float64))
+    Bi = np.asfortranarray(rng.integers(-1000, 1000, (k, n)).astype(np.float64))
+    exact = (Ai.astype(np.int64) @ Bi.astype(np.int64)).astype(np.float64)
+    rows = rng.integers(0, m, 50)
+    cols = rng.integers(0, n, 50)
+    rel, scaled = oracle.quad_errors(Ai, Bi, rows, cols, exact[rows, cols])
+    assert rel == 0.0 and scaled == 0.0
+
+    A = oracle.uniform(m, k, 9, 1)
+    B = oracle.uniform(k, n, 9, 2)
+    C = np.zeros((m, n), order="F")
+    oracle.matmul(A, B, C)
+    rel, scaled = oracle.quad_errors(A, B, rows, cols, C[rows, cols])
+    assert 0.0 < rel <= k * 2.0 ** -53 and scaled <= rel
+    bad = C[rows, cols].copy()
+    bad[7] *= 1.0 + 1e-10
+    rel_bad, _ = oracle.quad_errors(A, B, rows, cols, bad)
+    assert 0.5e-10 < rel_bad < 2e-10
+
+    # exactly rounded rational sums measure within one rounding of the quad result
+    ex = [float(sum(Fraction(A[i, l]) * Fraction(B[l, j]) for l in range(k))) for i, j in zip(rows[:8], cols[:8])]
+    rel_ex, _ = oracle.quad_errors(A, B, rows[:8], cols[:8], ex)
+    assert rel_ex <= 2.0 ** -53
