@@ -404,3 +404,98 @@ void oracle_quad_errors(const double* arows, const double* bcols, long k, long c
   *max_rel = mr;
   *max_scaled = ms;
 }
+
+/* ---- diagonal scaling (scaling/scaling.hpp) ---- */
+
+/* MaxAbsRow (scaling.hpp:63-73) / MaxAbsCol (:78-88): the largest |entry|,
+ * starting from 0 with a strict > (NaN entries never win). */
+static double o_max_abs_row(const double* a, long lda, int row, int cols) {
+  double mx = 0.0;
+  int c;
+  for (c = 0; c < cols; ++c) {
+    const double v = fabs(a[row + (long)c * lda]);
+    if (v > mx) mx = v;
+  }
+  return mx;
+}
+
+static double o_max_abs_col(const double* a, long lda, int col, int rows) {
+  double mx = 0.0;
+  int r;
+  for (r = 0; r < rows; ++r) {
+    const double v = fabs(a[r + (long)col * lda]);
+    if (v > mx) mx = v;
+  }
+  return mx;
+}
+
+/* RowScale (:28-35) and ColScale (:40-47): one multiplication per entry. */
+static void o_row_scale(double* a, long lda, int rows, int cols, const double* v) {
+  int i, j;
+  for (j = 0; j < cols; ++j)
+    for (i = 0; i < rows; ++i) a[i + (long)j * lda] *= v[i];
+}
+
+static void o_col_scale(double* a, long lda, int rows, int cols, const double* v) {
+  int i, j;
+  for (j = 0; j < cols; ++j)
+    for (i = 0; i < rows; ++i) a[i + (long)j * lda] *= v[j];
+}
+
+/* OuterScaling (:105-124): rows of A by 1 / max|row|, columns of B by
+ * 1 / max|column| (InverseVector, :52-58), maxima returned in x and y. */
+static void o_outer(double* a, long lda, double* b, long ldb, int m, int k, int n, double* x, double* y, double* tmp) {
+  int i;
+  for (i = 0; i < m; ++i) x[i] = o_max_abs_row(a, lda, i, k);
+  for (i = 0; i < m; ++i) tmp[i] = 1.0 / x[i];
+  o_row_scale(a, lda, m, k, tmp);
+  for (i = 0; i < n; ++i) y[i] = o_max_abs_col(b, ldb, i, k);
+  for (i = 0; i < n; ++i) tmp[i] = 1.0 / y[i];
+  o_col_scale(b, ldb, k, n, tmp);
+}
+
+/* InnerScaling (:129-138): z_k = sqrt(max|A(:,k)| / max|B(k,:)|); columns
+ * of A by 1 / z_k, rows of B by z_k. */
+static void o_inner(double* a, long lda, double* b, long ldb, int m, int k, int n, double* z, double* zinv) {
+  int l;
+  for (l = 0; l < k; ++l) z[l] = sqrt(o_max_abs_col(a, lda, l, m) / o_max_abs_row(b, ldb, l, n));
+  for (l = 0; l < k; ++l) zinv[l] = 1.0 / z[l];
+  o_col_scale(a, lda, m, k, zinv);
+  o_row_scale(b, ldb, k, n, z);
+}
+
+/* Scaling (:150-194) with type 0 OUTSIDE_INSIDE, 1 INSIDE_OUTSIDE, 2 INSIDE,
+ * 3 OUTSIDE; r (m) and s (n) start at 1 and collect the outer maxima
+ * (UpdateVals, :93-98).  Returns -1 for an unknown type. */
+int oracle_scaling(double* a, long lda, double* b, long ldb, int m, int k, int n, int num_steps, int type, double* r,
+                   double* s) {
+  const int big = (m > n ? m : n) > k ? (m > n ? m : n) : k;
+  double* x = (double*)malloc(sizeof(double) * (size_t)(m > 0 ? m : 1));
+  double* y = (double*)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+  double* t1 = (double*)malloc(sizeof(double) * (size_t)(big > 0 ? big : 1));
+  double* t2 = (double*)malloc(sizeof(double) * (size_t)(k > 0 ? k : 1));
+  int step, i, rc = 0;
+  for (i = 0; i < m; ++i) r[i] = 1.0;
+  for (i = 0; i < n; ++i) s[i] = 1.0;
+  if (type < 0 || type > 3) rc = -1;
+  for (step = 0; rc == 0 && step < num_steps; ++step) {
+    if (type == 1 || type == 2) o_inner(a, lda, b, ldb, m, k, n, t1, t2);
+    if (type != 2) {
+      o_outer(a, lda, b, ldb, m, k, n, x, y, t1);
+      for (i = 0; i < m; ++i) r[i] *= x[i];
+      for (i = 0; i < n; ++i) s[i] *= y[i];
+    }
+    if (type == 0) o_inner(a, lda, b, ldb, m, k, n, t1, t2);
+  }
+  free(x);
+  free(y);
+  free(t1);
+  free(t2);
+  return rc;
+}
+
+/* PostProcessScaling (:144-149): rows of C by r, then columns by s. */
+void oracle_scaling_postprocess(double* c, long ldc, int m, int n, const double* r, const double* s) {
+  o_row_scale(c, ldc, m, n, r);
+  o_col_scale(c, ldc, m, n, s);
+}

@@ -59,6 +59,10 @@ def oracle_lib() -> ctypes.CDLL:
         L.oracle_fill_uniform.argtypes = [_P, _L, ctypes.c_uint64, ctypes.c_uint64, _D, _D]
         L.oracle_quad_errors.argtypes = [_P, _P, _L, _L, _P, ctypes.POINTER(_D), ctypes.POINTER(_D)]
         L.oracle_quad_errors.restype = None
+        L.oracle_scaling.argtypes = [_P, _L, _P, _L, _I, _I, _I, _I, _I, _P, _P]
+        L.oracle_scaling.restype = _I
+        L.oracle_scaling_postprocess.argtypes = [_P, _L, _I, _I, _P, _P]
+        L.oracle_scaling_postprocess.restype = None
         L.oracle_fill_uniform.restype = None
         L.oracle_set_leaf_gemm.argtypes = [ctypes.c_void_p]
         L.oracle_set_leaf_gemm.restype = None
@@ -81,6 +85,10 @@ def ref_lib() -> Optional[ctypes.CDLL]:
         L.fmmref_matmul.argtypes = [_P, _I, _P, _I, _P, _I, _I, _I, _I, _D, _D]
         L.fmmref_matmul.restype = None
         L.fmmref_set_threads.argtypes = [_I]
+        L.fmmref_scaling.argtypes = [_P, _I, _P, _I, _I, _I, _I, _I, _I, _P, _P]
+        L.fmmref_scaling.restype = None
+        L.fmmref_scaling_postprocess.argtypes = [_P, _I, _I, _I, _P, _P]
+        L.fmmref_scaling_postprocess.restype = None
         L.fmmref_set_threads.restype = None
         L.fmmref_num_algorithms.restype = _I
         L.fmmref_algorithm_name.argtypes = [_I]
@@ -188,6 +196,36 @@ def quad_errors(A: np.ndarray, B: np.ndarray, rows, cols, values) -> tuple:
     L.oracle_quad_errors(ar.ctypes.data_as(_P), bc.ctypes.data_as(_P), A.shape[1], len(rows), v.ctypes.data_as(_P),
                          ctypes.byref(mr), ctypes.byref(ms))
     return mr.value, ms.value
+
+
+def scaling(A: np.ndarray, B: np.ndarray, num_steps: int, kind: int, ref: bool = False):
+    """Scaling<double>(A, B, num_steps, r, s, kind) (scaling/scaling.hpp) on
+    Fortran-ordered A, B in place; returns (r, s).  ref=True runs the
+    reference's own header through the reference build."""
+    m, k = A.shape
+    n = B.shape[1]
+    r = np.empty(m)
+    s = np.empty(n)
+    if ref:
+        ref_lib().fmmref_scaling(_p(A), max(m, 1), _p(B), max(k, 1), m, k, n, num_steps, kind,
+                                 r.ctypes.data_as(_P), s.ctypes.data_as(_P))
+    else:
+        rc = oracle_lib().oracle_scaling(_p(A), max(m, 1), _p(B), max(k, 1), m, k, n, num_steps, kind,
+                                         r.ctypes.data_as(_P), s.ctypes.data_as(_P))
+        if rc != 0:
+            raise ValueError("unknown scaling type %d" % kind)
+    return r, s
+
+
+def scaling_postprocess(C: np.ndarray, r: np.ndarray, s: np.ndarray, ref: bool = False) -> None:
+    """PostProcessScaling(C, r, s) (scaling/scaling.hpp) on Fortran-ordered C in place."""
+    m, n = C.shape
+    r = np.ascontiguousarray(r, dtype=np.float64)
+    s = np.ascontiguousarray(s, dtype=np.float64)
+    if ref:
+        ref_lib().fmmref_scaling_postprocess(_p(C), max(m, 1), m, n, r.ctypes.data_as(_P), s.ctypes.data_as(_P))
+    else:
+        oracle_lib().oracle_scaling_postprocess(_p(C), max(m, 1), m, n, r.ctypes.data_as(_P), s.ctypes.data_as(_P))
 
 
 def max_relative_diff(a: np.ndarray, b: np.ndarray) -> float:

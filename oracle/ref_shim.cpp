@@ -12,8 +12,10 @@
 
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "linalg.hpp"
+#include "scaling.hpp"
 
 #include "bini322_10_52_approx.hpp"
 #include "classical222.hpp"
@@ -151,6 +153,26 @@ void fmmref_matmul(double* a, int lda, double* b, int ldb, double* c, int ldc, i
   Matrix<double> B(b, ldb, k, n);
   Matrix<double> C(c, ldc, m, n, alpha);
   MatMul(A, B, C, beta);
+}
+
+// Scaling<double>(A, B, num_steps, r_vals, s_vals, type) from
+// scaling/scaling.hpp on caller buffers (A m x k, B k x n scaled in place);
+// r (m) and s (n) receive the factors.
+void fmmref_scaling(double* a, int lda, double* b, int ldb, int m, int k, int n, int num_steps, int type, double* r,
+                    double* s) {
+  Matrix<double> A(a, lda, m, k);
+  Matrix<double> B(b, ldb, k, n);
+  std::vector<double> rv, sv;
+  Scaling<double>(A, B, num_steps, rv, sv, type);
+  for (int i = 0; i < m; ++i) r[i] = rv[i];
+  for (int j = 0; j < n; ++j) s[j] = sv[j];
+}
+
+// PostProcessScaling(C, r_vals, s_vals) from scaling/scaling.hpp.
+void fmmref_scaling_postprocess(double* c, int ldc, int m, int n, const double* r, const double* s) {
+  Matrix<double> C(c, ldc, m, n);
+  std::vector<double> rv(r, r + m), sv(s, s + n);
+  PostProcessScaling(C, rv, sv);
 }
 
 }  // extern "C"

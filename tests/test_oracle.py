@@ -145,3 +145,35 @@ def test_quad_oracle_is_exact_on_integer_products_and_sees_fp64_rounding():
     ex = [float(sum(Fraction(A[i, l]) * Fraction(B[l, j]) for l in range(k))) for i, j in zip(rows[:8], cols[:8])]
     rel_ex, _ = oracle.quad_errors(A, B, rows[:8], cols[:8], ex)
     assert rel_ex <= 2.0 ** -53
+
+
+def scaled_normal(m, n, seed, per):
+    rng = np.random.default_rng(seed)
+    X = rng.standard_normal((m, n))
+    e = rng.integers(-16, 17, m if per == "row" else n)
+    X *= np.exp2(e)[:, None] if per == "row" else np.exp2(e)[None, :]
+    return np.asfortranarray(X)
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference build not present")
+@pytest.mark.parametrize("kind", [0, 1, 2, 3])
+def test_scaling_restatement_equals_reference_bit_for_bit(kind):
+    """oracle_scaling / oracle_scaling_postprocess against the reference's
+    Scaling<double> / PostProcessScaling (scaling/scaling.hpp)."""
+    for steps in (1, 2, 3):
+        A = scaled_normal(37, 53, kind + 10 * steps, "row")
+        B = scaled_normal(53, 29, kind + 10 * steps + 1, "col")
+        A1, B1 = A.copy(order="F"), B.copy(order="F")
+        A2, B2 = A.copy(order="F"), B.copy(order="F")
+        r1, s1 = oracle.scaling(A1, B1, steps, kind)
+        r2, s2 = oracle.scaling(A2, B2, steps, kind, ref=True)
+        for x, y in [(A1, A2), (B1, B2), (r1, r2), (s1, s2)]:
+            assert np.array_equal(x, y), (kind, steps)
+        C1 = A1 @ B1
+        C2 = np.asfortranarray(C1.copy())
+        C1 = np.asfortranarray(C1)
+        oracle.scaling_postprocess(C1, r1, s1)
+        oracle.scaling_postprocess(C2, r2, s2, ref=True)
+        assert np.array_equal(C1, C2)
+        # the unscaled product is recovered (up to rounding)
+        assert np.abs(C1 - A @ B).max() <= 1e-13 * np.abs(A @ B).max()
