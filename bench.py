@@ -53,11 +53,13 @@ def parse_args(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=4096, help="edge of the CPU baseline sample")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU work budget of the baseline sample")
-    ap.add_argument("--workload", default="product", choices=["product", "batch", "serve", "precision"],
+    ap.add_argument("--workload", default="product", choices=["product", "batch", "serve", "precision", "scaling"],
                     help="product: one large FastMatmul (the headline); batch: 4096 independent products "
                          "with log-uniform dimensions in [64, 1024] in one CUDA-graph plan; serve: a Poisson "
                          "request stream through the continuous-batching server; precision: split-BF16 leaf "
-                         "products (Strassen, Bini) against the FP64 oracle")
+                         "products (Strassen, Bini) against the FP64 oracle; scaling: diagonal scaling "
+                         "(Scaling + FastMatmul + PostProcessScaling) on skewed operands")
+    ap.add_argument("--scaling-size", type=int, default=16384, help="square size of the scaling workload")
     ap.add_argument("--precision-sizes", default="8192,16384",
                     help="square sizes of the precision workload")
     ap.add_argument("--batch-precision", default="fp64", choices=["fp64", "split_bf16"])
@@ -891,6 +893,155 @@ def run_precision_workload(a):
     return 0
 
 
+def skewed_pair(fmm, n, seed, dev):
+    """Seeded uniform [0, 1) operands with rows of A, columns of B and the
+    inner dimension scaled by powers of two 2^U{-20..20}: A = D_r U_A D_t,
+    B = D_t^-1 U_B D_c (the product is as well conditioned as U_A U_B)."""
+    import numpy as np
+    import torch
+
+    rng = np.random.default_rng(seed)
+    er, ec, et = (rng.integers(-20, 21, n) for _ in range(3))
+    A = fmm.random_matrix(n, n, 41, 1, device=dev.index)
+    B = fmm.random_matrix(n, n, 41, 2, device=dev.index)
+    p2 = lambda e: torch.from_numpy(np.ldexp(1.0, e)).to(dev)  # noqa: E731
+    A.mul_(p2(er)[:, None]).mul_(p2(et)[None, :])
+    B.mul_(p2(-et)[:, None]).mul_(p2(ec)[None, :])
+    return A, B
+
+
+def cpu_scaling_sample(edge, scaling_steps, seconds):
+    """Times the reference's Scaling<double> (scaling/scaling.hpp, single
+    host thread: the header has no parallel loop) on an edge x edge pair;
+    returns (median ms, runs)."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle  # the CPU baseline leg may load the reference build
+
+    if not oracle.ref_available():
+        raise RuntimeError("oracle/_ref/libfmm_ref.so is not built")
+    A = oracle.uniform(edge, edge, 7, 1)
+    B = oracle.uniform(edge, edge, 7, 2)
+    times = []
+    t_end = time.time() + seconds
+    while time.time() < t_end or len(times) < 2:
+        t0 = time.perf_counter()
+        oracle.scaling(A, B, scaling_steps, 0, ref=True)
+        times.append((time.perf_counter() - t0) * 1e3)
+    return statistics.median(times), len(times)
+
+
+def run_scaling_workload(a):
+    """Diagonal scaling (scaling/scaling.hpp) as the reference's
+    strassen_scaling_perf driver runs it: Scaling with 5 outside-inside
+    steps, Strassen with one step, PostProcessScaling, at n^3 on operands
+    skewed by powers of two.  Reported: the scaling's bandwidth against the
+    measured HBM copy peak (algorithmic bytes: one read of A and B, then one
+    read + write of both per outer or inner scaling), the time of the whole
+    scaled product against the unscaled one, the errors of both against the
+    classical FP64 product, and the reference's own Scaling on the host."""
+    import torch
+
+    import fast_matmul_b200 as fmm
+
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    h = fmm.default_handle(0)
+    n, sc_steps = a.scaling_size, 5
+    A, B = skewed_pair(fmm, n, 5, dev)
+    As, Bs = fmm.colmajor_empty(n, n, dev), fmm.colmajor_empty(n, n, dev)
+    C, ref = fmm.colmajor_empty(n, n, dev), fmm.colmajor_empty(n, n, dev)
+    fmm.matmul(A, B, ref, handle=h)
+
+    def timed(fn, reps):
+        for _ in range(max(a.warmup, 3)):
+            fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    # kernel bandwidth: inputs (2 x 2 GiB at 16384) are far larger than L2
+    As.copy_(A)
+    Bs.copy_(B)
+    launches0 = h.launches()
+    r, s = fmm.diagonal_scaling(As, Bs, sc_steps, fmm.OUTSIDE_INSIDE, handle=h)
+    launches_per_call = h.launches() - launches0
+    clocks = ClockSampler(0)
+    clocks.start()
+    ms_scale = timed(lambda: fmm.diagonal_scaling(As, Bs, sc_steps, fmm.OUTSIDE_INSIDE, handle=h), a.steps)
+    ms_post = timed(lambda: fmm.scaling_postprocess(C, r, s, handle=h), a.steps)
+    clk = clocks.stop()
+    passes = 1 + 2 * (2 * sc_steps)
+    bytes_scale = 8.0 * (2 * n * n) * passes
+    bytes_post = 16.0 * n * n
+    gbs_scale = bytes_scale / (ms_scale * 1e-3) / 1e9
+    gbs_post = bytes_post / (ms_post * 1e-3) / 1e9
+
+    def pipeline(kind, steps, **kw):
+        As.copy_(A)
+        Bs.copy_(B)
+        rr, ss = fmm.diagonal_scaling(As, Bs, sc_steps, kind, handle=h)
+        fmm.fast_matmul("strassen", As, Bs, C, steps, handle=h, **kw)
+        fmm.scaling_postprocess(C, rr, ss, handle=h)
+
+    rows = []
+    for label, steps, kw in [("fp64 strassen", 1, {}), ("fp64 strassen", 2, {}),
+                             ("split_bf16 x5 strassen", 1, {"precision": "split_bf16", "split_slices": 5})]:
+        ms_plain = timed(lambda: fmm.fast_matmul("strassen", A, B, C, steps, handle=h, **kw), 2)
+        e_plain, _ = fmm.max_relative_diff(ref, C, handle=h)
+        kind = fmm.INSIDE if "split" in label else fmm.OUTSIDE_INSIDE
+        # the copies of A and B are the caller's (the reference's driver
+        # copies too); they are timed apart and not charged to the scaling
+        ms_copy = timed(lambda: (As.copy_(A), Bs.copy_(B)), 2)
+        ms_scaled = timed(lambda: pipeline(kind, steps, **kw), 2) - ms_copy
+        e_scaled, _ = fmm.max_relative_diff(ref, C, handle=h)
+        row = {"product": label, "num_steps": steps, "scaling": ["outside_inside", "inside_outside", "inside",
+                                                                 "outside"][kind],
+               "scaling_steps": sc_steps, "ms_unscaled": ms_plain, "ms_scaled_pipeline": ms_scaled,
+               "overhead": ms_scaled / ms_plain - 1.0, "max_rel_err_unscaled": e_plain,
+               "max_rel_err_scaled": e_scaled}
+        rows.append(row)
+        print(json.dumps({"scaling_row": row}), file=sys.stderr, flush=True)
+
+    peaks, peak_src = measured_peaks()
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    traffic = committed_traffic("roofline_traffic_scaling.json")
+    cpu = None
+    if not a.no_cpu_baseline:
+        edge = 4096
+        cms, runs = cpu_scaling_sample(edge, sc_steps, a.cpu_seconds)
+        cpu = {"value": 8.0 * (2 * edge * edge) * passes / (cms * 1e-3) / 1e9, "unit": "GB/s", "cores": 1,
+               "kind": "reference",
+               "sample": "Scaling<double>(A, B, 5, r, s, OUTSIDE_INSIDE) of scaling/scaling.hpp, %d x %d "
+                         "uniform pair, median of %d runs, %.1f ms each" % (edge, edge, runs, cms)}
+    out = {
+        "metric": "diagonal scaling bandwidth (algorithmic bytes / time)", "value": gbs_scale, "unit": "GB/s",
+        "n_gpus": 1, "steps": a.steps, "warmup": max(a.warmup, 3), "ms_per_step": ms_scale,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "diagonal scaling: Scaling(A, B, 5, r, s, OUTSIDE_INSIDE) at %d x %d, "
+                               "strassen_scaling_perf's pipeline beside it" % (n, n),
+                   "l2": "inputs larger than L2"},
+        "gpu_launches": launches_per_call * a.steps,
+        "clocks": clk,
+        "roofline": {"kernel": "scale_reduce_kernel (+ factor kernels)", "bound": "hbm", "achieved": gbs_scale,
+                     "peak": hbm, "unit": "GB/s", "frac": gbs_scale / hbm,
+                     "peak_source": "hbm_gbs of MEASURED_PEAKS.json (%s)" % peak_src,
+                     "algorithmic_bytes_per_call": bytes_scale,
+                     "traffic": (traffic or {}).get("bytes_per_call"),
+                     "traffic_source": (traffic or {}).get("source")},
+        "postprocess": {"ms": ms_post, "achieved_gbs": gbs_post, "frac": gbs_post / hbm},
+        "cpu_baseline": cpu,
+        "pipelines": rows,
+    }
+    print(json.dumps(out))
+    return 0
+
+
 def main(argv=None):
     a = parse_args(argv)
     if a.impl == "reference":
@@ -903,6 +1054,8 @@ def main(argv=None):
         return run_serve_workload(a)
     if a.workload == "precision":
         return run_precision_workload(a)
+    if a.workload == "scaling":
+        return run_scaling_workload(a)
     return run_ours(a)
 
 

@@ -9,6 +9,10 @@ from ._lib import FmmError, lib  # noqa: F401
 from .api import (  # noqa: F401
     AUTO,
     CLASSICAL,
+    INSIDE,
+    INSIDE_OUTSIDE,
+    OUTSIDE,
+    OUTSIDE_INSIDE,
     Handle,
     Plan,
     Server,
@@ -22,6 +26,7 @@ from .api import (  # noqa: F401
     algorithm_names,
     colmajor_empty,
     default_handle,
+    diagonal_scaling,
     fast_matmul,
     fast_matmul_host,
     matmul,
@@ -29,6 +34,7 @@ from .api import (  # noqa: F401
     max_relative_diff,
     num_algorithms,
     random_matrix,
+    scaling_postprocess,
     synchronize,
     workspace_bytes,
 )

@@ -152,6 +152,11 @@ SIGNATURES = {
     "fmm_max_relative_diff": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
                                               ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, c_double_p,
                                               c_double_p]),
+    "fmm_diagonal_scaling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+                                             ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
+                                             ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]),
+    "fmm_scaling_postprocess": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
+                                                ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p]),
     "fmm_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
     "fmm_kernel_launch_count": (ctypes.c_int64, [ctypes.c_void_p]),
     "fmm_selftest_wait_timeout": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.POINTER(ctypes.c_int)]),

@@ -295,6 +295,48 @@ def max_relative_diff(A, B, handle: Optional[Handle] = None) -> Tuple[float, flo
 
 
 # ---------------------------------------------------------------------------
+# diagonal scaling (scaling/scaling.hpp)
+
+OUTSIDE_INSIDE, INSIDE_OUTSIDE, INSIDE, OUTSIDE = 0, 1, 2, 3
+_SCALING_TYPES = {"outside_inside": OUTSIDE_INSIDE, "inside_outside": INSIDE_OUTSIDE, "inside": INSIDE,
+                  "outside": OUTSIDE}
+
+
+def diagonal_scaling(A, B, num_steps: int, scaling_type=OUTSIDE_INSIDE, handle: Optional[Handle] = None):
+    """Scaling(A, B, num_steps, r_vals, s_vals, scaling_type)
+    (scaling/scaling.hpp:153-196): scales the device matrices A and B in
+    place and returns the factors (r_vals, s_vals) as device tensors, for
+    scaling_postprocess.  scaling_type is 0..3 or its name."""
+    torch = _torch()
+    m, k = A.shape
+    n = B.shape[1]
+    kind = _SCALING_TYPES.get(scaling_type, scaling_type) if isinstance(scaling_type, str) else scaling_type
+    if isinstance(kind, str):
+        raise ValueError("Unknown iteration type.")
+    pa, lda = _mat(A, m, k, "A")
+    pb, ldb = _mat(B, k, n, "B")
+    r = torch.empty(m, dtype=torch.float64, device=A.device)
+    s = torch.empty(n, dtype=torch.float64, device=A.device)
+    h = handle or default_handle(A.device.index)
+    check(lib().fmm_diagonal_scaling(h.ptr, pa, lda, pb, ldb, m, k, n, num_steps, int(kind), r.data_ptr(),
+                                     s.data_ptr()))
+    return r, s
+
+
+def scaling_postprocess(C, r_vals, s_vals, handle: Optional[Handle] = None) -> None:
+    """PostProcessScaling(C, r_vals, s_vals) (scaling/scaling.hpp:143-148):
+    C(i, j) := (C(i, j) * r_vals[i]) * s_vals[j] on the device."""
+    torch = _torch()
+    m, n = C.shape
+    pc, ldc = _mat(C, m, n, "C")
+    for v, size, name in ((r_vals, m, "r_vals"), (s_vals, n, "s_vals")):
+        if v.dtype != torch.float64 or tuple(v.shape) != (size,) or (size > 1 and v.stride(0) != 1):
+            raise ValueError("%s must be a contiguous float64 vector of length %d" % (name, size))
+    h = handle or default_handle(C.device.index)
+    check(lib().fmm_scaling_postprocess(h.ptr, pc, ldc, m, n, r_vals.data_ptr(), s_vals.data_ptr()))
+
+
+# ---------------------------------------------------------------------------
 # batches, autotuning and CUDA-graph plans (no counterpart in the reference)
 
 CLASSICAL = _lib.FMM_ALG_CLASSICAL

@@ -41,6 +41,8 @@ struct fmm_handle_s {
   double* io = nullptr;
   size_t io_cap = 0;
   double* d_small = nullptr;  // two doubles for reductions
+  void* scal = nullptr;       // maxima and factors of the diagonal scaling
+  size_t scal_cap = 0;
   int* d_err = nullptr;       // error codes of split-BF16 kernels (bounded waits that gave up)
   int64_t launches = 0;
   fmm::Program prog;

@@ -238,6 +238,7 @@ fmm_status fmm_handle_create(fmm_handle* out, int device) {
     cudaGetLastError();
     if (h->desc_done) cudaEventDestroy(h->desc_done);
     if (h->d_small) cudaFree(h->d_small);
+  if (h->scal) cudaFree(h->scal);
     if (h->d_err) cudaFree(h->d_err);
     delete h;
     return fail(FMM_ERR_CUDA, "handle setup failed");
@@ -255,6 +256,7 @@ fmm_status fmm_handle_destroy(fmm_handle h) {
   if (h->h_desc) cudaFreeHost(h->h_desc);
   if (h->io) cudaFree(h->io);
   if (h->d_small) cudaFree(h->d_small);
+  if (h->scal) cudaFree(h->scal);
   if (h->d_err) cudaFree(h->d_err);
   if (h->desc_done) cudaEventDestroy(h->desc_done);
   delete h;
@@ -555,6 +557,40 @@ fmm_status fmm_max_relative_diff(fmm_handle h, const double* a, int64_t lda, con
   FMM_CUDA_TRY(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
   if (max_rel) *max_rel = res[0];
   if (max_abs) *max_abs = res[1];
+  return FMM_OK;
+}
+
+fmm_status fmm_diagonal_scaling(fmm_handle h, double* A, int64_t lda, double* B, int64_t ldb, int64_t m, int64_t k,
+                                int64_t n, int num_steps, int type, double* r, double* s) {
+  if (!h) return fail(FMM_ERR_INVALID_ARGUMENT, "null handle");
+  fmm_status st = check_dims(m, k, n, lda, ldb, m > 1 ? m : 1);
+  if (st != FMM_OK) return st;
+  if (num_steps < 0) return fail(FMM_ERR_INVALID_ARGUMENT, "num_steps must be >= 0");
+  if (type < FMM_SCALING_OUTSIDE_INSIDE || type > FMM_SCALING_OUTSIDE)
+    return fail(FMM_ERR_INVALID_ARGUMENT, "Unknown iteration type.");
+  if ((m > 0 && !r) || (n > 0 && !s)) return fail(FMM_ERR_INVALID_ARGUMENT, "null factor pointer");
+  if ((m * k > 0 && !A) || (k * n > 0 && !B)) return fail(FMM_ERR_INVALID_ARGUMENT, "null matrix pointer");
+  DeviceGuard g(h->device);
+  if (!g.ok()) return fail(FMM_ERR_CUDA, "cudaSetDevice failed");
+  st = ensure_device_buffer(h, &h->scal, &h->scal_cap, fmm::scaling_scratch_bytes(m, k, n), "scaling scratch");
+  if (st != FMM_OK) return st;
+  FMM_CUDA_TRY(fmm::scaling_launch(A, lda, B, ldb, (int)m, (int)k, (int)n, num_steps, type, r, s, h->scal, h->stream,
+                                   &h->launches),
+               "diagonal scaling");
+  return FMM_OK;
+}
+
+fmm_status fmm_scaling_postprocess(fmm_handle h, double* C, int64_t ldc, int64_t m, int64_t n, const double* r,
+                                   const double* s) {
+  if (!h) return fail(FMM_ERR_INVALID_ARGUMENT, "null handle");
+  fmm_status st = check_dims(m, 0, n, m > 1 ? m : 1, 1, ldc);
+  if (st != FMM_OK) return st;
+  if (m == 0 || n == 0) return FMM_OK;
+  if (!C || !r || !s) return fail(FMM_ERR_INVALID_ARGUMENT, "null pointer");
+  DeviceGuard g(h->device);
+  if (!g.ok()) return fail(FMM_ERR_CUDA, "cudaSetDevice failed");
+  FMM_CUDA_TRY(fmm::scaling_postprocess_launch(C, ldc, (int)m, (int)n, r, s, h->stream, &h->launches),
+               "scaling postprocess");
   return FMM_OK;
 }
 

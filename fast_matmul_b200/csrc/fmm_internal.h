@@ -148,6 +148,20 @@ cudaError_t combine_launch(int alg, const CombineLaunch& L, const CoefSlots& cf,
                            cudaStream_t stream);
 
 // ---------------------------------------------------------------------------
+// Diagonal scaling (scaling.cu).
+//
+// Device scratch of scaling_launch for m x k x n operands.
+size_t scaling_scratch_bytes(int64_t m, int64_t k, int64_t n);
+// Scales A (m x k) and B (k x n) in place, `num_steps` steps of scaling
+// `type` (0 outside-inside, 1 inside-outside, 2 inside, 3 outside), and
+// writes the row factors r (m) and column factors s (n).
+cudaError_t scaling_launch(double* A, int64_t lda, double* B, int64_t ldb, int m, int k, int n, int num_steps,
+                           int type, double* r, double* s, void* scratch, cudaStream_t stream, int64_t* launches);
+// C(i,j) = (C(i,j) * r[i]) * s[j].
+cudaError_t scaling_postprocess_launch(double* C, int64_t ldc, int m, int n, const double* r, const double* s,
+                                       cudaStream_t stream, int64_t* launches);
+
+// ---------------------------------------------------------------------------
 // Utilities (util_kernels.cu).
 cudaError_t fill_uniform_launch(double* out, int64_t rows, int64_t cols, int64_t ld, uint64_t seed, uint64_t stream_id,
                                 double lo, double hi, cudaStream_t stream);

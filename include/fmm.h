@@ -164,6 +164,35 @@ fmm_status fmm_fill_uniform(fmm_handle h, double* out, int64_t rows, int64_t col
 fmm_status fmm_max_relative_diff(fmm_handle h, const double* a, int64_t lda, const double* b, int64_t ldb,
                                  int64_t m, int64_t n, double* max_rel, double* max_abs);
 
+/* Diagonal scaling types: the reference's unnamed enum OUTSIDE_INSIDE,
+ * INSIDE_OUTSIDE, INSIDE, OUTSIDE (scaling/scaling.hpp:19-24). */
+enum {
+  FMM_SCALING_OUTSIDE_INSIDE = 0,
+  FMM_SCALING_INSIDE_OUTSIDE = 1,
+  FMM_SCALING_INSIDE = 2,
+  FMM_SCALING_OUTSIDE = 3
+};
+
+/* Diagonal scaling of the operands before a product, replacing
+ * Scaling<double>(A, B, num_steps, r_vals, s_vals, scaling_type)
+ * (scaling/scaling.hpp:153-196).  A (m x k) and B (k x n), device
+ * matrices, are scaled in place on the handle's stream; r (m) and s (n),
+ * device arrays, are overwritten with the row and column factors (the
+ * reference resizes fresh vectors to 1 and multiplies the outer maxima in).
+ * Each step is an outer scaling (rows of A by 1 / max|A(i,:)|, columns of B
+ * by 1 / max|B(:,j)|) and/or an inner scaling (columns of A by 1 / z_l and
+ * rows of B by z_l, z_l = sqrt(max|A(:,l)| / max|B(l,:)|)) in the order of
+ * `type`.  Bit for bit the reference's result.  An unknown type returns
+ * FMM_ERR_INVALID_ARGUMENT (the reference throws "Unknown iteration type."). */
+fmm_status fmm_diagonal_scaling(fmm_handle h, double* A, int64_t lda, double* B, int64_t ldb, int64_t m, int64_t k,
+                                int64_t n, int num_steps, int type, double* r, double* s);
+
+/* C(i, j) := (C(i, j) * r[i]) * s[j] on the handle's stream, replacing
+ * PostProcessScaling(C, r_vals, s_vals) (scaling/scaling.hpp:143-148): the
+ * product of the scaled operands back to the product of the originals. */
+fmm_status fmm_scaling_postprocess(fmm_handle h, double* C, int64_t ldc, int64_t m, int64_t n, const double* r,
+                                   const double* s);
+
 /* Waits for all work queued on the handle's stream.  FMM_ERR_TIMEOUT if a
  * tensor-core kernel of a split-BF16 product gave up one of its bounded
  * waits since the last check (its results are then not valid). */
