@@ -157,6 +157,12 @@ SIGNATURES = {
                                              ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]),
     "fmm_scaling_postprocess": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
                                                 ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p]),
+    "fmm_diagonal_scaling_host": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+                                                  ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
+                                                  ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]),
+    "fmm_scaling_postprocess_host": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                                     ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p,
+                                                     ctypes.c_void_p]),
     "fmm_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
     "fmm_kernel_launch_count": (ctypes.c_int64, [ctypes.c_void_p]),
     "fmm_selftest_wait_timeout": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.POINTER(ctypes.c_int)]),

@@ -302,11 +302,15 @@ _SCALING_TYPES = {"outside_inside": OUTSIDE_INSIDE, "inside_outside": INSIDE_OUT
                   "outside": OUTSIDE}
 
 
-def diagonal_scaling(A, B, num_steps: int, scaling_type=OUTSIDE_INSIDE, handle: Optional[Handle] = None):
+def diagonal_scaling(A, B, num_steps: int, scaling_type=OUTSIDE_INSIDE, r_vals=None, s_vals=None,
+                     handle: Optional[Handle] = None):
     """Scaling(A, B, num_steps, r_vals, s_vals, scaling_type)
     (scaling/scaling.hpp:153-196): scales the device matrices A and B in
     place and returns the factors (r_vals, s_vals) as device tensors, for
-    scaling_postprocess.  scaling_type is 0..3 or its name."""
+    scaling_postprocess.  scaling_type is 0..3 or its name.  Given r_vals /
+    s_vals (float64 device vectors of length m / n) are updated in place and
+    returned, as the reference multiplies into vectors that arrive sized;
+    otherwise fresh vectors of ones are used."""
     torch = _torch()
     m, k = A.shape
     n = B.shape[1]
@@ -315,8 +319,11 @@ def diagonal_scaling(A, B, num_steps: int, scaling_type=OUTSIDE_INSIDE, handle: 
         raise ValueError("Unknown iteration type.")
     pa, lda = _mat(A, m, k, "A")
     pb, ldb = _mat(B, k, n, "B")
-    r = torch.empty(m, dtype=torch.float64, device=A.device)
-    s = torch.empty(n, dtype=torch.float64, device=A.device)
+    r = torch.ones(m, dtype=torch.float64, device=A.device) if r_vals is None else r_vals
+    s = torch.ones(n, dtype=torch.float64, device=A.device) if s_vals is None else s_vals
+    for v, size, name in ((r, m, "r_vals"), (s, n, "s_vals")):
+        if v.dtype != torch.float64 or tuple(v.shape) != (size,) or (size > 1 and v.stride(0) != 1):
+            raise ValueError("%s must be a contiguous float64 vector of length %d" % (name, size))
     h = handle or default_handle(A.device.index)
     check(lib().fmm_diagonal_scaling(h.ptr, pa, lda, pb, ldb, m, k, n, num_steps, int(kind), r.data_ptr(),
                                      s.data_ptr()))

@@ -594,6 +594,90 @@ fmm_status fmm_scaling_postprocess(fmm_handle h, double* C, int64_t ldc, int64_t
   return FMM_OK;
 }
 
+fmm_status fmm_diagonal_scaling_host(fmm_handle h, double* A, int64_t lda, double* B, int64_t ldb, int64_t m,
+                                     int64_t k, int64_t n, int num_steps, int type, double* r, double* s) {
+  if (!h) return fail(FMM_ERR_INVALID_ARGUMENT, "null handle");
+  fmm_status st = check_dims(m, k, n, lda, ldb, m > 1 ? m : 1);
+  if (st != FMM_OK) return st;
+  if ((m > 0 && !r) || (n > 0 && !s)) return fail(FMM_ERR_INVALID_ARGUMENT, "null factor pointer");
+  if ((m * k > 0 && !A) || (k * n > 0 && !B)) return fail(FMM_ERR_INVALID_ARGUMENT, "null matrix pointer");
+  DeviceGuard g(h->device);
+  if (!g.ok()) return fail(FMM_ERR_CUDA, "cudaSetDevice failed");
+  auto pad = [](size_t v) { return (v + 31) & ~(size_t)31; };
+  const size_t na = (size_t)m * (size_t)k, nb = (size_t)k * (size_t)n;
+  void* io = h->io;
+  size_t cap = h->io_cap;
+  if ((st = ensure_device_buffer(h, &io, &cap, (pad(na) + pad(nb) + pad(m) + pad(n)) * sizeof(double),
+                                 "host-call operands")) != FMM_OK)
+    return st;
+  h->io = static_cast<double*>(io);
+  h->io_cap = cap;
+  double* dA = h->io;
+  double* dB = dA + pad(na);
+  double* dr = dB + pad(nb);
+  double* ds = dr + pad(m);
+  const int64_t ldA = m > 1 ? m : 1, ldB = k > 1 ? k : 1;
+  if (na)
+    FMM_CUDA_TRY(cudaMemcpy2DAsync(dA, ldA * sizeof(double), A, lda * sizeof(double), m * sizeof(double), k,
+                                   cudaMemcpyHostToDevice, h->stream),
+                 "copy A to device");
+  if (nb)
+    FMM_CUDA_TRY(cudaMemcpy2DAsync(dB, ldB * sizeof(double), B, ldb * sizeof(double), k * sizeof(double), n,
+                                   cudaMemcpyHostToDevice, h->stream),
+                 "copy B to device");
+  if (m) FMM_CUDA_TRY(cudaMemcpyAsync(dr, r, m * sizeof(double), cudaMemcpyHostToDevice, h->stream), "copy r");
+  if (n) FMM_CUDA_TRY(cudaMemcpyAsync(ds, s, n * sizeof(double), cudaMemcpyHostToDevice, h->stream), "copy s");
+  st = fmm_diagonal_scaling(h, dA, ldA, dB, ldB, m, k, n, num_steps, type, dr, ds);
+  if (st != FMM_OK) return st;
+  if (na)
+    FMM_CUDA_TRY(cudaMemcpy2DAsync(A, lda * sizeof(double), dA, ldA * sizeof(double), m * sizeof(double), k,
+                                   cudaMemcpyDeviceToHost, h->stream),
+                 "copy A to host");
+  if (nb)
+    FMM_CUDA_TRY(cudaMemcpy2DAsync(B, ldb * sizeof(double), dB, ldB * sizeof(double), k * sizeof(double), n,
+                                   cudaMemcpyDeviceToHost, h->stream),
+                 "copy B to host");
+  if (m) FMM_CUDA_TRY(cudaMemcpyAsync(r, dr, m * sizeof(double), cudaMemcpyDeviceToHost, h->stream), "copy r back");
+  if (n) FMM_CUDA_TRY(cudaMemcpyAsync(s, ds, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream), "copy s back");
+  FMM_CUDA_TRY(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+  return FMM_OK;
+}
+
+fmm_status fmm_scaling_postprocess_host(fmm_handle h, double* C, int64_t ldc, int64_t m, int64_t n, const double* r,
+                                        const double* s) {
+  if (!h) return fail(FMM_ERR_INVALID_ARGUMENT, "null handle");
+  fmm_status st = check_dims(m, 0, n, m > 1 ? m : 1, 1, ldc);
+  if (st != FMM_OK) return st;
+  if (m == 0 || n == 0) return FMM_OK;
+  if (!C || !r || !s) return fail(FMM_ERR_INVALID_ARGUMENT, "null pointer");
+  DeviceGuard g(h->device);
+  if (!g.ok()) return fail(FMM_ERR_CUDA, "cudaSetDevice failed");
+  auto pad = [](size_t v) { return (v + 31) & ~(size_t)31; };
+  const size_t nc = (size_t)m * (size_t)n;
+  void* io = h->io;
+  size_t cap = h->io_cap;
+  if ((st = ensure_device_buffer(h, &io, &cap, (pad(nc) + pad(m) + pad(n)) * sizeof(double),
+                                 "host-call operands")) != FMM_OK)
+    return st;
+  h->io = static_cast<double*>(io);
+  h->io_cap = cap;
+  double* dC = h->io;
+  double* dr = dC + pad(nc);
+  double* ds = dr + pad(m);
+  FMM_CUDA_TRY(cudaMemcpy2DAsync(dC, m * sizeof(double), C, ldc * sizeof(double), m * sizeof(double), n,
+                                 cudaMemcpyHostToDevice, h->stream),
+               "copy C to device");
+  FMM_CUDA_TRY(cudaMemcpyAsync(dr, r, m * sizeof(double), cudaMemcpyHostToDevice, h->stream), "copy r");
+  FMM_CUDA_TRY(cudaMemcpyAsync(ds, s, n * sizeof(double), cudaMemcpyHostToDevice, h->stream), "copy s");
+  st = fmm_scaling_postprocess(h, dC, m, m, n, dr, ds);
+  if (st != FMM_OK) return st;
+  FMM_CUDA_TRY(cudaMemcpy2DAsync(C, ldc * sizeof(double), dC, m * sizeof(double), m * sizeof(double), n,
+                                 cudaMemcpyDeviceToHost, h->stream),
+               "copy C to host");
+  FMM_CUDA_TRY(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+  return FMM_OK;
+}
+
 fmm_status fmm_synchronize(fmm_handle h) {
   if (!h) return fail(FMM_ERR_INVALID_ARGUMENT, "null handle");
   DeviceGuard g(h->device);

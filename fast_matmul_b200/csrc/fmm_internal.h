@@ -154,7 +154,7 @@ cudaError_t combine_launch(int alg, const CombineLaunch& L, const CoefSlots& cf,
 size_t scaling_scratch_bytes(int64_t m, int64_t k, int64_t n);
 // Scales A (m x k) and B (k x n) in place, `num_steps` steps of scaling
 // `type` (0 outside-inside, 1 inside-outside, 2 inside, 3 outside), and
-// writes the row factors r (m) and column factors s (n).
+// multiplies the row factors into r (m) and the column factors into s (n).
 cudaError_t scaling_launch(double* A, int64_t lda, double* B, int64_t ldb, int m, int k, int n, int num_steps,
                            int type, double* r, double* s, void* scratch, cudaStream_t stream, int64_t* launches);
 // C(i,j) = (C(i,j) * r[i]) * s[j].

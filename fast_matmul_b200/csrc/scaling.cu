@@ -157,17 +157,13 @@ __global__ void scale_factors_kernel(Factors F) {
   if (t < F.n) F.col_b[t] = 0ull;
 }
 
-// r = s = 1 (Scaling, scaling.hpp:158-159) and every maximum cleared.
+// Every maximum cleared.  r and s keep the caller's starting values
+// (Scaling's resize(m, 1.0), scaling.hpp:158-159, keeps the entries of
+// vectors that arrive sized).
 __global__ void scale_init_kernel(Factors F) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < F.m) {
-    F.r[t] = 1.0;
-    F.row_a[t] = 0ull;
-  }
-  if (t < F.n) {
-    F.s[t] = 1.0;
-    F.col_b[t] = 0ull;
-  }
+  if (t < F.m) F.row_a[t] = 0ull;
+  if (t < F.n) F.col_b[t] = 0ull;
   if (t < F.k) {
     F.col_a[t] = 0ull;
     F.row_b[t] = 0ull;

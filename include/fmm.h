@@ -177,8 +177,10 @@ enum {
  * Scaling<double>(A, B, num_steps, r_vals, s_vals, scaling_type)
  * (scaling/scaling.hpp:153-196).  A (m x k) and B (k x n), device
  * matrices, are scaled in place on the handle's stream; r (m) and s (n),
- * device arrays, are overwritten with the row and column factors (the
- * reference resizes fresh vectors to 1 and multiplies the outer maxima in).
+ * device arrays, are in/out: the outer maxima are multiplied into their
+ * entries (UpdateVals, scaling.hpp:93-98).  Fill them with 1 for the
+ * reference's fresh vectors (its resize(m, 1.0) keeps the entries of
+ * vectors that arrive sized).
  * Each step is an outer scaling (rows of A by 1 / max|A(i,:)|, columns of B
  * by 1 / max|B(:,j)|) and/or an inner scaling (columns of A by 1 / z_l and
  * rows of B by z_l, z_l = sqrt(max|A(:,l)| / max|B(l,:)|)) in the order of
@@ -192,6 +194,15 @@ fmm_status fmm_diagonal_scaling(fmm_handle h, double* A, int64_t lda, double* B,
  * product of the scaled operands back to the product of the originals. */
 fmm_status fmm_scaling_postprocess(fmm_handle h, double* C, int64_t ldc, int64_t m, int64_t n, const double* r,
                                    const double* s);
+
+/* The two calls above with HOST matrices and factor vectors (copied in,
+ * scaled on the device, copied back; they return when the results are on
+ * the host): Scaling / PostProcessScaling over host buffers, for the C++
+ * adapter (include/fmm/scaling.hpp). */
+fmm_status fmm_diagonal_scaling_host(fmm_handle h, double* A, int64_t lda, double* B, int64_t ldb, int64_t m,
+                                     int64_t k, int64_t n, int num_steps, int type, double* r, double* s);
+fmm_status fmm_scaling_postprocess_host(fmm_handle h, double* C, int64_t ldc, int64_t m, int64_t n, const double* r,
+                                        const double* s);
 
 /* Waits for all work queued on the handle's stream.  FMM_ERR_TIMEOUT if a
  * tensor-core kernel of a split-BF16 product gave up one of its bounded

@@ -464,9 +464,11 @@ static void o_inner(double* a, long lda, double* b, long ldb, int m, int k, int 
   o_row_scale(b, ldb, k, n, z);
 }
 
-/* Scaling (:150-194) with type 0 OUTSIDE_INSIDE, 1 INSIDE_OUTSIDE, 2 INSIDE,
- * 3 OUTSIDE; r (m) and s (n) start at 1 and collect the outer maxima
- * (UpdateVals, :93-98).  Returns -1 for an unknown type. */
+/* Scaling (:153-196) with type 0 OUTSIDE_INSIDE, 1 INSIDE_OUTSIDE, 2 INSIDE,
+ * 3 OUTSIDE.  r (m) and s (n) hold their starting values (resize(m, 1.0) at
+ * :158-159 keeps the entries of vectors that arrive sized; fresh vectors are
+ * all 1) and collect the outer maxima (UpdateVals, :93-98).  Returns -1 for
+ * an unknown type. */
 int oracle_scaling(double* a, long lda, double* b, long ldb, int m, int k, int n, int num_steps, int type, double* r,
                    double* s) {
   const int big = (m > n ? m : n) > k ? (m > n ? m : n) : k;
@@ -475,8 +477,6 @@ int oracle_scaling(double* a, long lda, double* b, long ldb, int m, int k, int n
   double* t1 = (double*)malloc(sizeof(double) * (size_t)(big > 0 ? big : 1));
   double* t2 = (double*)malloc(sizeof(double) * (size_t)(k > 0 ? k : 1));
   int step, i, rc = 0;
-  for (i = 0; i < m; ++i) r[i] = 1.0;
-  for (i = 0; i < n; ++i) s[i] = 1.0;
   if (type < 0 || type > 3) rc = -1;
   for (step = 0; rc == 0 && step < num_steps; ++step) {
     if (type == 1 || type == 2) o_inner(a, lda, b, ldb, m, k, n, t1, t2);

@@ -198,14 +198,15 @@ def quad_errors(A: np.ndarray, B: np.ndarray, rows, cols, values) -> tuple:
     return mr.value, ms.value
 
 
-def scaling(A: np.ndarray, B: np.ndarray, num_steps: int, kind: int, ref: bool = False):
+def scaling(A: np.ndarray, B: np.ndarray, num_steps: int, kind: int, ref: bool = False, r=None, s=None):
     """Scaling<double>(A, B, num_steps, r, s, kind) (scaling/scaling.hpp) on
-    Fortran-ordered A, B in place; returns (r, s).  ref=True runs the
+    Fortran-ordered A, B in place; returns (r, s), which start as the given
+    vectors (fresh vectors of ones by default).  ref=True runs the
     reference's own header through the reference build."""
     m, k = A.shape
     n = B.shape[1]
-    r = np.empty(m)
-    s = np.empty(n)
+    r = np.ones(m) if r is None else np.array(r, dtype=np.float64)
+    s = np.ones(n) if s is None else np.array(s, dtype=np.float64)
     if ref:
         ref_lib().fmmref_scaling(_p(A), max(m, 1), _p(B), max(k, 1), m, k, n, num_steps, kind,
                                  r.ctypes.data_as(_P), s.ctypes.data_as(_P))

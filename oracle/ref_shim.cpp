@@ -157,12 +157,13 @@ void fmmref_matmul(double* a, int lda, double* b, int ldb, double* c, int ldc, i
 
 // Scaling<double>(A, B, num_steps, r_vals, s_vals, type) from
 // scaling/scaling.hpp on caller buffers (A m x k, B k x n scaled in place);
-// r (m) and s (n) receive the factors.
+// r (m) and s (n) are in/out: they arrive as vectors of the right size, which
+// Scaling's resize(m, 1.0) keeps, and receive the factors multiplied in.
 void fmmref_scaling(double* a, int lda, double* b, int ldb, int m, int k, int n, int num_steps, int type, double* r,
                     double* s) {
   Matrix<double> A(a, lda, m, k);
   Matrix<double> B(b, ldb, k, n);
-  std::vector<double> rv, sv;
+  std::vector<double> rv(r, r + m), sv(s, s + n);
   Scaling<double>(A, B, num_steps, rv, sv, type);
   for (int i = 0; i < m; ++i) r[i] = rv[i];
   for (int j = 0; j < n; ++j) s[j] = sv[j];

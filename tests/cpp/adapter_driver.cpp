@@ -1,11 +1,14 @@
 // Drop-in check of the C++ surface: a driver written against the
 // reference's API (RunAlgorithm, <ns>::FastMatmul, MatMul, MaxRelativeDiff,
-// RandomMatrix) built unchanged against include/fmm and libfmm.so.
+// RandomMatrix, Scaling / PostProcessScaling) built unchanged against
+// include/fmm and libfmm.so.
 // Exit status 0 when every error is within its bound.
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 
 #include "fmm/all_algorithms.hpp"
+#include "fmm/scaling.hpp"
 
 static int failures = 0;
 
@@ -64,6 +67,33 @@ int main() {
     strassen::FastMatmul(A11, B12, C1v, 2);
     MatMul(A11, B12, C2v);
     expect(MaxRelativeDiff(C1v, C2v) <= 1e-13, "strassen on strided views max rel diff", MaxRelativeDiff(C1v, C2v));
+  }
+  // diagonal scaling (benchmarks/scaling_stability.cpp pattern): rows of A
+  // and columns of B skewed by 2^-30..2^30; scaled Strassen back within the
+  // classical product's error
+  {
+    Matrix<double> A = RandomMatrix<double>(512, 384);
+    Matrix<double> B = RandomMatrix<double>(384, 448);
+    for (int j = 0; j < A.n(); ++j)
+      for (int i = 0; i < A.m(); ++i) A(i, j) = std::ldexp(A(i, j), i % 3 == 0 ? 30 : (i % 3 == 1 ? -30 : 0));
+    for (int j = 0; j < B.n(); ++j)
+      for (int i = 0; i < B.m(); ++i) B(i, j) = std::ldexp(B(i, j), j % 2 == 0 ? -30 : 30);
+    Matrix<double> C1(512, 448), C2(512, 448);
+    MatMul(A, B, C1);
+    Matrix<double> As = A, Bs = B;
+    std::vector<double> r_vals, s_vals;
+    Scaling(As, Bs, 5, r_vals, s_vals, OUTSIDE_INSIDE);
+    strassen::FastMatmul(As, Bs, C2, 2);
+    PostProcessScaling(C2, r_vals, s_vals);
+    expect(r_vals.size() == 512 && s_vals.size() == 448, "Scaling factor vector sizes", (double)r_vals.size());
+    expect(MaxRelativeDiff(C1, C2) <= 1e-13, "Scaling + strassen + PostProcessScaling", MaxRelativeDiff(C1, C2));
+    bool threw = false;
+    try {
+      Scaling(As, Bs, 1, r_vals, s_vals, 9);
+    } catch (const std::runtime_error&) {
+      threw = true;
+    }
+    expect(threw, "unknown scaling type throws", 0.0);
   }
   std::printf("%s\n", failures ? "FAILED" : "PASSED");
   return failures ? 1 : 0;

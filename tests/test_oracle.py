@@ -177,3 +177,18 @@ def test_scaling_restatement_equals_reference_bit_for_bit(kind):
         assert np.array_equal(C1, C2)
         # the unscaled product is recovered (up to rounding)
         assert np.abs(C1 - A @ B).max() <= 1e-13 * np.abs(A @ B).max()
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference build not present")
+def test_scaling_multiplies_into_vectors_that_arrive_sized():
+    """Scaling's r_vals.resize(m, 1.0) keeps the entries of vectors that
+    arrive sized; the outer maxima are multiplied into them."""
+    A = scaled_normal(20, 30, 1, "row")
+    B = scaled_normal(30, 25, 2, "col")
+    r0 = np.linspace(0.5, 3.0, 20)
+    s0 = np.linspace(1.5, 0.25, 25)
+    A1, B1, A2, B2 = A.copy(order="F"), B.copy(order="F"), A.copy(order="F"), B.copy(order="F")
+    r1, s1 = oracle.scaling(A1, B1, 2, 0, r=r0, s=s0)
+    r2, s2 = oracle.scaling(A2, B2, 2, 0, ref=True, r=r0, s=s0)
+    assert np.array_equal(r1, r2) and np.array_equal(s1, s2)
+    assert not np.array_equal(r1, oracle.scaling(A.copy(order="F"), B.copy(order="F"), 2, 0)[0])
