@@ -57,10 +57,33 @@ ScaleJob make_job(double* X, int64_t ld, int rows, int cols, const double* rowv,
   return j;
 }
 
-__device__ __forceinline__ double warp_max(double v) {
+// Maxima over the 32 lanes of a warp of 8 columns at once (a[u] = |X| of
+// column u in this lane's row), by recursive halving: at lane distance 16
+// each lane keeps 4 of the columns and trades the other 4, at 8 it keeps 2,
+// at 4 one, then two plain steps.  9 shuffles instead of 8 x 5.  Returns the
+// maximum of column column_of_lane(lane), valid in lanes with lane % 4 == 0.
+__device__ __forceinline__ double warp_max8(const double (&a)[8], int lane) {
+  const bool h16 = lane & 16, h8 = lane & 8, h4 = lane & 4;
+  double b4[4], b2[2];
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-  return v;
+  for (int j = 0; j < 4; ++j) {
+    const double keep = h16 ? a[j + 4] : a[j];
+    const double send = h16 ? a[j] : a[j + 4];
+    b4[j] = fmax(keep, __shfl_xor_sync(0xffffffffu, send, 16));
+  }
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    const double keep = h8 ? b4[j + 2] : b4[j];
+    const double send = h8 ? b4[j] : b4[j + 2];
+    b2[j] = fmax(keep, __shfl_xor_sync(0xffffffffu, send, 8));
+  }
+  double b = fmax(h4 ? b2[1] : b2[0], __shfl_xor_sync(0xffffffffu, h4 ? b2[0] : b2[1], 4));
+  b = fmax(b, __shfl_xor_sync(0xffffffffu, b, 2));
+  return fmax(b, __shfl_xor_sync(0xffffffffu, b, 1));
+}
+
+__device__ __forceinline__ int column_of_lane(int lane) {
+  return ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
 }
 
 // Blocks [0, j0.tiles) work on j0, the rest on j1.  A tile is kRows rows x
@@ -84,22 +107,24 @@ __global__ void __launch_bounds__(kRows) scale_reduce_kernel(ScaleJob j0, ScaleJ
   double* p = J.X + (in ? i : 0) + (int64_t)c0 * J.ld;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double rmax = 0.0;
+  static_assert(kUnroll == 8, "warp_max8 reduces 8 columns");
   for (int cb = 0; cb < nc; cb += kUnroll) {
-    double v[kUnroll];
+    double v[kUnroll], a[kUnroll];
+    double* q = p + (int64_t)cb * J.ld;
 #pragma unroll
-    for (int u = 0; u < kUnroll; ++u) v[u] = (in && cb + u < nc) ? p[(int64_t)(cb + u) * J.ld] : 0.0;
+    for (int u = 0; u < kUnroll; ++u) v[u] = (in && cb + u < nc) ? q[(int64_t)u * J.ld] : 0.0;
 #pragma unroll
     for (int u = 0; u < kUnroll; ++u) {
       const int c = cb + u;
       if (J.rowv) v[u] = v[u] * rv;
       if (J.colv) v[u] = v[u] * s_colv[c];
-      if (scales && in && c < nc) p[(int64_t)c * J.ld] = v[u];
-      const double a = fabs(v[u]);
-      rmax = fmax(rmax, a);
-      if (J.colmax) {
-        const double w = warp_max(a);
-        if (lane == 0) s_part[warp][c] = w;
-      }
+      if (scales && in && c < nc) q[(int64_t)u * J.ld] = v[u];
+      a[u] = fabs(v[u]);
+      rmax = fmax(rmax, a[u]);
+    }
+    if (J.colmax) {
+      const double w = warp_max8(a, lane);
+      if ((lane & 3) == 0) s_part[warp][cb + column_of_lane(lane)] = w;
     }
   }
   if (J.rowmax && in && rmax > 0.0) atomicMax(&J.rowmax[i], (unsigned long long)__double_as_longlong(rmax));
