@@ -268,3 +268,149 @@ def load_all(coeff_root: str) -> Dict[str, AlgorithmSpec]:
     for name, header, source, dims in ALGORITHM_TABLE:
         out[name] = load_algorithm(os.path.join(coeff_root, source), name, header, source, dims)
     return out
+
+
+# ---------------------------------------------------------------------------
+# Checks and counts for coefficient files (CI tooling for new algorithms)
+
+
+def as_record(spec: AlgorithmSpec) -> dict:
+    """The fields of an algorithm record in generated/algorithms.json that
+    the checks below read."""
+    return {"name": spec.name, "m0": spec.m0, "k0": spec.k0, "n0": spec.n0, "rank": spec.rank,
+            "raw": {"U": spec.U, "V": spec.V, "W": spec.W, "SX": spec.SX, "TX": spec.TX, "MX": spec.MX}}
+
+
+def coefficient_value(text: str, x=None):
+    """Exact rational value of a coefficient, or its value at x for one that
+    depends on the algorithm parameter (the generated C expression, which
+    only uses + - * / on x and double literals, evaluated in Python)."""
+    if is_zero_text(text):
+        return 0
+    frac = rational_value(text)
+    if frac is not None:
+        return frac
+    if x is None:
+        raise ValueError("coefficient %r depends on x" % text)
+    return eval(parse_coeff(text), {"__builtins__": {}}, {"x": x})
+
+
+def effective_uvw(rec: dict, x=None):
+    """U, V, W over the plain blocks with the common-subexpression
+    temporaries substituted (A_X, B_X, M_X rows folded into the products)."""
+    raw = rec["raw"]
+    m0, k0, n0, R = rec["m0"], rec["k0"], rec["n0"], rec["rank"]
+    nA, nB, nC = m0 * k0, k0 * n0, m0 * n0
+    val = lambda t: coefficient_value(t, x)  # noqa: E731
+    U = [[val(raw["U"][i][r]) for r in range(R)] for i in range(nA)]
+    V = [[val(raw["V"][i][r]) for r in range(R)] for i in range(nB)]
+    W = [[val(raw["W"][c][r]) for r in range(R)] for c in range(nC)]
+    for xi, row in enumerate(raw["SX"]):
+        for r in range(R):
+            u = val(raw["U"][nA + xi][r])
+            if u:
+                for i in range(nA):
+                    U[i][r] += u * val(row[i])
+    for xi, row in enumerate(raw["TX"]):
+        for r in range(R):
+            v = val(raw["V"][nB + xi][r])
+            if v:
+                for i in range(nB):
+                    V[i][r] += v * val(row[i])
+    for xi, row in enumerate(raw["MX"]):
+        for c in range(nC):
+            w = val(raw["W"][c][R + xi])
+            if w:
+                for r in range(R):
+                    W[c][r] += w * val(row[r])
+    return U, V, W
+
+
+def brent_residual(rec: dict, x=None):
+    """max over the Brent equations sum_r U[ik][r] V[k'j][r] W[i'j'][r] =
+    d(i,i') d(k,k') d(j,j') of |lhs - rhs|: exactly 0 (rationals) for an exact
+    algorithm, O(x) for an approximate one evaluated at x (the check of the
+    reference's codegen/verify.py:108-130 and verify2.py:163-319)."""
+    U, V, W = effective_uvw(rec, x)
+    m0, k0, n0, R = rec["m0"], rec["k0"], rec["n0"], rec["rank"]
+    worst = 0
+    for i in range(m0):
+        for k in range(k0):
+            for k2 in range(k0):
+                for j in range(n0):
+                    for i2 in range(m0):
+                        for j2 in range(n0):
+                            s = sum(U[i * k0 + k][r] * V[k2 * n0 + j][r] * W[i2 * n0 + j2][r] for r in range(R))
+                            want = 1 if (i == i2 and k == k2 and j == j2) else 0
+                            worst = max(worst, abs(s - want))
+    return worst
+
+
+def _nonzero(text: str) -> bool:
+    # codegen/gen.py:61-62 of the reference compares the text with '0' and '0.0'
+    return text not in ("0", "0.0")
+
+
+def operation_counts(rec: dict) -> Dict[str, Tuple[int, int, int]]:
+    """Additions, reads and writes of one recursion level, with the
+    definitions of the reference's codegen/counts.py:36-58: per product, its
+    S (T) operand costs nnz - 1 additions, nnz reads and one write when nnz >
+    1 (columns of U, V); per C block the same over its row of W; per
+    common-subexpression temporary nnz - 1 additions, nnz reads, one write.
+    Returns rows A, B, C, AX, BX, CX, xtot, tot."""
+    raw = rec["raw"]
+
+    def base(cols):
+        nnz = [sum(1 for t in col if _nonzero(t)) for col in cols]
+        return (sum(c - 1 for c in nnz), sum(nnz), sum(1 for c in nnz if c > 1))
+
+    def elim(rows):
+        if not rows or any(len(r) == 0 for r in rows):
+            return (0, 0, 0)
+        nnz = [sum(1 for t in row if _nonzero(t)) for row in rows]
+        return (sum(c - 1 for c in nnz), sum(nnz), len(rows))
+
+    transpose = lambda m: [list(c) for c in zip(*m)] if m else []  # noqa: E731
+    out = {"A": base(transpose(raw["U"])), "B": base(transpose(raw["V"])), "C": base(raw["W"]),
+           "AX": elim(raw["SX"]), "BX": elim(raw["TX"]), "CX": elim(raw["MX"])}
+    out["xtot"] = tuple(sum(v) for v in zip(out["AX"], out["BX"], out["CX"]))
+    out["tot"] = tuple(sum(v) for v in zip(*(out[k] for k in ("A", "B", "C", "AX", "BX", "CX"))))
+    return out
+
+
+def format_counts(counts: Dict[str, Tuple[int, int, int]]) -> str:
+    lines = ["      +   r   w"]
+    for key in ("A", "B", "C", "AX", "BX", "CX", "xtot", "tot"):
+        lines.append("%-4s %4d %3d %3d" % ((key,) + tuple(counts[key])))
+    return "\n".join(lines)
+
+
+def main(argv=None) -> int:
+    """python coeffs.py counts|verify COEFF_FILE M0,K0,N0
+
+    counts  additions / reads / writes of one level (A, B, C, temporaries)
+    verify  Brent equations: exit 0 when an exact algorithm satisfies them
+            exactly, or an approximate one converges as x -> 0"""
+    import sys
+
+    argv = sys.argv[1:] if argv is None else argv
+    if len(argv) != 3 or argv[0] not in ("counts", "verify"):
+        print(main.__doc__)
+        return 2
+    dims = tuple(int(d) for d in argv[2].split(","))
+    spec = load_algorithm(argv[1], os.path.basename(argv[1]), "", argv[1], dims)
+    rec = as_record(spec)
+    if argv[0] == "counts":
+        print(format_counts(operation_counts(rec)))
+        return 0
+    if not spec.approximate:
+        res = brent_residual(rec)
+        print("exact algorithm: max Brent residual %s" % res)
+        return 0 if res == 0 else 1
+    r1, r2 = brent_residual(rec, 1e-3), brent_residual(rec, 1e-5)
+    print("approximate algorithm: residual %.3e at x = 1e-3, %.3e at x = 1e-5" % (r1, r2))
+    return 0 if r2 < r1 and r2 < 1e-3 else 1
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -46,59 +46,7 @@ def test_parse_coeff_rejects_garbage():
         coeffs.parse_coeff("3x3x3")
 
 
-def _value(text, x):
-    if coeffs.is_zero_text(text):
-        return 0
-    frac = coeffs.rational_value(text)
-    if frac is not None:
-        return frac
-    return eval(coeffs.parse_coeff(text), {"__builtins__": {}}, {"x": x})  # generated C-like expression
-
-
-def effective_uvw(a, x=None):
-    """U, V, W over the plain blocks with the CSE temporaries substituted."""
-    raw = a["raw"]
-    m0, k0, n0, R = a["m0"], a["k0"], a["n0"], a["rank"]
-    nA, nB, nC = m0 * k0, k0 * n0, m0 * n0
-    val = lambda t: _value(t, x)
-    U = [[val(raw["U"][i][r]) for r in range(R)] for i in range(nA)]
-    V = [[val(raw["V"][i][r]) for r in range(R)] for i in range(nB)]
-    W = [[val(raw["W"][c][r]) for r in range(R)] for c in range(nC)]
-    for xi, row in enumerate(raw["SX"]):
-        for r in range(R):
-            u = val(raw["U"][nA + xi][r])
-            if u:
-                for i in range(nA):
-                    U[i][r] += u * val(row[i])
-    for xi, row in enumerate(raw["TX"]):
-        for r in range(R):
-            v = val(raw["V"][nB + xi][r])
-            if v:
-                for i in range(nB):
-                    V[i][r] += v * val(row[i])
-    for xi, row in enumerate(raw["MX"]):
-        for c in range(nC):
-            w = val(raw["W"][c][R + xi])
-            if w:
-                for r in range(R):
-                    W[c][r] += w * val(row[r])
-    return U, V, W
-
-
-def brent_residual(a, x=None):
-    U, V, W = effective_uvw(a, x)
-    m0, k0, n0, R = a["m0"], a["k0"], a["n0"], a["rank"]
-    worst = 0
-    for i in range(m0):
-        for k in range(k0):
-            for k2 in range(k0):
-                for j in range(n0):
-                    for i2 in range(m0):
-                        for j2 in range(n0):
-                            s = sum(U[i * k0 + k][r] * V[k2 * n0 + j][r] * W[i2 * n0 + j2][r] for r in range(R))
-                            want = 1 if (i == i2 and k == k2 and j == j2) else 0
-                            worst = max(worst, abs(s - want))
-    return worst
+brent_residual = coeffs.brent_residual
 
 
 EXACT = [a for a in ALGS if not a["approximate"]]
@@ -173,3 +121,46 @@ def test_generated_files_are_current():
                     "fast_matmul_b200/generated/algorithms.json"):
             with open(os.path.join(tmp, rel)) as a, open(os.path.join(REPO, rel)) as b:
                 assert a.read() == b.read(), rel
+
+
+def test_operation_counts_of_grey333_23_125_match_the_reference_example():
+    """The example output in the docstring of the reference's
+    codegen/counts.py:15-28 for algorithms/eliminated/grey333-23-125."""
+    alg = next(a for a in ALGS if a["name"] == "grey333_23_125")
+    c = coeffs.operation_counts(alg)
+    assert c["A"] == (12, 35, 10) and c["B"] == (11, 34, 10) and c["C"] == (29, 38, 9)
+    assert c["AX"] == (6, 12, 6) and c["BX"] == (7, 14, 7) and c["CX"] == (5, 10, 5)
+    assert c["tot"] == (70, 143, 47)
+
+
+def test_strassen_has_eighteen_additions():
+    c = coeffs.operation_counts(next(a for a in ALGS if a["name"] == "strassen"))
+    assert c["A"] == (5, 12, 5) and c["B"] == (5, 12, 5) and c["C"] == (8, 12, 4)
+    assert c["tot"][0] == 18 and c["xtot"] == (0, 0, 0)
+
+
+def test_counts_and_verify_command_line(tmp_path):
+    """python coeffs.py counts|verify FILE M0,K0,N0 on a coefficient file
+    written from the generated tables (the reference tree is not needed)."""
+    script = os.path.join(REPO, "fast_matmul_b200", "codegen", "coeffs.py")
+    for name in ("strassen", "grey333_23_125", "bini322_10_52_approx"):
+        alg = next(a for a in ALGS if a["name"] == name)
+        raw = alg["raw"]
+        path = tmp_path / name
+        secs = [raw["U"], raw["V"], raw["W"]] + ([raw["SX"], raw["TX"], raw["MX"]] if raw["SX"] else [])
+        path.write_text("\n#\n".join("\n".join(" ".join(r) for r in sec) for sec in secs) + "\n")
+        dims = "%d,%d,%d" % (alg["m0"], alg["k0"], alg["n0"])
+        out = subprocess.run([sys.executable, script, "counts", str(path), dims], capture_output=True, text=True)
+        assert out.returncode == 0, out.stderr
+        tot = coeffs.operation_counts(alg)["tot"]
+        assert out.stdout.strip().splitlines()[-1].split()[1:] == [str(v) for v in tot]
+        out = subprocess.run([sys.executable, script, "verify", str(path), dims], capture_output=True, text=True)
+        assert out.returncode == 0, out.stdout + out.stderr
+    # a broken algorithm fails verification
+    alg = next(a for a in ALGS if a["name"] == "strassen")
+    U = [row[:] for row in alg["raw"]["U"]]
+    U[0][0] = "-1"
+    path = tmp_path / "broken"
+    path.write_text("\n#\n".join("\n".join(" ".join(r) for r in sec) for sec in (U, alg["raw"]["V"], alg["raw"]["W"])) + "\n")
+    out = subprocess.run([sys.executable, script, "verify", str(path), "2,2,2"], capture_output=True, text=True)
+    assert out.returncode == 1, out.stdout
