@@ -41,7 +41,8 @@ cudaError_t gemm_launch(const GemmDesc* d_descs, int n, int64_t total_tiles, int
 constexpr int kSplitMinSlices = 2;
 constexpr int kSplitMaxSlices = 6;
 constexpr int kSplitDefaultSlices = 5;
-constexpr int kSplitTile = 128;   // output tile rows and columns
+constexpr int kSplitTile = 128;   // output tile rows of one CTA, and columns
+constexpr int kSplitPairRows = 2 * kSplitTile;  // rows of the tile of a CTA pair (two-SM MMA)
 constexpr int kSplitKBlock = 64;  // k-depth of one TMA box (128 bytes of BF16)
 constexpr int kSplitChunk = 128;  // k-depth accumulated exactly in FP32 (two k-blocks)
 
@@ -53,8 +54,8 @@ struct SplitDesc {
   double alpha, beta;
   int m, n, k;
   int kblocks;          // padded k / kSplitKBlock
-  int tiles_m, tiles_n; // padded m / kSplitTile, padded n / kSplitTile
-  int64_t tile_begin;   // first output tile of this problem
+  int tiles_m, tiles_n; // padded m / kSplitTile (even: m is padded to kSplitPairRows), padded n / kSplitTile
+  int64_t tile_begin;   // first output tile (kSplitPairRows x kSplitTile, one CTA pair) of this problem
   int64_t sa_begin;     // first A-splitting work tile (32 rows x one k-block)
   int64_t a_row;        // first 128-byte row of this problem's A slices
   int64_t b_row;        // first 128-byte row of this problem's B slices
@@ -65,7 +66,7 @@ struct SplitDesc {
 // Scratch layout of one split launch (offsets from the scratch base).
 struct SplitPlan {
   int slices = 0;
-  int64_t tiles = 0;     // output tiles over all problems
+  int64_t tiles = 0;     // output tiles (one per CTA pair) over all problems
   int64_t sa_work = 0;   // A-splitting work tiles
   int64_t rows_a = 0, rows_b = 0;  // 128-byte slice rows
   int64_t n_e = 0, n_f = 0;        // row / column exponents

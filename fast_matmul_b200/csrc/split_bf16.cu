@@ -18,15 +18,22 @@
 // Error: |x - sum_t d_t 2^-8t| <= 2^-(8S+1) 2^e per operand entry plus the
 // dropped diagonals, so |C - AB| <~ 3 * 2^-8S * k * max|a_i.| * max|b_.j|.
 //
-// Product kernel: persistent CTAs over the 128 x 128 output tiles of every
-// problem.  Warp 0 issues TMA loads of (A_t, B_u) over one 128-deep chunk
-// (64 KB) into a 3-stage ring, warp 1 issues 8 tcgen05.mma (M128 N128 K16)
-// per stage -- few waits and commits per MMA keep the single issuing thread
-// ahead of the tensor pipe -- into one of four TMEM accumulators of 128 FP32
-// columns, warps 2-9 (two warpgroups of 64
-// columns) drain each finished accumulator into FP64 registers.  Every
-// mbarrier wait is bounded; on a timeout the kernel records a code in *err,
-// lets its copies and MMAs in flight finish, frees its TMEM and returns.
+// Product kernel: persistent CTA pairs (clusters of 2) over the 256 x 128
+// output tiles of every problem, with the two-SM MMA: one thread of the
+// pair leader issues tcgen05.mma.cta_group::2 (M256 N128 K16), which reads
+// A rows 0-127 and B columns 0-63 from the leader's shared memory, A rows
+// 128-255 and B columns 64-127 from the peer's, and accumulates each CTA's
+// 128 rows in its own tensor memory.  One issuing thread thus drives two
+// SMs, halving the per-MMA issue work (the limit of the one-SM form) and the
+// B traffic per SM.  In each CTA warp 0 issues TMA loads of its halves of
+// (A_t, B_u) over one 128-deep chunk (48 KB) into a 4-stage ring, counted on
+// the leader's full barrier; the leader's warp 1 issues 8 MMAs per stage
+// into one of four TMEM accumulators of 128 FP32 columns and multicasts its
+// commits to both CTAs; warps 2-9 of each CTA (two warpgroups of 64
+// columns) drain each finished accumulator into FP64 registers and release
+// it on the leader's barrier.  Every mbarrier wait is bounded; on a timeout
+// the kernel records a code in *err, lets its copies and MMAs in flight
+// finish, frees its TMEM and returns.
 
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -43,22 +50,24 @@ namespace {
 
 using namespace sm100;
 
-constexpr int kBM = kSplitTile, kBN = kSplitTile, kBK = kSplitKBlock;
+constexpr int kBM = kSplitTile, kBN = kSplitTile, kBK = kSplitKBlock;  // per CTA: 128 rows, all 128 columns
+constexpr int kBHalf = kBN / 2;                    // columns of B held by each CTA of the pair
 constexpr int kChunkBlocks = kSplitChunk / kBK;    // 64-deep k-blocks per chunk (2)
-constexpr int kTileBytes = kBM * kBK * 2;          // one 128 x 64 BF16 box: 16 KB
-// Two k-blocks of A and of B per stage (64 KB), 3 stages: measured faster
-// than 7 stages of one k-block (fewer waits and commits per MMA).
+constexpr int kATileBytes = kBM * kBK * 2;         // one 128 x 64 BF16 box: 16 KB
+constexpr int kBTileBytes = kBHalf * kBK * 2;      // one 64 x 64 BF16 box: 8 KB
+// Two k-blocks of A and of the B half per stage (48 KB per CTA), 4 stages.
 constexpr int kStageKBlocks = 2;
-constexpr int kStageBytes = 2 * kStageKBlocks * kTileBytes;
-constexpr int kStages = 3;
+constexpr int kStageBytes = kStageKBlocks * (kATileBytes + kBTileBytes);
+constexpr int kStages = 4;
 constexpr int kAccBufs = 4;  // TMEM accumulators of 128 FP32 columns
+constexpr uint16_t kPairMask = 0x3;  // both CTAs of the cluster
 // TMA warp, MMA warp, 2 x 4 epilogue warps.  Registers are budgeted per
 // group of four warps, so the 10 warps are charged as 12: 168 per thread.
 constexpr int kGemmThreads = 320;
 constexpr size_t kGemmSmem = (size_t)kStages * kStageBytes + 1024;
 static_assert(kChunkBlocks == 2 && kChunkBlocks % kStageKBlocks == 0, "stages tile the chunk");
-static_assert(kBM == kBN, "A and B boxes share the box size");
 static_assert(kBK * 2 == 128, "one k-block row is one 128-byte swizzle row");
+static_assert(kATileBytes % 1024 == 0 && kBTileBytes % 1024 == 0, "128-byte-swizzled tiles start 1024-aligned");
 
 // Largest i in [0, n) with key(d[i]) <= x (keys non-decreasing).
 template <typename Key>
@@ -256,35 +265,43 @@ struct TileCoord {
   int q, tm, tn;
 };
 
-// Tiles of a problem are walked in groups of kRasterRows tile rows, row
-// index fastest within a group: the CTAs of one wave cover a compact block
-// of the output, so the A and B slices they read stay in L2 between them.
-constexpr int kRasterRows = 16;
+// Tiles of a problem (256 x 128, one per CTA pair; tm counts 256-row tiles)
+// are walked in groups of kRasterRows tile rows, row index fastest within a
+// group: the pairs of one wave cover a compact block of the output, so the
+// A and B slices they read stay in L2 between them.
+constexpr int kRasterRows = 8;
 
 __device__ __forceinline__ TileCoord tile_coord(const GemmParams& g, int64_t tile) {
   TileCoord c;
   c.q = find_desc(g.desc, g.nd, tile, [](const SplitDesc& s) { return s.tile_begin; });
   const SplitDesc& s = g.desc[c.q];
+  const int pair_rows = s.tiles_m / 2;
   const int64_t rem = tile - s.tile_begin;
   const int64_t per_group = (int64_t)kRasterRows * s.tiles_n;
   const int64_t group = rem / per_group;
   const int first = (int)(group * kRasterRows);
-  const int rows = s.tiles_m - first < kRasterRows ? s.tiles_m - first : kRasterRows;
+  const int rows = pair_rows - first < kRasterRows ? pair_rows - first : kRasterRows;
   const int64_t local = rem - group * per_group;
   c.tm = first + (int)(local % rows);
   c.tn = (int)(local / rows);
   return c;
 }
 
-__global__ void __launch_bounds__(kGemmThreads, 1)
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
     split_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                       const GemmParams g) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  // full: the leader's count both CTAs' copies of a stage; empty, acc_full:
+  // MMA commits multicast to both CTAs; acc_empty (leader's): 8 epilogue
+  // warps of each CTA
   __shared__ __align__(8) uint64_t full[kStages], empty[kStages], acc_full[kAccBufs], acc_empty[kAccBufs], mma_done;
   __shared__ uint32_t tmem_slot;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int S = g.slices;
+  const uint32_t rank = cluster_ctarank();
+  const bool leader = rank == 0;
+  const int64_t pair = blockIdx.x >> 1, pairs = gridDim.x >> 1;
   if (tid == 0) {
     for (int s = 0; s < kStages; ++s) {
       mbar_init(&full[s], 1);
@@ -292,36 +309,37 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     }
     for (int b = 0; b < kAccBufs; ++b) {
       mbar_init(&acc_full[b], 1);
-      mbar_init(&acc_empty[b], 8);
+      mbar_init(&acc_empty[b], 16);
     }
     mbar_init(&mma_done, 1);
     fence_barrier_init();
   }
-  if (warp == 1) tmem_alloc(&tmem_slot, kAccBufs * kBN);
+  if (warp == 1) tmem_alloc_pair(&tmem_slot, kAccBufs * kBN);
   tc_fence_before();
-  __syncthreads();
+  cluster_sync();  // barriers of both CTAs initialised, tensor memory allocated
   tc_fence_after();
   const uint32_t tmem = tmem_slot;
 
   if (warp == 0) {
     if (lane == 0) {
-      // one stage = one slice product over one 128-deep chunk: A_t and B_u,
-      // two 64-deep k-blocks each (four 16 KB boxes)
+      // one stage = one slice product over one 128-deep chunk: this CTA's
+      // 128 rows of A_t and 64 columns of B_u, two 64-deep k-blocks each
       prefetch_tensormap(&tmA);
       prefetch_tensormap(&tmB);
       uint32_t n = 0, st = 0, ph = 0;  // stages filled, current stage, its round parity
       bool ok = true;
-      for (int64_t tile = blockIdx.x; tile < g.tiles && ok; tile += gridDim.x) {
+      for (int64_t tile = pair; tile < g.tiles && ok; tile += pairs) {
         const TileCoord tc = tile_coord(g, tile);
         const SplitDesc& s = g.desc[tc.q];
         const int64_t mp = (int64_t)s.tiles_m * kBM, np = (int64_t)s.tiles_n * kBN;
-        const int64_t ya_tile = s.a_row + (int64_t)tc.tm * kBM, yb_tile = s.b_row + (int64_t)tc.tn * kBN;
+        const int64_t ya_tile = s.a_row + (int64_t)tc.tm * kSplitPairRows + rank * kBM;
+        const int64_t yb_tile = s.b_row + (int64_t)tc.tn * kBN + rank * kBHalf;
         const int chunks = s.kblocks / kChunkBlocks;
         for (int c = 0; c < chunks && ok; ++c)
           for (int D = 0; D < S && ok; ++D)
             for (int t = 0; t <= D && ok; ++t)
               for (int h = 0; h < kChunkBlocks; h += kStageKBlocks) {
-                if (n >= (uint32_t)kStages && !mbar_wait(&empty[st], ph ^ 1u, g.err, 1)) {
+                if (n >= (uint32_t)kStages && !mbar_wait<true>(&empty[st], ph ^ 1u, g.err, 1)) {
                   ok = false;
                   break;
                 }
@@ -329,12 +347,13 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
                 const int64_t ya = ya_tile + ((int64_t)t * s.kblocks + blk) * mp;
                 const int64_t yb = yb_tile + ((int64_t)(D - t) * s.kblocks + blk) * np;
                 uint8_t* dst = base + st * kStageBytes;
-                uint64_t* bar = &full[st];
-                mbar_arrive_expect_tx(bar, kStageBytes);
+                const uint32_t bar = cluster_addr(&full[st], 0);  // the leader's
+                if (leader) mbar_arrive_expect_tx(&full[st], 2 * kStageBytes);
 #pragma unroll
                 for (int b = 0; b < kStageKBlocks; ++b) {
-                  tma_load_2d(dst + b * kTileBytes, &tmA, bar, 0, (int)(ya + b * mp));
-                  tma_load_2d(dst + (kStageKBlocks + b) * kTileBytes, &tmB, bar, 0, (int)(yb + b * np));
+                  tma_load_2d_pair(dst + b * kATileBytes, &tmA, bar, 0, (int)(ya + b * mp));
+                  tma_load_2d_pair(dst + kStageKBlocks * kATileBytes + b * kBTileBytes, &tmB, bar, 0,
+                                   (int)(yb + b * np));
                 }
                 ++n;
                 if (++st == (uint32_t)kStages) {
@@ -343,24 +362,30 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
                 }
               }
       }
-      // let every copy in flight land before the CTA can exit
+      // Before the CTA can leave, its copies must have landed: each stage's
+      // last round is released by the MMAs that read it, which waited for
+      // the copies.  After an error the releases may never come; the wait
+      // is then bounded and a short pause lets copies in flight land.
+      bool drained = true;
       for (uint32_t sx = 0; sx < (uint32_t)kStages && sx < n; ++sx) {
-        const uint32_t last = sx + ((n - 1 - sx) / kStages) * kStages;
-        mbar_wait(&full[sx], (last / kStages) & 1, g.err, 5);
+        const uint32_t last = (n - 1 - sx) / kStages;  // round of stage sx
+        drained = mbar_drain(&empty[sx], last & 1, 1000000ull) && drained;
       }
+      if (!drained) spin_ns(100000ull);
     }
   } else if (warp == 1) {
-    if (lane == 0) {
-      const uint32_t idesc = idesc_bf16_f32(kBM, kBN);
+    if (lane == 0 && leader) {
+      const uint32_t idesc = idesc_bf16_f32(kSplitPairRows, kBN);
       uint32_t st = 0, ph = 0, ai = 0;
       bool ok = true;
-      for (int64_t tile = blockIdx.x; tile < g.tiles && ok; tile += gridDim.x) {
+      for (int64_t tile = pair; tile < g.tiles && ok; tile += pairs) {
         const TileCoord tc = tile_coord(g, tile);
         const int chunks = g.desc[tc.q].kblocks / kChunkBlocks;
         for (int c = 0; c < chunks && ok; ++c)
           for (int D = 0; D < S && ok; ++D, ++ai) {
             const uint32_t buf = ai % kAccBufs;
-            if (ai >= (uint32_t)kAccBufs && !mbar_wait(&acc_empty[buf], ((ai / kAccBufs) - 1) & 1, g.err, 2)) {
+            if (ai >= (uint32_t)kAccBufs &&
+                !mbar_wait<true>(&acc_empty[buf], ((ai / kAccBufs) - 1) & 1, g.err, 2)) {
               ok = false;
               break;
             }
@@ -368,39 +393,41 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
             const uint32_t d_tmem = tmem + buf * kBN;
             for (int t = 0; t <= D && ok; ++t)
               for (int h = 0; h < kChunkBlocks; h += kStageKBlocks) {
-                if (!mbar_wait(&full[st], ph, g.err, 3)) {
+                if (!mbar_wait<true>(&full[st], ph, g.err, 3)) {
                   ok = false;
                   break;
                 }
                 tc_fence_after();
                 const uint32_t a = smem_addr(base + st * kStageBytes);
-                const uint32_t b = a + kStageKBlocks * kTileBytes;
+                const uint32_t b = a + kStageKBlocks * kATileBytes;
 #pragma unroll
                 for (int kk = 0; kk < kStageKBlocks * kBK / 16; ++kk) {
-                  const uint32_t off = (kk >> 2) * kTileBytes + (kk & 3) * 32;
-                  mma_bf16(d_tmem, smem_desc_sw128(a + off), smem_desc_sw128(b + off), idesc, t > 0 || h > 0 || kk > 0);
+                  const uint32_t koff = (kk & 3) * 32;
+                  mma_bf16_pair(d_tmem, smem_desc_sw128(a + (kk >> 2) * kATileBytes + koff),
+                                smem_desc_sw128(b + (kk >> 2) * kBTileBytes + koff), idesc,
+                                t > 0 || h > 0 || kk > 0);
                 }
-                mma_commit(&empty[st]);
+                mma_commit_pair(&empty[st], kPairMask);
                 if (++st == (uint32_t)kStages) {
                   st = 0;
                   ph ^= 1u;
                 }
               }
-            if (ok) mma_commit(&acc_full[buf]);
+            if (ok) mma_commit_pair(&acc_full[buf], kPairMask);
           }
       }
-      // every MMA issued by this thread completes before TMEM is freed
-      mma_commit(&mma_done);
-      mbar_wait(&mma_done, 0, g.err, 6);
+      // every MMA issued by this thread completes before tensor memory is freed
+      mma_commit_pair(&mma_done, 0x1);
+      mbar_drain(&mma_done, 0, 1000000000ull);
     }
   } else {
     // warpgroup wg owns columns [64 wg, 64 wg + 64) of the tile; warp
-    // quadrant qd owns TMEM lanes (tile rows) [32 qd, 32 qd + 32)
+    // quadrant qd owns TMEM lanes (this CTA's tile rows) [32 qd, 32 qd + 32)
     const int wg = (warp - 2) >> 2, qd = warp & 3;
     const int row_in_tile = qd * 32 + lane;
     uint32_t ai = 0;
     bool ok = true;
-    for (int64_t tile = blockIdx.x; tile < g.tiles && ok; tile += gridDim.x) {
+    for (int64_t tile = pair; tile < g.tiles && ok; tile += pairs) {
       const TileCoord tc = tile_coord(g, tile);
       const SplitDesc& s = g.desc[tc.q];
       const int chunks = s.kblocks / kChunkBlocks;
@@ -410,7 +437,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
       for (int c = 0; c < chunks && ok; ++c)
         for (int D = 0; D < S; ++D, ++ai) {
           const int buf = ai % kAccBufs;
-          if (!mbar_wait(&acc_full[buf], (ai / kAccBufs) & 1, g.err, 4)) {
+          if (!mbar_wait<true>(&acc_full[buf], (ai / kAccBufs) & 1, g.err, 4)) {
             ok = false;
             break;
           }
@@ -433,7 +460,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
             if (g8 + 2 == 8) {  // the accumulator is free once the last piece is in registers
               tc_fence_before();
               __syncwarp();
-              if (lane == 0) mbar_arrive(&acc_empty[buf]);
+              if (lane == 0) mbar_arrive_cluster(cluster_addr(&acc_empty[buf], 0));  // the leader's
             }
 #pragma unroll
             for (int j = 0; j < 8; ++j)
@@ -442,7 +469,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
           }
         }
       if (!ok) break;
-      const int64_t row = (int64_t)tc.tm * kBM + row_in_tile;
+      const int64_t row = (int64_t)tc.tm * kSplitPairRows + rank * kBM + row_in_tile;
       if (row < s.m) {
         const int er = g.ea[s.e_off + row];
         const int64_t col0 = (int64_t)tc.tn * kBN + wg * 64;
@@ -461,10 +488,15 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
       }
     }
   }
+  // no CTA of the pair leaves (or frees tensor memory) while the other may
+  // still read its shared memory or arrive on its barriers
   tc_fence_before();
-  __syncthreads();
+  cluster_sync();
   tc_fence_after();
-  if (warp == 1) tmem_dealloc(tmem, kAccBufs * kBN);
+  if (warp == 1) {
+    __syncwarp();
+    tmem_dealloc_pair(tmem, kAccBufs * kBN);
+  }
 }
 
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
@@ -538,7 +570,7 @@ cudaError_t split_gemm_launch(const SplitDesc* d_descs, int n, const SplitPlan& 
   if (e != cudaSuccess) return e;
   if (split_done && (e = cudaEventRecord(split_done, stream)) != cudaSuccess) return e;
   CUtensorMap tA, tB;
-  if (!encode_slices(&tA, as, plan.rows_a, kBM) || !encode_slices(&tB, bs, plan.rows_b, kBN))
+  if (!encode_slices(&tA, as, plan.rows_a, kBM) || !encode_slices(&tB, bs, plan.rows_b, kBHalf))
     return cudaErrorInvalidValue;
   GemmParams gp;
   gp.desc = d_descs;
@@ -560,7 +592,9 @@ cudaError_t split_gemm_launch(const SplitDesc* d_descs, int n, const SplitPlan& 
       if (dev >= 0 && dev < 64) opted_in[dev] = true;
     }
   }
-  split_gemm_kernel<<<grid_for(plan.tiles, num_sms), kGemmThreads, kGemmSmem, stream>>>(tA, tB, gp);
+  // CTA pairs: the grid is even and a pair's CTAs are consecutive blocks
+  const unsigned pairs = grid_for(plan.tiles, num_sms / 2 > 0 ? num_sms / 2 : 1);
+  split_gemm_kernel<<<2 * pairs, kGemmThreads, kGemmSmem, stream>>>(tA, tB, gp);
   e = cudaGetLastError();
   if (e == cudaSuccess && launches) *launches += 4;
   return e;

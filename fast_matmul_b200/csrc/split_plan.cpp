@@ -5,7 +5,9 @@
 // padded rows (or columns) of that block form consecutive 128-byte rows of 64
 // BF16 values.  One 2-D tensor map {64, rows} then covers every slice of
 // every problem, whatever the shapes: a 128 x 64 operand tile is the box at
-// x = 0, y = a_row + (t * kblocks + b) * padded_rows + tile_row.
+// x = 0, y = a_row + (t * kblocks + b) * padded_rows + tile_row.  Rows of A
+// are padded to a multiple of 256, the rows of the output tile of one CTA
+// pair; output tiles are counted per pair (256 x 128).
 
 #include <algorithm>
 
@@ -23,7 +25,7 @@ struct Geometry {
 
 Geometry geometry(int64_t m, int64_t k, int64_t n) {
   Geometry g;
-  g.tiles_m = (m + kSplitTile - 1) / kSplitTile;
+  g.tiles_m = (m + kSplitPairRows - 1) / kSplitPairRows * (kSplitPairRows / kSplitTile);
   g.tiles_n = (n + kSplitTile - 1) / kSplitTile;
   g.kblocks = std::max<int64_t>(1, (k + kSplitChunk - 1) / kSplitChunk) * (kSplitChunk / kSplitKBlock);
   return g;
@@ -49,7 +51,7 @@ SplitPlan split_prepare(SplitDesc* descs, int n, int slices) {
     d.f_off = p.n_f;
     if (empty) continue;
     const int64_t mp = g.tiles_m * kSplitTile, np = g.tiles_n * kSplitTile;
-    p.tiles += g.tiles_m * g.tiles_n;
+    p.tiles += g.tiles_m / 2 * g.tiles_n;
     p.sa_work += (mp / 32) * g.kblocks;
     p.rows_a += (int64_t)slices * g.kblocks * mp;
     p.rows_b += (int64_t)slices * g.kblocks * np;
@@ -64,7 +66,7 @@ void split_accumulate(SplitPlan* p, int64_t m, int64_t k, int64_t n, int64_t cou
   if (m <= 0 || n <= 0 || count <= 0) return;
   const Geometry g = geometry(m, k, n);
   const int64_t mp = g.tiles_m * kSplitTile, np = g.tiles_n * kSplitTile;
-  p->tiles += count * g.tiles_m * g.tiles_n;
+  p->tiles += count * (g.tiles_m / 2) * g.tiles_n;
   p->sa_work += count * (mp / 32) * g.kblocks;
   p->rows_a += count * p->slices * g.kblocks * mp;
   p->rows_b += count * p->slices * g.kblocks * np;
