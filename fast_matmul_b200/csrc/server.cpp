@@ -213,9 +213,14 @@ bool turn(fmm_server s) {
         progressed = true;
         continue;
       }
-      if (need + bytes + 256 > avail) break;  // admit in order: wait for memory
-      need += (bytes + 255) & ~(size_t)255;
-      for (const fmm::BatchItem& b : one) batch.push_back(b);
+      // the footprint of the batch with this request, laid out as the batch
+      // program lays it out (alignment between items included)
+      std::vector<fmm::BatchItem> trial = batch;
+      trial.insert(trial.end(), one.begin(), one.end());
+      const size_t total = trial.empty() ? 0 : fmm::batch_workspace_bytes(trial.data(), (int)trial.size());
+      if (total + 256 > avail) break;  // admit in order: wait for memory
+      need = (total + 255) & ~(size_t)255;
+      batch.swap(trial);
       tickets.push_back(p.ticket);
       s->pending.pop_front();
     }
@@ -234,7 +239,7 @@ bool turn(fmm_server s) {
       } catch (const std::exception&) {
         st = FMM_ERR_OUT_OF_MEMORY;
       }
-      // the batch's own layout never exceeds the summed per-request footprints
+      // the program lays the batch out exactly as batch_workspace_bytes does
       if (st == FMM_OK && sl.prog.workspace_bytes > need) st = FMM_ERR_OUT_OF_MEMORY;
       if (st == FMM_OK && !ensure_slot_buffers(sl, sl.prog.desc.size() + 64)) st = FMM_ERR_OUT_OF_MEMORY;
       if (st == FMM_OK) {

@@ -56,19 +56,6 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// The same with cluster-scope acquire: for barriers that threads or copies
-// of the other CTA of a cluster arrive on.
-__device__ __forceinline__ bool mbar_try_wait_cluster(uint64_t* bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n"
-      " selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(smem_addr(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
 __device__ __forceinline__ uint64_t global_timer_ns() {
   uint64_t t;
   asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
@@ -77,15 +64,14 @@ __device__ __forceinline__ uint64_t global_timer_ns() {
 
 // Waits for the phase with the given parity to complete; false (and *err set
 // to `code`) if it did not within limit_ns, or if *err is already set.
-// kCluster selects the cluster-scope acquire.
-template <bool kCluster = false>
+// Barriers that copies or threads of the other CTA of a pair arrive on are
+// waited on the same way (CTA scope, as for the copies of this CTA).
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int code,
                                           uint64_t limit_ns = kWaitLimitNs) {
-  auto test = [&] { return kCluster ? mbar_try_wait_cluster(bar, parity) : mbar_try_wait(bar, parity); };
-  if (test()) return true;
+  if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = global_timer_ns();
   for (uint32_t i = 1;; ++i) {
-    if (test()) return true;
+    if (mbar_try_wait(bar, parity)) return true;
     if ((i & 63) == 0) {
       if (*reinterpret_cast<volatile int*>(err)) return false;  // another role gave up
       if (global_timer_ns() - t0 > limit_ns) {
@@ -96,12 +82,12 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* e
   }
 }
 
-// Waits (cluster scope) for the phase with the given parity for at most
+// Waits for the phase with the given parity for at most
 // limit_ns, whatever *err holds: used before a CTA leaves, so that copies it
 // started have landed.  Returns whether the phase completed.
 __device__ __forceinline__ bool mbar_drain(uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
   const uint64_t t0 = global_timer_ns();
-  while (!mbar_try_wait_cluster(bar, parity))
+  while (!mbar_try_wait(bar, parity))
     if (global_timer_ns() - t0 > limit_ns) return false;
   return true;
 }
@@ -133,9 +119,12 @@ __device__ __forceinline__ uint32_t cluster_addr(const void* p, uint32_t rank) {
   return r;
 }
 
-// Arrive (release, cluster scope) on an mbarrier given by its cluster address.
+// Arrive on an mbarrier given by its cluster address (possibly the other
+// CTA's).  Default (CTA-scope) semantics: the only data it orders is tensor
+// memory, which tcgen05.fence::before/after_thread_sync order around the
+// arrive and the wait; a cluster-scope release would cost a memory barrier.
 __device__ __forceinline__ void mbar_arrive_cluster(uint32_t bar_cluster_addr) {
-  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];\n" ::"r"(bar_cluster_addr) : "memory");
+  asm volatile("mbarrier.arrive.shared::cluster.b64 _, [%0];\n" ::"r"(bar_cluster_addr) : "memory");
 }
 
 // ---- TMA

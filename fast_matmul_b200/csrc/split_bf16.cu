@@ -339,7 +339,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
           for (int D = 0; D < S && ok; ++D)
             for (int t = 0; t <= D && ok; ++t)
               for (int h = 0; h < kChunkBlocks; h += kStageKBlocks) {
-                if (n >= (uint32_t)kStages && !mbar_wait<true>(&empty[st], ph ^ 1u, g.err, 1)) {
+                if (n >= (uint32_t)kStages && !mbar_wait(&empty[st], ph ^ 1u, g.err, 1)) {
                   ok = false;
                   break;
                 }
@@ -385,7 +385,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
           for (int D = 0; D < S && ok; ++D, ++ai) {
             const uint32_t buf = ai % kAccBufs;
             if (ai >= (uint32_t)kAccBufs &&
-                !mbar_wait<true>(&acc_empty[buf], ((ai / kAccBufs) - 1) & 1, g.err, 2)) {
+                !mbar_wait(&acc_empty[buf], ((ai / kAccBufs) - 1) & 1, g.err, 2)) {
               ok = false;
               break;
             }
@@ -393,7 +393,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
             const uint32_t d_tmem = tmem + buf * kBN;
             for (int t = 0; t <= D && ok; ++t)
               for (int h = 0; h < kChunkBlocks; h += kStageKBlocks) {
-                if (!mbar_wait<true>(&full[st], ph, g.err, 3)) {
+                if (!mbar_wait(&full[st], ph, g.err, 3)) {
                   ok = false;
                   break;
                 }
@@ -437,7 +437,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
       for (int c = 0; c < chunks && ok; ++c)
         for (int D = 0; D < S; ++D, ++ai) {
           const int buf = ai % kAccBufs;
-          if (!mbar_wait<true>(&acc_full[buf], (ai / kAccBufs) & 1, g.err, 4)) {
+          if (!mbar_wait(&acc_full[buf], (ai / kAccBufs) & 1, g.err, 4)) {
             ok = false;
             break;
           }
