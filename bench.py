@@ -53,12 +53,15 @@ def parse_args(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=4096, help="edge of the CPU baseline sample")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU work budget of the baseline sample")
-    ap.add_argument("--workload", default="product", choices=["product", "batch", "serve", "precision", "scaling"],
+    ap.add_argument("--workload", default="product",
+                    choices=["product", "batch", "serve", "precision", "scaling", "fp32"],
                     help="product: one large FastMatmul (the headline); batch: 4096 independent products "
                          "with log-uniform dimensions in [64, 1024] in one CUDA-graph plan; serve: a Poisson "
                          "request stream through the continuous-batching server; precision: split-BF16 leaf "
                          "products (Strassen, Bini) against the FP64 oracle; scaling: diagonal scaling "
-                         "(Scaling + FastMatmul + PostProcessScaling) on skewed operands")
+                         "(Scaling + FastMatmul + PostProcessScaling) on skewed operands; fp32: "
+                         "FastMatmul<float> against cuBLAS SGEMM")
+    ap.add_argument("--fp32-size", type=int, default=16384, help="square size of the fp32 workload")
     ap.add_argument("--scaling-size", type=int, default=16384, help="square size of the scaling workload")
     ap.add_argument("--precision-sizes", default="8192,16384",
                     help="square sizes of the precision workload")
@@ -1043,6 +1046,114 @@ def run_scaling_workload(a):
     return 0
 
 
+def run_fp32_workload(a):
+    """FastMatmul<float> (fmm_fast_matmul_f32): FP32 operands widened to FP64
+    on the device, split-BF16 leaf products (4 slices by default), rounded to
+    FP32 once.  At n^3: Strassen with 1 and 2 steps and the classical
+    product (fmm_sgemm) against cuBLAS SGEMM (torch.matmul in float32, TF32
+    off) on the same inputs, errors against the exact product of the FP32
+    inputs on sampled entries, and the reference's own FastMatmul<float>
+    (sgemm leaves, all host threads) on a bounded sample."""
+    import numpy as np
+    import torch
+
+    import fast_matmul_b200 as fmm
+
+    torch.cuda.set_device(0)
+    torch.backends.cuda.matmul.allow_tf32 = False
+    dev = torch.device("cuda", 0)
+    h = fmm.default_handle(0)
+    n = a.fp32_size
+    flops = 2.0 * n ** 3
+    A64 = fmm.random_matrix(n, n, 51, 1, handle=h)
+    B64 = fmm.random_matrix(n, n, 51, 2, handle=h)
+    A = A64.float()
+    B = B64.float()
+    A64 = A.double()  # the exact values of the FP32 operands
+    B64 = B.double()
+    C = torch.empty((n, n), dtype=torch.float32, device=dev).t()
+
+    def timed(fn, reps):
+        for _ in range(max(a.warmup, 3)):
+            fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    def errors(Cf):
+        rel, _ = exact_sample_errors(A64, B64, Cf.double(), count=32)
+        return rel
+
+    rows = []
+    Cb = torch.matmul(A, B)
+    ms_cublas = timed(lambda: torch.matmul(A, B, out=Cb), a.steps)
+    rows.append({"product": "cuBLAS SGEMM (torch.matmul, float32, TF32 off)", "ms": ms_cublas,
+                 "tflops": flops / (ms_cublas * 1e-3) / 1e12, "max_rel_vs_exact_32_sampled": errors(Cb)})
+    del Cb
+    clocks = ClockSampler(0)
+    clocks.start()
+    configs = [("classical (fmm_sgemm)", None, 0, 4), ("strassen", "strassen", 1, 4), ("strassen", "strassen", 2, 4),
+               ("strassen", "strassen", 2, 3), ("grey424_26_206", "grey424_26_206", 2, 4)]
+    for label, alg, steps, sl in configs:
+        if alg is None:
+            fn = lambda: fmm.matmul(A, B, C, handle=h)  # noqa: E731
+        else:
+            fn = lambda: fmm.fast_matmul(alg, A, B, C, steps, precision="split_bf16", split_slices=sl,  # noqa: E731
+                                         handle=h)
+        ms = timed(fn, a.steps)
+        fmm.synchronize(h)
+        rows.append({"product": label, "num_steps": steps, "precision": "split_bf16 x%d" % sl, "ms": ms,
+                     "tflops": flops / (ms * 1e-3) / 1e12, "max_rel_vs_exact_32_sampled": errors(C)})
+        print(json.dumps({"fp32_row": rows[-1]}), file=sys.stderr, flush=True)
+    clk = clocks.stop()
+    best = max((r for r in rows[1:] if r["max_rel_vs_exact_32_sampled"] <= rows[0]["max_rel_vs_exact_32_sampled"]
+                or r["max_rel_vs_exact_32_sampled"] <= 2.0 ** -23), key=lambda r: r["tflops"])
+    cpu = None
+    if not a.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+        import oracle  # the CPU baseline leg may load the reference build
+
+        if oracle.ref_available():
+            edge = 4096
+            threads = os.cpu_count() or 1
+            oracle.ref_lib().fmmref_set_threads(threads)
+            Ah = np.asfortranarray(oracle.uniform(edge, edge, 7, 1).astype(np.float32))
+            Bh = np.asfortranarray(oracle.uniform(edge, edge, 7, 2).astype(np.float32))
+            Ch = np.zeros((edge, edge), dtype=np.float32, order="F")
+            oracle.ref_fast_matmul_f32("strassen", Ah, Bh, Ch, 2)
+            ts = []
+            t_end = time.time() + a.cpu_seconds
+            while time.time() < t_end or len(ts) < 2:
+                t0 = time.perf_counter()
+                oracle.ref_fast_matmul_f32("strassen", Ah, Bh, Ch, 2)
+                ts.append((time.perf_counter() - t0) * 1e3)
+            cms = statistics.median(ts)
+            cpu = {"value": 2.0 * edge ** 3 / (cms * 1e-3) / 1e12, "unit": "TFLOP/s", "cores": threads,
+                   "kind": "reference",
+                   "sample": "strassen::FastMatmul<float>(A, B, C, 2) of the reference (sgemm leaves), %d^3, "
+                             "median of %d runs, %.0f ms each" % (edge, len(ts), cms)}
+    peaks, peak_src = measured_peaks()
+    out = {
+        "metric": "effective TFLOP/s (2MNK/t), FP32 operands, vs cuBLAS SGEMM", "value": best["tflops"],
+        "unit": "TFLOP/s", "n_gpus": 1, "steps": a.steps, "warmup": max(a.warmup, 3), "ms_per_step": best["ms"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 in/out (bf16 slices, f64 accumulation)", "data": "synthetic",
+        "config": {"workload": "FastMatmul<float> at %d^3, seeded uniform [0,1) rounded to FP32; headline = fastest "
+                               "configuration whose sampled error is within cuBLAS SGEMM's or 2^-23" % n,
+                   "headline": best, "l2": "inputs larger than L2"},
+        "speedup_vs_cublas_sgemm": best["tflops"] / rows[0]["tflops"],
+        "clocks": clk, "cpu_baseline": cpu, "peak_source": peak_src, "rows": rows,
+    }
+    print(json.dumps(out))
+    return 0
+
+
 def main(argv=None):
     a = parse_args(argv)
     if a.impl == "reference":
@@ -1057,6 +1168,8 @@ def main(argv=None):
         return run_precision_workload(a)
     if a.workload == "scaling":
         return run_scaling_workload(a)
+    if a.workload == "fp32":
+        return run_fp32_workload(a)
     return run_ours(a)
 
 

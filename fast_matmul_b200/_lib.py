@@ -163,6 +163,23 @@ SIGNATURES = {
     "fmm_scaling_postprocess_host": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
                                                      ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p,
                                                      ctypes.c_void_p]),
+    "fmm_fast_matmul_f32": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int64,
+                                            ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64,
+                                            ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int,
+                                            ctypes.c_double, ctypes.c_float, ctypes.c_float,
+                                            ctypes.POINTER(Options)]),
+    "fmm_sgemm": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64,
+                                 ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
+                                 ctypes.c_float, ctypes.c_float, ctypes.POINTER(Options)]),
+    "fmm_fast_matmul_f32_host": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int64,
+                                                 ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64,
+                                                 ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int,
+                                                 ctypes.c_double, ctypes.c_float, ctypes.c_float,
+                                                 ctypes.POINTER(Options), c_double_p]),
+    "fmm_sgemm_host": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+                                      ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
+                                      ctypes.c_int64, ctypes.c_int64, ctypes.c_float, ctypes.c_float,
+                                      ctypes.POINTER(Options)]),
     "fmm_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
     "fmm_kernel_launch_count": (ctypes.c_int64, [ctypes.c_void_p]),
     "fmm_selftest_wait_timeout": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.POINTER(ctypes.c_int)]),

@@ -151,10 +151,14 @@ def colmajor_empty(m: int, n: int, device="cuda"):
     return torch.empty((n, m), dtype=torch.float64, device=device).t()
 
 
-def _mat(t, rows: int, cols: int, name: str) -> Tuple[int, int]:
+F32_DEFAULT_SLICES = 4  # FMM_F32_DEFAULT_SLICES of include/fmm.h
+
+
+def _mat(t, rows: int, cols: int, name: str, dtype=None) -> Tuple[int, int]:
     torch = _torch()
-    if t.dtype != torch.float64:
-        raise TypeError("%s must be float64" % name)
+    want = torch.float64 if dtype is None else dtype
+    if t.dtype != want:
+        raise TypeError("%s must be %s" % (name, str(want).replace("torch.", "")))
     if tuple(t.shape) != (rows, cols):
         raise ValueError("%s has shape %s, expected %s" % (name, tuple(t.shape), (rows, cols)))
     if rows > 1 and cols > 1 and t.stride(0) != 1:
@@ -176,21 +180,37 @@ def _options(schedule="auto", dfs_levels=-1, workspace_limit=0, precision="fp64"
 
 def fast_matmul(alg, A, B, C, num_steps: int, x: float = 1e-8, alpha: float = 1.0, beta: float = 0.0,
                 schedule: str = "auto", dfs_levels: int = -1, workspace_limit: int = 0,
-                precision: str = "fp64", split_slices: int = 0, handle: Optional[Handle] = None) -> None:
+                precision: Optional[str] = None, split_slices: int = 0, handle: Optional[Handle] = None) -> None:
     """C := alpha * A * B + beta * C with `num_steps` levels of algorithm
     `alg` -- <alg>::FastMatmul(A, B, C, num_steps, x, alpha, beta).
     precision "split_bf16" runs the leaf products on the BF16 tensor cores
-    over `split_slices` slices (0 = 5).  Queued on torch's current stream."""
+    over `split_slices` slices (0 = 5).  Queued on torch's current stream.
+
+    float32 operands (all three) select FastMatmul<float>
+    (fmm_fast_matmul_f32): computed on FP64 copies and rounded to FP32 once;
+    precision None there means split-BF16 leaves with 4 slices."""
+    torch = _torch()
     idx = algorithm_index(alg)
     m, k = A.shape
     k2, n = B.shape
     if k2 != k:
         raise ValueError("inner dimensions differ")
+    h = handle or default_handle(C.device.index)
+    if A.dtype == torch.float32:
+        pa, lda = _mat(A, m, k, "A", torch.float32)
+        pb, ldb = _mat(B, k, n, "B", torch.float32)
+        pc, ldc = _mat(C, m, n, "C", torch.float32)
+        if precision is None:  # the FP32 default: split-BF16 leaves, FMM_F32_DEFAULT_SLICES slices
+            o = _options(schedule, dfs_levels, workspace_limit, "split_bf16", split_slices or F32_DEFAULT_SLICES)
+        else:
+            o = _options(schedule, dfs_levels, workspace_limit, precision, split_slices)
+        check(lib().fmm_fast_matmul_f32(h.ptr, idx, pa, lda, pb, ldb, pc, ldc, m, k, n, num_steps, x, alpha, beta,
+                                        ctypes.byref(o)))
+        return
     pa, lda = _mat(A, m, k, "A")
     pb, ldb = _mat(B, k, n, "B")
     pc, ldc = _mat(C, m, n, "C")
-    h = handle or default_handle(C.device.index)
-    o = _options(schedule, dfs_levels, workspace_limit, precision, split_slices)
+    o = _options(schedule, dfs_levels, workspace_limit, precision or "fp64", split_slices)
     check(lib().fmm_fast_matmul(h.ptr, idx, pa, lda, pb, ldb, pc, ldc, m, k, n, num_steps, x, alpha, beta,
                                 ctypes.byref(o)))
 
@@ -241,9 +261,18 @@ def fast_matmul_host(alg, A, B, C, num_steps: int, x: float = 1e-8, alpha: float
 
 def matmul(A, B, C, alpha: float = 1.0, beta: float = 0.0, handle: Optional[Handle] = None) -> None:
     """Classical C := alpha * A * B + beta * C on the engine's FP64 GEMM
-    (MatMul with C's multiplier as alpha)."""
+    (MatMul with C's multiplier as alpha).  float32 operands: MatMul<float>
+    (fmm_sgemm: FP64 copies, split-BF16 with 4 slices, rounded to FP32)."""
+    torch = _torch()
     m, k = A.shape
     n = B.shape[1]
+    if A.dtype == torch.float32:
+        pa, lda = _mat(A, m, k, "A", torch.float32)
+        pb, ldb = _mat(B, k, n, "B", torch.float32)
+        pc, ldc = _mat(C, m, n, "C", torch.float32)
+        h = handle or default_handle(C.device.index)
+        check(lib().fmm_sgemm(h.ptr, pa, lda, pb, ldb, pc, ldc, m, k, n, alpha, beta, None))
+        return
     pa, lda = _mat(A, m, k, "A")
     pb, ldb = _mat(B, k, n, "B")
     pc, ldc = _mat(C, m, n, "C")

@@ -43,6 +43,10 @@ struct fmm_handle_s {
   double* d_small = nullptr;  // two doubles for reductions
   void* scal = nullptr;       // maxima and factors of the diagonal scaling
   size_t scal_cap = 0;
+  void* wide = nullptr;       // FP64 staging of the FP32 entry points
+  size_t wide_cap = 0;
+  void* narrow_io = nullptr;  // device copies of host FP32 operands
+  size_t narrow_io_cap = 0;
   int* d_err = nullptr;       // error codes of split-BF16 kernels (bounded waits that gave up)
   int64_t launches = 0;
   fmm::Program prog;

@@ -239,6 +239,8 @@ fmm_status fmm_handle_create(fmm_handle* out, int device) {
     if (h->desc_done) cudaEventDestroy(h->desc_done);
     if (h->d_small) cudaFree(h->d_small);
   if (h->scal) cudaFree(h->scal);
+  if (h->wide) cudaFree(h->wide);
+  if (h->narrow_io) cudaFree(h->narrow_io);
     if (h->d_err) cudaFree(h->d_err);
     delete h;
     return fail(FMM_ERR_CUDA, "handle setup failed");

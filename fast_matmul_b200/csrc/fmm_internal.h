@@ -163,6 +163,13 @@ cudaError_t scaling_postprocess_launch(double* C, int64_t ldc, int m, int n, con
                                        cudaStream_t stream, int64_t* launches);
 
 // ---------------------------------------------------------------------------
+// FP32 <-> FP64 conversions of column-major matrices (convert.cu).
+cudaError_t widen_launch(const float* src, int64_t lds, double* dst, int64_t ldd, int64_t rows, int64_t cols,
+                         int num_sms, cudaStream_t stream);
+cudaError_t narrow_launch(const double* src, int64_t lds, float* dst, int64_t ldd, int64_t rows, int64_t cols,
+                          int num_sms, cudaStream_t stream);
+
+// ---------------------------------------------------------------------------
 // Utilities (util_kernels.cu).
 cudaError_t fill_uniform_launch(double* out, int64_t rows, int64_t cols, int64_t ld, uint64_t seed, uint64_t stream_id,
                                 double lo, double hi, cudaStream_t stream);

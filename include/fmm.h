@@ -153,6 +153,33 @@ fmm_status fmm_dgemm_split_bf16(fmm_handle h, const double* A, int64_t lda, cons
 fmm_status fmm_dgemm_host(fmm_handle h, const double* A, int64_t lda, const double* B, int64_t ldb, double* C,
                           int64_t ldc, int64_t m, int64_t k, int64_t n, double alpha, double beta);
 
+/* FP32 operands: the reference's templates with Scalar = float --
+ * <ns>::FastMatmul<float> (algorithms/strassen.hpp:661-722 and the other
+ * headers) and MatMul<float>, whose leaf is sgemm (linalg/linalg.hpp:261-269,
+ * linalg/blas_wrap.hpp:116-120).  The operands are widened to FP64 once
+ * (exact), the product runs on the FP64 engine, and C is rounded to FP32
+ * once (round to nearest), so every result is at least as accurate as the
+ * reference's, which rounds in FP32 at every addition and leaf product.
+ * opts == NULL selects split-BF16 leaf products with FMM_F32_DEFAULT_SLICES
+ * slices (32 bits per operand entry, beyond FP32's 24); other options are
+ * taken as given (FMM_PRECISION_FP64 runs FP64 leaves).  Device pointers,
+ * the handle's stream; FP64 staging of m*k + k*n + m*n doubles is held by
+ * the handle.  num_steps == 0 ignores beta, as FastMatmul does. */
+#define FMM_F32_DEFAULT_SLICES 4
+fmm_status fmm_fast_matmul_f32(fmm_handle h, int alg, const float* A, int64_t lda, const float* B, int64_t ldb,
+                               float* C, int64_t ldc, int64_t m, int64_t k, int64_t n, int num_steps, double x,
+                               float alpha, float beta, const fmm_options* opts);
+fmm_status fmm_sgemm(fmm_handle h, const float* A, int64_t lda, const float* B, int64_t ldb, float* C, int64_t ldc,
+                     int64_t m, int64_t k, int64_t n, float alpha, float beta, const fmm_options* opts);
+/* The same with HOST matrices; they return when C is on the host (for the
+ * C++ adapter's Matrix<float>). */
+fmm_status fmm_fast_matmul_f32_host(fmm_handle h, int alg, const float* A, int64_t lda, const float* B, int64_t ldb,
+                                    float* C, int64_t ldc, int64_t m, int64_t k, int64_t n, int num_steps, double x,
+                                    float alpha, float beta, const fmm_options* opts, double* elapsed_ms);
+fmm_status fmm_sgemm_host(fmm_handle h, const float* A, int64_t lda, const float* B, int64_t ldb, float* C,
+                          int64_t ldc, int64_t m, int64_t k, int64_t n, float alpha, float beta,
+                          const fmm_options* opts);
+
 /* Seeded input generator: out(i, j) = lo + (hi - lo) * u, u in [0, 1) from a
  * counter-based splitmix64 stream (element index i + j * rows), identical to
  * the host generator used by the tests. */

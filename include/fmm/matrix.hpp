@@ -7,7 +7,8 @@
 // a pointer, Subblock/Submatrix return views, the copy constructor deep
 // copies, and every matrix carries a scalar multiplier.  Each FastMatmul /
 // MatMul call copies its operands to the device, computes there and copies
-// C back.  Only Scalar = double is supported by the engine.
+// C back.  Scalar is double or float; float matrices run through the FP32
+// entry points (widened to FP64 on the device, rounded back once).
 //
 // Engine failures throw std::runtime_error with the engine's message (the
 // reference has no error reporting; its FastMatmul returns elapsed ms).
@@ -132,18 +133,41 @@ inline fmm_handle ThreadHandle() {
 // Multiplier side effects as in the reference: A's multiplier is set to
 // alpha, then A's and B's multipliers are folded into C's and reset to 1
 // (:669, :380-383), so C keeps multiplier = C.mult * alpha * B.mult.
+inline fmm_status FastHost(int alg, double* A, int lda, double* B, int ldb, double* C, int ldc, int m, int k, int n,
+                           int steps, double x, double alpha, double beta, double* ms) {
+  return fmm_fast_matmul_host(ThreadHandle(), alg, A, lda, B, ldb, C, ldc, m, k, n, steps, x, alpha, beta, nullptr,
+                              ms);
+}
+
+inline fmm_status FastHost(int alg, float* A, int lda, float* B, int ldb, float* C, int ldc, int m, int k, int n,
+                           int steps, double x, float alpha, float beta, double* ms) {
+  return fmm_fast_matmul_f32_host(ThreadHandle(), alg, A, lda, B, ldb, C, ldc, m, k, n, steps, x, alpha, beta,
+                                  nullptr, ms);
+}
+
+inline fmm_status GemmHost(double* A, int lda, double* B, int ldb, double* C, int ldc, int m, int k, int n,
+                           double alpha, double beta) {
+  return fmm_dgemm_host(ThreadHandle(), A, lda, B, ldb, C, ldc, m, k, n, alpha, beta);
+}
+
+inline fmm_status GemmHost(float* A, int lda, float* B, int ldb, float* C, int ldc, int m, int k, int n, float alpha,
+                           float beta) {
+  return fmm_sgemm_host(ThreadHandle(), A, lda, B, ldb, C, ldc, m, k, n, alpha, beta, nullptr);
+}
+
 template <typename Scalar>
 double RunFastMatmul(int alg, Matrix<Scalar>& A, Matrix<Scalar>& B, Matrix<Scalar>& C, int num_steps, double x,
                      Scalar alpha, Scalar beta) {
-  static_assert(std::is_same<Scalar, double>::value, "the B200 engine computes in FP64 (Scalar = double)");
+  static_assert(std::is_same<Scalar, double>::value || std::is_same<Scalar, float>::value,
+                "the B200 engine computes with Scalar = double or float");
   A.set_multiplier(alpha);
   C.UpdateMultiplier(A.multiplier());
   C.UpdateMultiplier(B.multiplier());
   A.set_multiplier(Scalar(1));
   B.set_multiplier(Scalar(1));
   double ms = 0.0;
-  Check(fmm_fast_matmul_host(ThreadHandle(), alg, A.data(), A.stride(), B.data(), B.stride(), C.data(), C.stride(),
-                             C.m(), A.n(), C.n(), num_steps, x, C.multiplier(), beta, nullptr, &ms));
+  Check(FastHost(alg, A.data(), A.stride(), B.data(), B.stride(), C.data(), C.stride(), C.m(), A.n(), C.n(),
+                 num_steps, x, C.multiplier(), beta, &ms));
   return ms;
 }
 
@@ -152,11 +176,13 @@ double RunFastMatmul(int alg, Matrix<Scalar>& A, Matrix<Scalar>& B, Matrix<Scala
 
 // C <- C.multiplier * A * B + beta * C (linalg/linalg.hpp:261-269), on the
 // engine's FP64 GEMM.
+// Scalar = float: sgemm's role, through fmm_sgemm_host.
 template <typename Scalar>
 void MatMul(Matrix<Scalar>& A, Matrix<Scalar>& B, Matrix<Scalar>& C, Scalar beta = Scalar(0.0)) {
-  static_assert(std::is_same<Scalar, double>::value, "the B200 engine computes in FP64 (Scalar = double)");
-  fmm::detail::Check(fmm_dgemm_host(fmm::detail::ThreadHandle(), A.data(), A.stride(), B.data(), B.stride(), C.data(),
-                                    C.stride(), C.m(), A.n(), C.n(), C.multiplier(), beta));
+  static_assert(std::is_same<Scalar, double>::value || std::is_same<Scalar, float>::value,
+                "the B200 engine computes with Scalar = double or float");
+  fmm::detail::Check(fmm::detail::GemmHost(A.data(), A.stride(), B.data(), B.stride(), C.data(), C.stride(), C.m(),
+                                           A.n(), C.n(), C.multiplier(), beta));
 }
 
 // max_ij |a_ij - b_ij| / |a_ij| (linalg/linalg.hpp:280-295)

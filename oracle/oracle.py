@@ -84,6 +84,12 @@ def ref_lib() -> Optional[ctypes.CDLL]:
         L.fmmref_fast_matmul.restype = _D
         L.fmmref_matmul.argtypes = [_P, _I, _P, _I, _P, _I, _I, _I, _I, _D, _D]
         L.fmmref_matmul.restype = None
+        _F = ctypes.c_float
+        _PF = ctypes.POINTER(ctypes.c_float)
+        L.fmmref_fast_matmul_f32.argtypes = [ctypes.c_char_p, _PF, _I, _PF, _I, _PF, _I, _I, _I, _I, _I, _D, _F, _F]
+        L.fmmref_fast_matmul_f32.restype = _D
+        L.fmmref_matmul_f32.argtypes = [_PF, _I, _PF, _I, _PF, _I, _I, _I, _I, _F, _F]
+        L.fmmref_matmul_f32.restype = None
         L.fmmref_set_threads.argtypes = [_I]
         L.fmmref_scaling.argtypes = [_P, _I, _P, _I, _I, _I, _I, _I, _I, _P, _P]
         L.fmmref_scaling.restype = None
@@ -169,6 +175,35 @@ def ref_matmul(A, B, C, alpha=1.0, beta=0.0) -> None:
     m, k = A.shape
     n = B.shape[1]
     L.fmmref_matmul(_p(A), max(m, 1), _p(B), max(k, 1), _p(C), max(m, 1), m, k, n, alpha, beta)
+
+
+def _pf(a: np.ndarray):
+    assert a.dtype == np.float32 and a.flags.f_contiguous
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def ref_fast_matmul_f32(alg: str, A: np.ndarray, B: np.ndarray, C: np.ndarray, num_steps: int, x: float = 1e-8,
+                        alpha: float = 1.0, beta: float = 0.0) -> float:
+    """The reference's <alg>::FastMatmul<float> (sgemm leaves) on
+    Fortran-ordered float32 arrays, C in place; returns its ms."""
+    L = ref_lib()
+    if L is None:
+        raise RuntimeError("reference build oracle/_ref is not available")
+    m, k = A.shape
+    n = B.shape[1]
+    ms = L.fmmref_fast_matmul_f32(alg.encode(), _pf(A), max(m, 1), _pf(B), max(k, 1), _pf(C), max(m, 1), m, k, n,
+                                  num_steps, x, alpha, beta)
+    if ms < 0:
+        raise KeyError(alg)
+    return ms
+
+
+def ref_matmul_f32(A, B, C, alpha=1.0, beta=0.0) -> None:
+    """The reference's MatMul<float> (sgemm) on float32 arrays, C in place."""
+    L = ref_lib()
+    m, k = A.shape
+    n = B.shape[1]
+    L.fmmref_matmul_f32(_pf(A), max(m, 1), _pf(B), max(k, 1), _pf(C), max(m, 1), m, k, n, alpha, beta)
 
 
 def use_reference_leaf(enabled: bool) -> None:

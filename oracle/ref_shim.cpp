@@ -118,6 +118,61 @@ const Entry kEntries[] = {
     FMMREF_ENTRY(tichavsky_kovac363_40_960),
 };
 
+// The same headers with Scalar = float (leaf products through sgemm).
+typedef double (*FastFnF)(Matrix<float>&, Matrix<float>&, Matrix<float>&, int, double, float, float);
+
+struct EntryF {
+  const char* name;
+  FastFnF fn;
+};
+
+#define FMMREF_ENTRY_F(ns) {#ns, &ns::FastMatmul<float>}
+
+const EntryF kEntriesF[] = {
+    FMMREF_ENTRY_F(strassen),
+    FMMREF_ENTRY_F(classical222_8_24),
+    FMMREF_ENTRY_F(grey322_11_50),
+    FMMREF_ENTRY_F(bini322_10_52_approx),
+    FMMREF_ENTRY_F(grey332_15_103),
+    FMMREF_ENTRY_F(grey323_15_103),
+    FMMREF_ENTRY_F(hk332_15_94),
+    FMMREF_ENTRY_F(hk323_15_94),
+    FMMREF_ENTRY_F(hk323_15_84),
+    FMMREF_ENTRY_F(grey323_15_89),
+    FMMREF_ENTRY_F(grey333_23_152),
+    FMMREF_ENTRY_F(grey333_23_221),
+    FMMREF_ENTRY_F(grey333_23_125),
+    FMMREF_ENTRY_F(smirnov333_23_139),
+    FMMREF_ENTRY_F(smirnov333_23_128),
+    FMMREF_ENTRY_F(classical333_27_81),
+    FMMREF_ENTRY_F(schonhage333_21_117_approx),
+    FMMREF_ENTRY_F(smirnov333_20_182_approx),
+    FMMREF_ENTRY_F(grey422_14_84),
+    FMMREF_ENTRY_F(grey432_20_144),
+    FMMREF_ENTRY_F(grey423_20_144),
+    FMMREF_ENTRY_F(grey324_20_144),
+    FMMREF_ENTRY_F(grey342_20_144),
+    FMMREF_ENTRY_F(grey234_20_144),
+    FMMREF_ENTRY_F(grey243_20_144),
+    FMMREF_ENTRY_F(classical423_24_72),
+    FMMREF_ENTRY_F(fast423_130),
+    FMMREF_ENTRY_F(fast423_134),
+    FMMREF_ENTRY_F(fast423_138),
+    FMMREF_ENTRY_F(fast423_156),
+    FMMREF_ENTRY_F(grey433_29_234),
+    FMMREF_ENTRY_F(grey343_29_234),
+    FMMREF_ENTRY_F(grey442_26_257),
+    FMMREF_ENTRY_F(grey424_26_257),
+    FMMREF_ENTRY_F(grey424_26_206),
+    FMMREF_ENTRY_F(grey522_18_99),
+    FMMREF_ENTRY_F(grey252_18_99),
+    FMMREF_ENTRY_F(smirnov336_40_960),
+    FMMREF_ENTRY_F(smirnov363_40_960),
+    FMMREF_ENTRY_F(smirnov633_40_960),
+    FMMREF_ENTRY_F(tichavsky_kovac336_40_960),
+    FMMREF_ENTRY_F(tichavsky_kovac363_40_960),
+};
+
 }  // namespace
 
 extern "C" {
@@ -152,6 +207,29 @@ void fmmref_matmul(double* a, int lda, double* b, int ldb, double* c, int ldc, i
   Matrix<double> A(a, lda, m, k);
   Matrix<double> B(b, ldb, k, n);
   Matrix<double> C(c, ldc, m, n, alpha);
+  MatMul(A, B, C, beta);
+}
+
+// <name>::FastMatmul<float> on caller buffers; -1 for an unknown name.
+double fmmref_fast_matmul_f32(const char* name, float* a, int lda, float* b, int ldb, float* c, int ldc, int m, int k,
+                              int n, int num_steps, double x, float alpha, float beta) {
+  for (const EntryF& e : kEntriesF) {
+    if (std::strcmp(e.name, name) == 0) {
+      Matrix<float> A(a, lda, m, k);
+      Matrix<float> B(b, ldb, k, n);
+      Matrix<float> C(c, ldc, m, n);
+      return e.fn(A, B, C, num_steps, x, alpha, beta);
+    }
+  }
+  return -1.0;
+}
+
+// MatMul<float>: C <- alpha * A * B + beta * C through the host sgemm.
+void fmmref_matmul_f32(float* a, int lda, float* b, int ldb, float* c, int ldc, int m, int k, int n, float alpha,
+                       float beta) {
+  Matrix<float> A(a, lda, m, k);
+  Matrix<float> B(b, ldb, k, n);
+  Matrix<float> C(c, ldc, m, n, alpha);
   MatMul(A, B, C, beta);
 }
 

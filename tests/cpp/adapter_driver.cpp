@@ -68,6 +68,24 @@ int main() {
     MatMul(A11, B12, C2v);
     expect(MaxRelativeDiff(C1v, C2v) <= 1e-13, "strassen on strided views max rel diff", MaxRelativeDiff(C1v, C2v));
   }
+  // Scalar = float (scaling/fast_scaling.cpp runs strassen::FastMatmul on
+  // Matrix<float>): FP32 results of the fast and the classical product agree
+  // to about one FP32 rounding
+  {
+    Matrix<float> A = RandomMatrix<float>(300, 260);
+    Matrix<float> B = RandomMatrix<float>(260, 280);
+    Matrix<float> C1(300, 280), C2(300, 280);
+    strassen::FastMatmul(A, B, C1, 2);
+    MatMul(A, B, C2);
+    expect(MaxRelativeDiff(C1, C2) <= 1e-6, "float strassen steps=2 vs MatMul<float>", MaxRelativeDiff(C1, C2));
+    Matrix<float> C3 = RandomMatrix<float>(300, 280);
+    Matrix<float> C4 = C3;
+    grey424_26_206::FastMatmul(A, B, C3, 1, 1e-8, 2.0f, 0.5f);
+    C4.set_multiplier(2.0f);
+    MatMul(A, B, C4, 0.5f);
+    expect(MaxRelativeDiff(C3, C4) <= 1e-6, "float grey424 alpha=2 beta=0.5 vs MatMul<float>",
+           MaxRelativeDiff(C3, C4));
+  }
   // diagonal scaling (benchmarks/scaling_stability.cpp pattern): rows of A
   // and columns of B skewed by 2^-30..2^30; scaled Strassen back within the
   // classical product's error

@@ -192,3 +192,21 @@ def test_scaling_multiplies_into_vectors_that_arrive_sized():
     r2, s2 = oracle.scaling(A2, B2, 2, 0, ref=True, r=r0, s=s0)
     assert np.array_equal(r1, r2) and np.array_equal(s1, s2)
     assert not np.array_equal(r1, oracle.scaling(A.copy(order="F"), B.copy(order="F"), 2, 0)[0])
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference build not present")
+def test_reference_fp32_build_rounds_in_fp32():
+    """The reference's FastMatmul<float> / MatMul<float> (sgemm) built here:
+    errors of FP32 arithmetic against the exact product of the FP32 inputs."""
+    n = 256
+    A = np.asfortranarray(oracle.uniform(n, n, 1, 1).astype(np.float32))
+    B = np.asfortranarray(oracle.uniform(n, n, 1, 2).astype(np.float32))
+    want = A.astype(np.float64) @ B.astype(np.float64)
+    C = np.zeros((n, n), dtype=np.float32, order="F")
+    oracle.ref_fast_matmul_f32("strassen", A, B, C, 2)
+    e = float((np.abs(C - want) / want).max())
+    assert 1e-8 < e < 1e-4, e
+    C[:] = 0
+    oracle.ref_matmul_f32(A, B, C)
+    e = float((np.abs(C - want) / want).max())
+    assert 1e-9 < e < 1e-5, e
