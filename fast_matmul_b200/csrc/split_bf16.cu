@@ -29,9 +29,9 @@
 // (A_t, B_u) over one 128-deep chunk (48 KB) into a 4-stage ring, counted on
 // the leader's full barrier; the leader's warp 1 issues 8 MMAs per stage
 // into one of four TMEM accumulators of 128 FP32 columns and multicasts its
-// commits to both CTAs; warps 2-9 of each CTA (two warpgroups of 64
-// columns) drain each finished accumulator into FP64 registers and release
-// it on the leader's barrier.  Every mbarrier wait is bounded; on a timeout
+// commits to both CTAs; the epilogue warps of each CTA (two or four
+// warpgroups, splitting the 128 columns) drain each finished accumulator
+// into FP64 registers and release it on the leader's barrier.  Every mbarrier wait is bounded; on a timeout
 // the kernel records a code in *err, lets its copies and MMAs in flight
 // finish, frees its TMEM and returns.
 
@@ -61,9 +61,12 @@ constexpr int kStageBytes = kStageKBlocks * (kATileBytes + kBTileBytes);
 constexpr int kStages = 4;
 constexpr int kAccBufs = 4;  // TMEM accumulators of 128 FP32 columns
 constexpr uint16_t kPairMask = 0x3;  // both CTAs of the cluster
-// TMA warp, MMA warp, 2 x 4 epilogue warps.  Registers are budgeted per
-// group of four warps, so the 10 warps are charged as 12: 168 per thread.
-constexpr int kGemmThreads = 320;
+// TMA warp, MMA warp, kEpiGroups x 4 epilogue warps, each warpgroup owning
+// kBN / kEpiGroups columns of the tile.  Few slices mean few products per
+// drained diagonal, so the drains weigh more: 3 slices or fewer use four
+// warpgroups of 32 columns (measured +6-8% at 3 slices), more slices two of
+// 64 (four were 2% slower at 5).
+constexpr int gemm_threads(int epi_groups) { return 32 * (2 + 4 * epi_groups); }
 constexpr size_t kGemmSmem = (size_t)kStages * kStageBytes + 1024;
 static_assert(kChunkBlocks == 2 && kChunkBlocks % kStageKBlocks == 0, "stages tile the chunk");
 static_assert(kBK * 2 == 128, "one k-block row is one 128-byte swizzle row");
@@ -287,9 +290,13 @@ __device__ __forceinline__ TileCoord tile_coord(const GemmParams& g, int64_t til
   return c;
 }
 
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
+template <int kEpiGroups>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(gemm_threads(kEpiGroups), 1)
     split_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                       const GemmParams g) {
+  constexpr int kEpiCols = kBN / kEpiGroups;
+  constexpr int kEpiWarps = 4 * kEpiGroups;
+  static_assert(kEpiCols % 16 == 0, "drains move pairs of 8-column pieces");
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   // full: the leader's count both CTAs' copies of a stage; empty, acc_full:
@@ -309,7 +316,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
     }
     for (int b = 0; b < kAccBufs; ++b) {
       mbar_init(&acc_full[b], 1);
-      mbar_init(&acc_empty[b], 16);
+      mbar_init(&acc_empty[b], 2 * kEpiWarps);
     }
     mbar_init(&mma_done, 1);
     fence_barrier_init();
@@ -421,7 +428,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
       mbar_drain(&mma_done, 0, 1000000000ull);
     }
   } else {
-    // warpgroup wg owns columns [64 wg, 64 wg + 64) of the tile; warp
+    // warpgroup wg owns columns [kEpiCols wg, kEpiCols (wg + 1)) of the tile; warp
     // quadrant qd owns TMEM lanes (this CTA's tile rows) [32 qd, 32 qd + 32)
     const int wg = (warp - 2) >> 2, qd = warp & 3;
     const int row_in_tile = qd * 32 + lane;
@@ -431,9 +438,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
       const TileCoord tc = tile_coord(g, tile);
       const SplitDesc& s = g.desc[tc.q];
       const int chunks = s.kblocks / kChunkBlocks;
-      double acc[64];
+      double acc[kEpiCols];
 #pragma unroll
-      for (int j = 0; j < 64; ++j) acc[j] = 0.0;
+      for (int j = 0; j < kEpiCols; ++j) acc[j] = 0.0;
       for (int c = 0; c < chunks && ok; ++c)
         for (int D = 0; D < S; ++D, ++ai) {
           const int buf = ai % kAccBufs;
@@ -443,21 +450,21 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
           }
           tc_fence_after();
           const double scale = ldexp(1.0, -8 * (D + 2));
-          const uint32_t taddr = tmem + ((uint32_t)(qd * 32) << 16) + buf * kBN + wg * 64;
+          const uint32_t taddr = tmem + ((uint32_t)(qd * 32) << 16) + buf * kBN + wg * kEpiCols;
           // eight pieces of 8 columns, software-pipelined: the load of piece
           // g + 1 is in flight while piece g is converted and accumulated
           uint32_t r0[8], r1[8];
           tmem_ld_32x32b_x8(taddr, r0);
           tmem_ld_wait();
 #pragma unroll
-          for (int g8 = 0; g8 < 8; g8 += 2) {
+          for (int g8 = 0; g8 < kEpiCols / 8; g8 += 2) {
             tmem_ld_32x32b_x8(taddr + (g8 + 1) * 8, r1);
 #pragma unroll
             for (int j = 0; j < 8; ++j)
               acc[g8 * 8 + j] = fma((double)__uint_as_float(r0[j]), scale, acc[g8 * 8 + j]);
             tmem_ld_wait();
-            if (g8 + 2 < 8) tmem_ld_32x32b_x8(taddr + (g8 + 2) * 8, r0);
-            if (g8 + 2 == 8) {  // the accumulator is free once the last piece is in registers
+            if (g8 + 2 < kEpiCols / 8) tmem_ld_32x32b_x8(taddr + (g8 + 2) * 8, r0);
+            if (g8 + 2 == kEpiCols / 8) {  // the accumulator is free once the last piece is in registers
               tc_fence_before();
               __syncwarp();
               if (lane == 0) mbar_arrive_cluster(cluster_addr(&acc_empty[buf], 0));  // the leader's
@@ -465,19 +472,19 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
 #pragma unroll
             for (int j = 0; j < 8; ++j)
               acc[(g8 + 1) * 8 + j] = fma((double)__uint_as_float(r1[j]), scale, acc[(g8 + 1) * 8 + j]);
-            if (g8 + 2 < 8) tmem_ld_wait();
+            if (g8 + 2 < kEpiCols / 8) tmem_ld_wait();
           }
         }
       if (!ok) break;
       const int64_t row = (int64_t)tc.tm * kSplitPairRows + rank * kBM + row_in_tile;
       if (row < s.m) {
         const int er = g.ea[s.e_off + row];
-        const int64_t col0 = (int64_t)tc.tn * kBN + wg * 64;
+        const int64_t col0 = (int64_t)tc.tn * kBN + wg * kEpiCols;
         const int* fcol = g.fb + s.f_off + col0;
         double* cp = s.C + row;
         const double alpha = s.alpha, beta = s.beta;
 #pragma unroll
-        for (int j = 0; j < 64; ++j) {
+        for (int j = 0; j < kEpiCols; ++j) {
           const int64_t col = col0 + j;
           if (col < s.n) {
             double v = __dmul_rn(alpha, ldexp(acc[j], er + fcol[j]));
@@ -587,14 +594,19 @@ cudaError_t split_gemm_launch(const SplitDesc* d_descs, int n, const SplitPlan& 
   {
     std::lock_guard<std::mutex> lock(mu);
     if (dev < 0 || dev >= 64 || !opted_in[dev]) {
-      e = cudaFuncSetAttribute(split_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem);
+      e = cudaFuncSetAttribute(split_gemm_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem);
+      if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(split_gemm_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem);
       if (e != cudaSuccess) return e;
       if (dev >= 0 && dev < 64) opted_in[dev] = true;
     }
   }
   // CTA pairs: the grid is even and a pair's CTAs are consecutive blocks
   const unsigned pairs = grid_for(plan.tiles, num_sms / 2 > 0 ? num_sms / 2 : 1);
-  split_gemm_kernel<<<2 * pairs, kGemmThreads, kGemmSmem, stream>>>(tA, tB, gp);
+  if (plan.slices <= 3)
+    split_gemm_kernel<4><<<2 * pairs, gemm_threads(4), kGemmSmem, stream>>>(tA, tB, gp);
+  else
+    split_gemm_kernel<2><<<2 * pairs, gemm_threads(2), kGemmSmem, stream>>>(tA, tB, gp);
   e = cudaGetLastError();
   if (e == cudaSuccess && launches) *launches += 4;
   return e;
