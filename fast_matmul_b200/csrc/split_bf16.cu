@@ -103,25 +103,45 @@ __device__ __forceinline__ double scale_pow2(double x, int e) {
   return ldexp(x, -e);
 }
 
-// Row exponents of A: one thread per padded row (coalesced down each column).
-__global__ void __launch_bounds__(256) split_row_exponents(const SplitDesc* __restrict__ d, int nd, int64_t total,
-                                                           int* __restrict__ ea) {
-  for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < total; x += (int64_t)gridDim.x * blockDim.x) {
-    const int q = find_desc(d, nd, x, [](const SplitDesc& s) { return s.e_off; });
+// Row exponents of A.  A block owns 32 padded rows (lane = row, so each
+// column load of a warp is 256 contiguous bytes) and its kExpWarps warps
+// split the columns, 8 loads in flight per thread; the warps' maxima meet
+// in shared memory.  (One thread per row walking all k columns left a
+// single large product with a few dozen blocks, latency-bound.)
+constexpr int kExpWarps = 16;
+
+__global__ void __launch_bounds__(kExpWarps * 32) split_row_exponents(const SplitDesc* __restrict__ d, int nd,
+                                                                      int64_t row_tiles, int* __restrict__ ea) {
+  __shared__ double part[kExpWarps][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int64_t w = blockIdx.x; w < row_tiles; w += gridDim.x) {
+    const int64_t x0 = w * 32;  // padded rows of one problem come in multiples of 256
+    const int q = find_desc(d, nd, x0, [](const SplitDesc& s) { return s.e_off; });
     const SplitDesc& s = d[q];
-    const int64_t i = x - s.e_off;
+    const int64_t i = x0 - s.e_off + lane;
     double mx = 0.0;
     if (i < s.m) {
       const double* a = s.A + i;
       const int64_t lda = s.lda;
-      int p = 0;
-      for (; p + 4 <= s.k; p += 4) {
-        const double v0 = a[p * lda], v1 = a[(p + 1) * lda], v2 = a[(p + 2) * lda], v3 = a[(p + 3) * lda];
-        mx = fmax(mx, fmax(fmax(fabs(v0), fabs(v1)), fmax(fabs(v2), fabs(v3))));
+      int p = warp;
+      for (; p + 7 * kExpWarps < s.k; p += 8 * kExpWarps) {
+        double v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) v[u] = a[(int64_t)(p + u * kExpWarps) * lda];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) mx = fmax(mx, fabs(v[u]));
       }
-      for (; p < s.k; ++p) mx = fmax(mx, fabs(a[p * lda]));
+      for (; p < s.k; p += kExpWarps) mx = fmax(mx, fabs(a[(int64_t)p * lda]));
     }
-    ea[x] = exponent_above(mx);
+    part[warp][lane] = mx;
+    __syncthreads();
+    if (warp == 0) {
+      double v = part[0][lane];
+#pragma unroll
+      for (int u = 1; u < kExpWarps; ++u) v = fmax(v, part[u][lane]);
+      ea[x0 + lane] = exponent_above(v);
+    }
+    __syncthreads();  // part is reused by the next row tile
   }
 }
 
@@ -162,21 +182,34 @@ __global__ void __launch_bounds__(256) split_a(const SplitDesc* __restrict__ d, 
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
   const int row = threadIdx.x >> 3, kc = (threadIdx.x & 7) * 8;
   auto at = [](int k, int r) { return k * 32 + (r ^ (((k >> 3) & 3) << 2)); };
+  // The next tile's loads are issued before this tile's digits are computed
+  // and stored, so each thread keeps a tile of loads in flight.
+  auto load = [&](int64_t w, double (&v)[8]) {
+    const int q = find_desc(d, nd, w, [](const SplitDesc& s) { return s.sa_begin; });
+    const SplitDesc& s = d[q];
+    const int64_t mp = (int64_t)s.tiles_m * kBM;
+    const int64_t local = w - s.sa_begin;
+    const int64_t i = (local % (mp / 32)) * 32 + tx, p0 = (local / (mp / 32)) * kBK;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const int64_t p = p0 + ty + 8 * r;
+      v[r] = (i < s.m && p < s.k) ? s.A[i + p * s.lda] : 0.0;
+    }
+  };
+  double pre[8];
+  if ((int64_t)blockIdx.x < total) load(blockIdx.x, pre);
   for (int64_t w = blockIdx.x; w < total; w += gridDim.x) {
     const int q = find_desc(d, nd, w, [](const SplitDesc& s) { return s.sa_begin; });
     const SplitDesc& s = d[q];
     const int64_t mp = (int64_t)s.tiles_m * kBM;
     const int64_t local = w - s.sa_begin;
     const int64_t rt = local % (mp / 32), kb = local / (mp / 32);
-    const int64_t i0 = rt * 32, p0 = kb * kBK;
+    const int64_t i0 = rt * 32;
     __syncthreads();  // previous tile's readers are done
 #pragma unroll
-    for (int r = 0; r < 8; ++r) {
-      const int k = ty + 8 * r;
-      const int64_t p = p0 + k, i = i0 + tx;
-      tile[at(k, tx)] = (i < s.m && p < s.k) ? s.A[i + p * s.lda] : 0.0;
-    }
+    for (int r = 0; r < 8; ++r) tile[at(ty + 8 * r, tx)] = pre[r];
     __syncthreads();
+    if (w + gridDim.x < total) load(w + gridDim.x, pre);
     const int e = ea[s.e_off + i0 + row];
     double x[8];
 #pragma unroll
@@ -570,7 +603,8 @@ cudaError_t split_gemm_launch(const SplitDesc* d_descs, int n, const SplitPlan& 
   int* ea = reinterpret_cast<int*>(base + plan.off_e);
   int* fb = reinterpret_cast<int*>(base + plan.off_f);
   const int64_t cap = (int64_t)num_sms * 16;
-  split_row_exponents<<<grid_for((plan.n_e + 255) / 256, cap), 256, 0, stream>>>(d_descs, n, plan.n_e, ea);
+  split_row_exponents<<<grid_for(plan.n_e / 32, (int64_t)num_sms * 4), kExpWarps * 32, 0, stream>>>(d_descs, n,
+                                                                                             plan.n_e / 32, ea);
   split_a<<<grid_for(plan.sa_work, cap), 256, 0, stream>>>(d_descs, n, plan.sa_work, plan.slices, ea, as);
   split_b<<<grid_for(plan.n_f, cap), 256, 0, stream>>>(d_descs, n, plan.n_f, plan.slices, fb, bs);
   cudaError_t e = cudaGetLastError();
