@@ -303,9 +303,12 @@ struct TileCoord {
 
 // Tiles of a problem (256 x 128, one per CTA pair; tm counts 256-row tiles)
 // are walked in groups of kRasterRows tile rows, row index fastest within a
-// group: the pairs of one wave cover a compact block of the output, so the
-// A and B slices they read stay in L2 between them.
-constexpr int kRasterRows = 8;
+// group: the pairs of one wave share A slices across a group's columns and B
+// slices down its rows, so both stay in L2 between them.  Measured on one
+// B200 at 16384^3 and 8192^3 (5 and 3 slices, and Strassen's 49-leaf
+// launches): groups of 1 and 2 pair rows within noise of each other, 4 about
+// 1.5% and 8 about 3% slower, 16 slower still.
+constexpr int kRasterRows = 2;
 
 __device__ __forceinline__ TileCoord tile_coord(const GemmParams& g, int64_t tile) {
   TileCoord c;
