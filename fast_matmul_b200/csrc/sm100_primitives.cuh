@@ -1,6 +1,8 @@
-// sm_100a building blocks written directly in PTX: mbarriers with bounded
-// waits, TMA tile loads (cp.async.bulk.tensor), tensor-memory allocation,
-// tcgen05 MMA issue / commit and tensor-memory loads.
+// sm_100a building blocks written directly in PTX for CTA pairs (clusters of
+// two, the two-SM MMA): mbarriers with bounded waits, cluster barriers and
+// remote arrives, TMA tile loads (cp.async.bulk.tensor.cta_group::2),
+// tensor-memory allocation, tcgen05 MMA issue / commit and tensor-memory
+// loads.
 //
 // Every wait gives up after kWaitLimitNs of wall-clock time (the device's
 // global timer): it records a code in the caller's error word and returns
@@ -129,14 +131,6 @@ __device__ __forceinline__ void mbar_arrive_cluster(uint32_t bar_cluster_addr) {
 
 // ---- TMA
 
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];\n" ::
-          "r"(smem_addr(dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_addr(bar)), "r"(c0), "r"(c1)
-      : "memory");
-}
-
 // Tile load into this CTA's shared memory for a two-SM MMA: the byte count
 // completes on the mbarrier at cluster address `bar` (the pair leader's).
 __device__ __forceinline__ void tma_load_2d_pair(void* dst, const CUtensorMap* map, uint32_t bar, int c0, int c1) {
@@ -153,21 +147,9 @@ __device__ __forceinline__ void prefetch_tensormap(const CUtensorMap* map) {
 
 // ---- tensor memory
 
-// Allocates `ncols` (power of two >= 32) columns; one whole warp calls it.
-// The base address is written to *slot (shared memory).
-__device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols) {
-  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_addr(slot)),
-               "r"(ncols)
-               : "memory");
-  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
-}
-
-__device__ __forceinline__ void tmem_dealloc(uint32_t base, uint32_t ncols) {
-  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(base), "r"(ncols) : "memory");
-}
-
-// The same for a CTA pair: the warp with the same index in both CTAs calls
-// them, with the same `slot` offset.
+// Tensor memory of a CTA pair: the warp with the same index in both CTAs
+// allocates `ncols` (power of two >= 32) columns, the base address written to
+// *slot (the same shared-memory offset in both), and frees them.
 __device__ __forceinline__ void tmem_alloc_pair(uint32_t* slot, uint32_t ncols) {
   asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_addr(slot)),
                "r"(ncols)
@@ -211,19 +193,10 @@ __host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
-// D[tmem] (+)= A[smem] * B[smem]^T, issued by one thread.
-__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
-                                         bool accumulate) {
-  asm volatile(
-      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d_tmem),
-      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"((uint32_t)accumulate)
-      : "memory");
-}
-
-// Two-SM form (issued by the pair leader only): A rows 0-127 from the
-// leader's shared memory and 128-255 from the peer's at the same offset, B
-// columns split in halves the same way, D rows in each CTA's tensor memory.
+// D[tmem] (+)= A[smem] * B[smem]^T in the two-SM form, issued by one thread
+// of the pair leader: A rows 0-127 from the leader's shared memory and
+// 128-255 from the peer's at the same offset, B columns split in halves the
+// same way, D rows in each CTA's tensor memory.
 __device__ __forceinline__ void mma_bf16_pair(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
                                               bool accumulate) {
   asm volatile(
@@ -243,42 +216,12 @@ __device__ __forceinline__ void mma_commit_pair(uint64_t* bar, uint16_t cta_mask
       : "memory");
 }
 
-// Arrives on `bar` once all previously issued MMAs of this thread complete.
-__device__ __forceinline__ void mma_commit(uint64_t* bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
-                   smem_addr(bar))
-               : "memory");
-}
-
-// 32 lanes x 32 consecutive 32-bit columns into 32 registers per thread.
-__device__ __forceinline__ void tmem_ld_32x32b_x32(uint32_t taddr, uint32_t (&r)[32]) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-      : "r"(taddr)
-      : "memory");
-}
-
 // 32 lanes x 8 consecutive 32-bit columns into 8 registers per thread.
 __device__ __forceinline__ void tmem_ld_32x32b_x8(uint32_t taddr, uint32_t (&r)[8]) {
   asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
                : "r"(taddr)
                : "memory");
-}
-
-// 32 lanes x 16 consecutive 32-bit columns into 16 registers per thread.
-__device__ __forceinline__ void tmem_ld_32x32b_x16(uint32_t taddr, uint32_t (&r)[16]) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr)
-      : "memory");
 }
 
 __device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
