@@ -234,25 +234,62 @@ def committed_traffic(name="roofline_traffic.json"):
         return None
 
 
+class Replicas:
+    """N independent replicas, one process per GPU (torch.distributed.run):
+    the only collectives are a barrier around the timed region and the
+    maximum over ranks of a measured time.  `backend` is "nccl" on GPUs
+    ("gloo" lets the same logic run on host processes); with WORLD_SIZE 1
+    nothing is initialised.  Every rank calls the same methods in the same
+    order."""
+
+    def __init__(self, backend: str = "nccl", device=None, timeout_s: float = 600.0):
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        self.dist = dist
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.device = device if device is not None else torch.device("cpu")
+        if self.world > 1:
+            kw = {"device_id": self.device} if backend == "nccl" else {}
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s), **kw)
+
+    def barrier(self) -> None:
+        if self.world > 1:
+            self.dist.barrier()
+
+    def max(self, value: float) -> float:
+        """The maximum of `value` over the ranks (every rank gets it)."""
+        import torch
+
+        t = torch.tensor([value], dtype=torch.float64, device=self.device)
+        if self.world > 1:
+            self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def whole_job_rate(self, units_per_rank: float, seconds_max: float) -> float:
+        """Units all ranks processed per second of the slowest rank."""
+        return self.world * units_per_rank / seconds_max
+
+    def close(self) -> None:
+        if self.world > 1:
+            self.barrier()
+            self.dist.destroy_process_group()
+
+
 def run_ours(a):
     import torch
-    import torch.distributed as dist
 
     import fast_matmul_b200 as fmm
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
+    rep = Replicas("nccl", torch.device("cuda", local))
+    world, rank = rep.world, rep.rank
+    barrier = rep.barrier
 
     m, k, n = a.m, a.k, a.n
     h = fmm.default_handle(local)
@@ -290,12 +327,9 @@ def run_ours(a):
     h.profile(False)
     clk = clocks.stop()
 
-    t = torch.tensor([elapsed_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    t_max = float(t.item())
+    t_max = rep.max(elapsed_ms)
     ms_step = t_max / a.steps
-    value = world * flops * a.steps / (t_max * 1e-3) / 1e12
+    value = rep.whole_job_rate(flops * a.steps, t_max * 1e-3) / 1e12
 
     # ---- classical comparators and error (outside the timed region)
     Cc = fmm.colmajor_empty(m, n, torch.device("cuda", local))
@@ -342,11 +376,8 @@ def run_ours(a):
         for _ in range(e2e_steps):
             fmm.fast_matmul_host(a.alg, Ah, Bh, Ch, a.num_steps, schedule=a.schedule, handle=h)
         e2e_s = time.perf_counter() - t0
-        te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-        if world > 1:
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        e2e_s = float(te.item())
-        e2e = {"value": world * flops * e2e_steps / e2e_s / 1e12, "unit": "TFLOP/s",
+        e2e_s = rep.max(e2e_s)
+        e2e = {"value": rep.whole_job_rate(flops * e2e_steps, e2e_s) / 1e12, "unit": "TFLOP/s",
                "h2d_bytes_per_step": 8 * (m * k + k * n), "d2h_bytes_per_step": 8 * m * n,
                "ms_per_step": e2e_s * 1e3 / e2e_steps, "api": "fmm_fast_matmul_host (include/fmm.h)"}
         del Ah, Bh, Ch
@@ -418,9 +449,7 @@ def run_ours(a):
             "workspace_bytes": fmm.workspace_bytes(a.alg, m, k, n, a.num_steps, a.schedule, handle=h),
         }
         print(json.dumps(out))
-    if world > 1:
-        barrier()
-        dist.destroy_process_group()
+    rep.close()
     return 0
 
 
