@@ -507,49 +507,43 @@ void build_program(int alg, int64_t m, int64_t k, int64_t n, int steps, double x
   place_split_scratch(out, static_cast<char*>(ws));
 }
 
-namespace {
-
 // Split scratch of a batch: one split launch per distinct slice count, all
-// sharing one region.
-size_t batch_split_bytes(const BatchItem* items, int count) {
-  std::map<int, SplitPlan> plans;
-  for (int i = 0; i < count; ++i) {
-    const BatchItem& it = items[i];
-    if (it.split_slices <= 0) continue;
-    SplitPlan& p = plans[it.split_slices];
-    p.slices = it.split_slices;
-    if (it.classical) {
-      split_accumulate(&p, it.m, it.k, it.n, 1);
-      continue;
-    }
+// sharing one region sized for the largest.
+void BatchFootprint::add(const BatchItem& it) {
+  if (!it.classical) {
     const fmm_alg_table& t = fmm_algorithms[it.alg];
-    const std::vector<LevelDims> dims = level_dims(t, it.m, it.k, it.n, it.steps);
-    int64_t leaves = 1;
-    for (int l = 0; l < it.steps; ++l) leaves *= t.rank;
-    split_accumulate(&p, dims[(size_t)it.steps].m, dims[(size_t)it.steps].k, dims[(size_t)it.steps].n, leaves);
+    size_t end = 0;
+    layout(t, level_dims(t, it.m, it.k, it.n, it.steps), it.steps, 0, 0, &end);
+    fp64_ += (size_t)round_up((int64_t)end, 256);  // items are laid out back to back, 256-byte aligned
   }
-  size_t mx = 0;
-  for (auto& kv : plans) {
-    split_finish(&kv.second);
-    if (kv.second.tiles > 0) mx = std::max(mx, kv.second.bytes);
+  if (it.split_slices <= 0) return;
+  SplitPlan& p = split_[it.split_slices];
+  p.slices = it.split_slices;
+  if (it.classical) {
+    split_accumulate(&p, it.m, it.k, it.n, 1);
+    return;
   }
-  return mx;
+  const fmm_alg_table& t = fmm_algorithms[it.alg];
+  const std::vector<LevelDims> dims = level_dims(t, it.m, it.k, it.n, it.steps);
+  int64_t leaves = 1;
+  for (int l = 0; l < it.steps; ++l) leaves *= t.rank;
+  split_accumulate(&p, dims[(size_t)it.steps].m, dims[(size_t)it.steps].k, dims[(size_t)it.steps].n, leaves);
 }
 
-}  // namespace
+size_t BatchFootprint::bytes() const {
+  size_t mx = 0;
+  for (const auto& kv : split_) {
+    SplitPlan p = kv.second;
+    split_finish(&p);
+    if (p.tiles > 0) mx = std::max(mx, p.bytes);
+  }
+  return mx > 0 ? (size_t)round_up((int64_t)fp64_, 1024) + mx : fp64_;
+}
 
 size_t batch_workspace_bytes(const BatchItem* items, int count) {
-  size_t off = 0;
-  for (int i = 0; i < count; ++i) {
-    if (items[i].classical) continue;
-    const fmm_alg_table& t = fmm_algorithms[items[i].alg];
-    size_t end = 0;
-    layout(t, level_dims(t, items[i].m, items[i].k, items[i].n, items[i].steps), items[i].steps, 0, off, &end);
-    off = (size_t)round_up((int64_t)end, 256);
-  }
-  const size_t sb = batch_split_bytes(items, count);
-  if (sb > 0) off = (size_t)round_up((int64_t)off, 1024) + sb;
-  return off;
+  BatchFootprint f;
+  for (int i = 0; i < count; ++i) f.add(items[i]);
+  return f.bytes();
 }
 
 void build_batch_program(const BatchItem* items, int count, void* ws, Program* out) {

@@ -5,6 +5,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <map>
 #include <vector>
 
 #include "fmm_internal.h"
@@ -102,6 +103,19 @@ struct BatchItem {
 
 // Workspace of a batch (every item planned breadth-first, regions back to back).
 size_t batch_workspace_bytes(const BatchItem* items, int count);
+
+// The same footprint built one item at a time (batch_workspace_bytes uses
+// it): a request loop can price each candidate in O(1) instead of laying
+// the whole batch out again.
+class BatchFootprint {
+ public:
+  void add(const BatchItem& it);
+  size_t bytes() const;
+
+ private:
+  size_t fp64_ = 0;                 // FP64 temporaries of the items, 256-byte aligned each
+  std::map<int, SplitPlan> split_;  // split-BF16 leaves per slice count (one launch each)
+};
 
 // Builds one program for the whole batch: operand formations level by level
 // (one launch per algorithm and level over all items), ONE grouped GEMM over

@@ -193,6 +193,7 @@ bool turn(fmm_server s) {
     if (sl.busy || s->pending.empty()) continue;
     std::vector<fmm::BatchItem> batch;
     std::vector<uint64_t> tickets;
+    fmm::BatchFootprint footprint;
     size_t need = 0;
     const size_t avail = largest_free(s);
     while (!s->pending.empty() && (int)batch.size() < s->max_batch) {
@@ -215,12 +216,13 @@ bool turn(fmm_server s) {
       }
       // the footprint of the batch with this request, laid out as the batch
       // program lays it out (alignment between items included)
-      std::vector<fmm::BatchItem> trial = batch;
-      trial.insert(trial.end(), one.begin(), one.end());
-      const size_t total = trial.empty() ? 0 : fmm::batch_workspace_bytes(trial.data(), (int)trial.size());
+      fmm::BatchFootprint trial = footprint;
+      for (const fmm::BatchItem& b : one) trial.add(b);
+      const size_t total = trial.bytes();
       if (total + 256 > avail) break;  // admit in order: wait for memory
       need = (total + 255) & ~(size_t)255;
-      batch.swap(trial);
+      footprint = trial;
+      batch.insert(batch.end(), one.begin(), one.end());
       tickets.push_back(p.ticket);
       s->pending.pop_front();
     }
