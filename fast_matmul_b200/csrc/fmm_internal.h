@@ -46,6 +46,41 @@ constexpr int kSplitPairRows = 2 * kSplitTile;  // rows of the tile of a CTA pai
 constexpr int kSplitKBlock = 64;  // k-depth of one TMA box (128 bytes of BF16)
 constexpr int kSplitChunk = 128;  // k-depth accumulated exactly in FP32 (two k-blocks)
 
+// Accumulation groups of one output tile, in order: for each pair of
+// 128-deep k-chunks, diagonal 0 over both chunks, diagonal 1 over both, then
+// diagonals 2..S-1 of the first chunk and of the second (a last single chunk
+// forms its own pair).  Pairs are used at 3 slices or fewer, where they save
+// a third of the drains; with more slices every chunk forms its own group
+// set (diagonals 0..S-1), which measured faster on Strassen's leaf launches.  With digits |d_1| <= 256 and |d_t| <= 128 every FP32
+// partial sum of a group stays an integer of magnitude <= 2^24 -- diagonals
+// 0 and 1 add at most 2^16 per k over 256 k, diagonal D >= 2 at most
+// (D + 3) 2^14 per k over 128 k -- so the tensor cores accumulate each group
+// exactly, and the FP64 recombination adds the groups in this order.
+struct SplitGroup {
+  int D;       // diagonal: slice pairs (t, D - t), t = 0..D (0-based slices)
+  int c0, c1;  // chunks [c0, c1)
+};
+
+// Chunks per pair (1 or 2) and groups of a pair of nch chunks.
+__host__ __device__ inline int split_chunk_span(int slices) { return slices <= 3 ? 2 : 1; }
+__host__ __device__ inline int split_groups_in_pair(int nch, int slices) { return 2 + nch * (slices - 2); }
+
+// Group gi of the chunk pair starting at chunk cp (nch = 1 or 2 chunks).
+__host__ __device__ inline SplitGroup split_group(int cp, int nch, int slices, int gi) {
+  SplitGroup g;
+  if (gi < 2) {
+    g.D = gi;
+    g.c0 = cp;
+    g.c1 = cp + nch;
+  } else {
+    const int r = gi - 2;
+    g.D = 2 + r % (slices - 2);
+    g.c0 = cp + r / (slices - 2);
+    g.c1 = g.c0 + 1;
+  }
+  return g;
+}
+
 struct SplitDesc {
   const double* A;
   const double* B;

@@ -10,11 +10,13 @@
 //     |d_1| <= 256 and |d_t| <= 128 are exact BF16 values;
 //   * C_ij = alpha 2^(e_i + f_j) sum_{t+u <= S+1} 2^-8(t+u) (dA_t dB_u)_ij,
 //     S (S + 1) / 2 slice products.  The products of one diagonal t + u are
-//     accumulated by the tensor cores in FP32 over k chunks of 128: every
-//     partial sum is an integer of magnitude <= 2^24, so the accumulation is
-//     exact.  After each chunk the diagonal's sum is scaled by 2^-8(t+u) and
-//     added into an FP64 accumulator: all rounding happens in FP64, in a
-//     fixed order.
+//     accumulated by the tensor cores in FP32 over a group of k: 256 deep for
+//     the diagonals t + u = 2, 3 at 3 slices or fewer, 128 deep otherwise
+//     (SplitGroup in fmm_internal.h); every partial sum is an integer of
+//     magnitude <= 2^24,
+//     so the accumulation is exact.  Each group's sum is scaled by
+//     2^-8(t+u) and added into an FP64 accumulator: all rounding happens in
+//     FP64, in a fixed order.
 // Error: |x - sum_t d_t 2^-8t| <= 2^-(8S+1) 2^e per operand entry plus the
 // dropped diagonals, so |C - AB| <~ 3 * 2^-8S * k * max|a_i.| * max|b_.j|.
 //
@@ -326,12 +328,36 @@ __device__ __forceinline__ TileCoord tile_coord(const GemmParams& g, int64_t til
   return c;
 }
 
+// Calls fn(D, c0, c1) for the accumulation groups of a tile in order
+// (split_group), until fn returns false; returns whether all ran.  With one
+// chunk per group the loops are the plain chunk-then-diagonal order.
+template <int kSpan, class Fn>
+__device__ __forceinline__ bool for_each_group(int chunks, int S, Fn&& fn) {
+  if constexpr (kSpan == 1) {
+    for (int c = 0; c < chunks; ++c)
+      for (int D = 0; D < S; ++D)
+        if (!fn(D, c, c + 1)) return false;
+  } else {
+    for (int cp = 0; cp < chunks; cp += kSpan) {
+      const int nch = min(kSpan, chunks - cp);
+      for (int gi = 0; gi < split_groups_in_pair(nch, S); ++gi) {
+        const SplitGroup G = split_group(cp, nch, S, gi);
+        if (!fn(G.D, G.c0, G.c1)) return false;
+      }
+    }
+  }
+  return true;
+}
+
 template <int kEpiGroups>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(gemm_threads(kEpiGroups), 1)
     split_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                       const GemmParams g) {
   constexpr int kEpiCols = kBN / kEpiGroups;
   constexpr int kEpiWarps = 4 * kEpiGroups;
+  // chunks per accumulation pair: the four-warpgroup form runs 3 slices or
+  // fewer, where split_chunk_span pairs chunks (the launch checks this)
+  constexpr int kSpan = kEpiGroups == 4 ? 2 : 1;
   static_assert(kEpiCols % 16 == 0, "drains move pairs of 8-column pieces");
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -378,14 +404,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(gemm_threads(kEpiGro
         const int64_t ya_tile = s.a_row + (int64_t)tc.tm * kSplitPairRows + rank * kBM;
         const int64_t yb_tile = s.b_row + (int64_t)tc.tn * kBN + rank * kBHalf;
         const int chunks = s.kblocks / kChunkBlocks;
-        for (int c = 0; c < chunks && ok; ++c)
-          for (int D = 0; D < S && ok; ++D)
-            for (int t = 0; t <= D && ok; ++t)
+        ok = for_each_group<kSpan>(chunks, S, [&](int D, int c0, int c1) {
+          for (int c = c0; c < c1; ++c)
+            for (int t = 0; t <= D; ++t)
               for (int h = 0; h < kChunkBlocks; h += kStageKBlocks) {
-                if (n >= (uint32_t)kStages && !mbar_wait(&empty[st], ph ^ 1u, g.err, 1)) {
-                  ok = false;
-                  break;
-                }
+                if (n >= (uint32_t)kStages && !mbar_wait(&empty[st], ph ^ 1u, g.err, 1)) return false;
                 const int64_t blk = (int64_t)c * kChunkBlocks + h;
                 const int64_t ya = ya_tile + ((int64_t)t * s.kblocks + blk) * mp;
                 const int64_t yb = yb_tile + ((int64_t)(D - t) * s.kblocks + blk) * np;
@@ -404,6 +427,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(gemm_threads(kEpiGro
                   ph ^= 1u;
                 }
               }
+          return true;
+        });
       }
       // Before the CTA can leave, its copies must have landed: each stage's
       // last round is released by the MMAs that read it, which waited for
@@ -424,22 +449,16 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(gemm_threads(kEpiGro
       for (int64_t tile = pair; tile < g.tiles && ok; tile += pairs) {
         const TileCoord tc = tile_coord(g, tile);
         const int chunks = g.desc[tc.q].kblocks / kChunkBlocks;
-        for (int c = 0; c < chunks && ok; ++c)
-          for (int D = 0; D < S && ok; ++D, ++ai) {
-            const uint32_t buf = ai % kAccBufs;
-            if (ai >= (uint32_t)kAccBufs &&
-                !mbar_wait(&acc_empty[buf], ((ai / kAccBufs) - 1) & 1, g.err, 2)) {
-              ok = false;
-              break;
-            }
-            tc_fence_after();
-            const uint32_t d_tmem = tmem + buf * kBN;
-            for (int t = 0; t <= D && ok; ++t)
+        ok = for_each_group<kSpan>(chunks, S, [&](int D, int c0, int c1) {
+          const uint32_t buf = ai % kAccBufs;
+          if (ai >= (uint32_t)kAccBufs && !mbar_wait(&acc_empty[buf], ((ai / kAccBufs) - 1) & 1, g.err, 2))
+            return false;
+          tc_fence_after();
+          const uint32_t d_tmem = tmem + buf * kBN;
+          for (int c = c0; c < c1; ++c)
+            for (int t = 0; t <= D; ++t)
               for (int h = 0; h < kChunkBlocks; h += kStageKBlocks) {
-                if (!mbar_wait(&full[st], ph, g.err, 3)) {
-                  ok = false;
-                  break;
-                }
+                if (!mbar_wait(&full[st], ph, g.err, 3)) return false;
                 tc_fence_after();
                 const uint32_t a = smem_addr(base + st * kStageBytes);
                 const uint32_t b = a + kStageKBlocks * kATileBytes;
@@ -448,7 +467,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(gemm_threads(kEpiGro
                   const uint32_t koff = (kk & 3) * 32;
                   mma_bf16_pair(d_tmem, smem_desc_sw128(a + (kk >> 2) * kATileBytes + koff),
                                 smem_desc_sw128(b + (kk >> 2) * kBTileBytes + koff), idesc,
-                                t > 0 || h > 0 || kk > 0);
+                                c > c0 || t > 0 || h > 0 || kk > 0);
                 }
                 mma_commit_pair(&empty[st], kPairMask);
                 if (++st == (uint32_t)kStages) {
@@ -456,8 +475,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(gemm_threads(kEpiGro
                   ph ^= 1u;
                 }
               }
-            if (ok) mma_commit_pair(&acc_full[buf], kPairMask);
-          }
+          mma_commit_pair(&acc_full[buf], kPairMask);
+          ++ai;
+          return true;
+        });
       }
       // every MMA issued by this thread completes before tensor memory is freed
       mma_commit_pair(&mma_done, 0x1);
@@ -477,13 +498,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(gemm_threads(kEpiGro
       double acc[kEpiCols];
 #pragma unroll
       for (int j = 0; j < kEpiCols; ++j) acc[j] = 0.0;
-      for (int c = 0; c < chunks && ok; ++c)
-        for (int D = 0; D < S; ++D, ++ai) {
+      ok = for_each_group<kSpan>(chunks, S, [&](int D, int, int) {
           const int buf = ai % kAccBufs;
-          if (!mbar_wait(&acc_full[buf], (ai / kAccBufs) & 1, g.err, 4)) {
-            ok = false;
-            break;
-          }
+          if (!mbar_wait(&acc_full[buf], (ai / kAccBufs) & 1, g.err, 4)) return false;
           tc_fence_after();
           const double scale = ldexp(1.0, -8 * (D + 2));
           const uint32_t taddr = tmem + ((uint32_t)(qd * 32) << 16) + buf * kBN + wg * kEpiCols;
@@ -510,7 +527,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(gemm_threads(kEpiGro
               acc[(g8 + 1) * 8 + j] = fma((double)__uint_as_float(r1[j]), scale, acc[(g8 + 1) * 8 + j]);
             if (g8 + 2 < kEpiCols / 8) tmem_ld_wait();
           }
-        }
+          ++ai;
+          return true;
+        });
       if (!ok) break;
       const int64_t row = (int64_t)tc.tm * kSplitPairRows + rank * kBM + row_in_tile;
       if (row < s.m) {
@@ -640,6 +659,7 @@ cudaError_t split_gemm_launch(const SplitDesc* d_descs, int n, const SplitPlan& 
   }
   // CTA pairs: the grid is even and a pair's CTAs are consecutive blocks
   const unsigned pairs = grid_for(plan.tiles, num_sms / 2 > 0 ? num_sms / 2 : 1);
+  if (split_chunk_span(plan.slices) != (plan.slices <= 3 ? 2 : 1)) return cudaErrorInvalidValue;
   if (plan.slices <= 3)
     split_gemm_kernel<4><<<2 * pairs, gemm_threads(4), kGemmSmem, stream>>>(tA, tB, gp);
   else

@@ -13,7 +13,8 @@
 //
 // Split-BF16 leaf products are executed by a model of the device arithmetic
 // (power-of-two scaling, 8-bit digit slices, exact integer sums per
-// diagonal and 128-deep k-chunk, FP64 recombination in the device's order),
+// diagonal and accumulation group of k (SplitGroup), FP64 recombination in
+// the device's order),
 // so the device result must equal the model's bit for bit.
 
 #include <algorithm>
@@ -178,9 +179,12 @@ void split_product(const fmm::SplitDesc& d, int slices) {
   }
   std::vector<double> acc((size_t)m * n, 0.0), part((size_t)m * n);
   const int chunks = std::max(1, (k + fmm::kSplitChunk - 1) / fmm::kSplitChunk);
-  for (int c = 0; c < chunks; ++c) {
-    const int p0 = c * fmm::kSplitChunk, p1 = std::min(k, p0 + fmm::kSplitChunk);
-    for (int D = 0; D < S; ++D) {
+  for (int cp = 0; cp < chunks; cp += fmm::split_chunk_span(S)) {
+    const int nch = std::min(fmm::split_chunk_span(S), chunks - cp);
+    for (int gi = 0; gi < fmm::split_groups_in_pair(nch, S); ++gi) {
+      const fmm::SplitGroup G = fmm::split_group(cp, nch, S, gi);
+      const int D = G.D;
+      const int p0 = G.c0 * fmm::kSplitChunk, p1 = std::min(k, G.c1 * fmm::kSplitChunk);
       std::fill(part.begin(), part.end(), 0.0);
       for (int t = 0; t <= D; ++t)
         for (int p = p0; p < p1; ++p) {
