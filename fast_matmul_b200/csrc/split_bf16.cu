@@ -26,16 +26,16 @@
 // A rows 0-127 and B columns 0-63 from the leader's shared memory, A rows
 // 128-255 and B columns 64-127 from the peer's, and accumulates each CTA's
 // 128 rows in its own tensor memory.  One issuing thread thus drives two
-// SMs, halving the per-MMA issue work (the limit of the one-SM form) and the
-// B traffic per SM.  In each CTA warp 0 issues TMA loads of its halves of
-// (A_t, B_u) over one 128-deep chunk (48 KB) into a 4-stage ring, counted on
-// the leader's full barrier; the leader's warp 1 issues 8 MMAs per stage
-// into one of four TMEM accumulators of 128 FP32 columns and multicasts its
-// commits to both CTAs; the epilogue warps of each CTA (two or four
-// warpgroups, splitting the 128 columns) drain each finished accumulator
-// into FP64 registers and release it on the leader's barrier.  Every mbarrier wait is bounded; on a timeout
-// the kernel records a code in *err, lets its copies and MMAs in flight
-// finish, frees its TMEM and returns.
+// SMs, and each SM reads half of B.  In each CTA warp 0 issues TMA loads of
+// its halves of (A_t, B_u) over one 128-deep chunk (48 KB) into a 4-stage
+// ring, counted on the leader's full barrier; the leader's warp 1 issues 8
+// MMAs per stage into one of four TMEM accumulators of 128 FP32 columns and
+// multicasts its commits to both CTAs; the epilogue warps of each CTA (two
+// or four warpgroups, splitting the 128 columns) drain each finished
+// accumulator into FP64 registers and release it on the leader's barrier.
+// Every mbarrier wait is bounded; on a timeout the kernel records a code in
+// *err, lets its copies and MMAs in flight finish, frees its TMEM and
+// returns.
 
 #include <cuda.h>
 #include <cuda_bf16.h>
