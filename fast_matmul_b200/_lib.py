@@ -180,6 +180,19 @@ SIGNATURES = {
                                       ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
                                       ctypes.c_int64, ctypes.c_int64, ctypes.c_float, ctypes.c_float,
                                       ctypes.POINTER(Options)]),
+    "fmm_diagonal_scaling_f32": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+                                                 ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
+                                                 ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]),
+    "fmm_scaling_postprocess_f32": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                                    ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p,
+                                                    ctypes.c_void_p]),
+    "fmm_diagonal_scaling_f32_host": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                                      ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
+                                                      ctypes.c_int64, ctypes.c_int64, ctypes.c_int, ctypes.c_int,
+                                                      ctypes.c_void_p, ctypes.c_void_p]),
+    "fmm_scaling_postprocess_f32_host": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                                         ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p,
+                                                         ctypes.c_void_p]),
     "fmm_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
     "fmm_kernel_launch_count": (ctypes.c_int64, [ctypes.c_void_p]),
     "fmm_selftest_wait_timeout": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.POINTER(ctypes.c_int)]),

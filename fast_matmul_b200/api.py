@@ -346,16 +346,17 @@ def diagonal_scaling(A, B, num_steps: int, scaling_type=OUTSIDE_INSIDE, r_vals=N
     kind = _SCALING_TYPES.get(scaling_type, scaling_type) if isinstance(scaling_type, str) else scaling_type
     if isinstance(kind, str):
         raise ValueError("Unknown iteration type.")
-    pa, lda = _mat(A, m, k, "A")
-    pb, ldb = _mat(B, k, n, "B")
-    r = torch.ones(m, dtype=torch.float64, device=A.device) if r_vals is None else r_vals
-    s = torch.ones(n, dtype=torch.float64, device=A.device) if s_vals is None else s_vals
+    dt = A.dtype if A.dtype == torch.float32 else torch.float64  # float32: Scaling<float>
+    pa, lda = _mat(A, m, k, "A", dt)
+    pb, ldb = _mat(B, k, n, "B", dt)
+    r = torch.ones(m, dtype=dt, device=A.device) if r_vals is None else r_vals
+    s = torch.ones(n, dtype=dt, device=A.device) if s_vals is None else s_vals
     for v, size, name in ((r, m, "r_vals"), (s, n, "s_vals")):
-        if v.dtype != torch.float64 or tuple(v.shape) != (size,) or (size > 1 and v.stride(0) != 1):
-            raise ValueError("%s must be a contiguous float64 vector of length %d" % (name, size))
+        if v.dtype != dt or tuple(v.shape) != (size,) or (size > 1 and v.stride(0) != 1):
+            raise ValueError("%s must be a contiguous %s vector of length %d" % (name, dt, size))
     h = handle or default_handle(A.device.index)
-    check(lib().fmm_diagonal_scaling(h.ptr, pa, lda, pb, ldb, m, k, n, num_steps, int(kind), r.data_ptr(),
-                                     s.data_ptr()))
+    fn = lib().fmm_diagonal_scaling_f32 if dt == torch.float32 else lib().fmm_diagonal_scaling
+    check(fn(h.ptr, pa, lda, pb, ldb, m, k, n, num_steps, int(kind), r.data_ptr(), s.data_ptr()))
     return r, s
 
 
@@ -364,12 +365,14 @@ def scaling_postprocess(C, r_vals, s_vals, handle: Optional[Handle] = None) -> N
     C(i, j) := (C(i, j) * r_vals[i]) * s_vals[j] on the device."""
     torch = _torch()
     m, n = C.shape
-    pc, ldc = _mat(C, m, n, "C")
+    dt = C.dtype if C.dtype == torch.float32 else torch.float64
+    pc, ldc = _mat(C, m, n, "C", dt)
     for v, size, name in ((r_vals, m, "r_vals"), (s_vals, n, "s_vals")):
-        if v.dtype != torch.float64 or tuple(v.shape) != (size,) or (size > 1 and v.stride(0) != 1):
-            raise ValueError("%s must be a contiguous float64 vector of length %d" % (name, size))
+        if v.dtype != dt or tuple(v.shape) != (size,) or (size > 1 and v.stride(0) != 1):
+            raise ValueError("%s must be a contiguous %s vector of length %d" % (name, dt, size))
     h = handle or default_handle(C.device.index)
-    check(lib().fmm_scaling_postprocess(h.ptr, pc, ldc, m, n, r_vals.data_ptr(), s_vals.data_ptr()))
+    fn = lib().fmm_scaling_postprocess_f32 if dt == torch.float32 else lib().fmm_scaling_postprocess
+    check(fn(h.ptr, pc, ldc, m, n, r_vals.data_ptr(), s_vals.data_ptr()))
 
 
 # ---------------------------------------------------------------------------

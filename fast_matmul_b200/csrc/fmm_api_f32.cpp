@@ -202,3 +202,122 @@ fmm_status fmm_sgemm_host(fmm_handle h, const float* A, int64_t lda, const float
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Diagonal scaling with Scalar = float: Scaling<float> / PostProcessScaling
+// (scaling/scaling.hpp:143-196), as the reference's scaling/fast_scaling.cpp
+// runs it on Matrix<float>.
+
+extern "C" {
+
+fmm_status fmm_diagonal_scaling_f32(fmm_handle h, float* A, int64_t lda, float* B, int64_t ldb, int64_t m, int64_t k,
+                                    int64_t n, int num_steps, int type, float* r, float* s) {
+  if (!h) return fail(FMM_ERR_INVALID_ARGUMENT, "null handle");
+  fmm_status st = check_dims(m, k, n, lda, ldb, m > 1 ? m : 1);
+  if (st != FMM_OK) return st;
+  if (num_steps < 0) return fail(FMM_ERR_INVALID_ARGUMENT, "num_steps must be >= 0");
+  if (type < FMM_SCALING_OUTSIDE_INSIDE || type > FMM_SCALING_OUTSIDE)
+    return fail(FMM_ERR_INVALID_ARGUMENT, "Unknown iteration type.");
+  if ((m > 0 && !r) || (n > 0 && !s)) return fail(FMM_ERR_INVALID_ARGUMENT, "null factor pointer");
+  if ((m * k > 0 && !A) || (k * n > 0 && !B)) return fail(FMM_ERR_INVALID_ARGUMENT, "null matrix pointer");
+  DeviceGuard g(h->device);
+  if (!g.ok()) return fail(FMM_ERR_CUDA, "cudaSetDevice failed");
+  st = ensure_device_buffer(h, &h->scal, &h->scal_cap, fmm::scaling_scratch_bytes(m, k, n), "scaling scratch");
+  if (st != FMM_OK) return st;
+  FMM_CUDA_TRY(fmm::scaling_launch(A, lda, B, ldb, (int)m, (int)k, (int)n, num_steps, type, r, s, h->scal, h->stream,
+                                   &h->launches),
+               "diagonal scaling");
+  return FMM_OK;
+}
+
+fmm_status fmm_scaling_postprocess_f32(fmm_handle h, float* C, int64_t ldc, int64_t m, int64_t n, const float* r,
+                                       const float* s) {
+  if (!h) return fail(FMM_ERR_INVALID_ARGUMENT, "null handle");
+  fmm_status st = check_dims(m, 0, n, m > 1 ? m : 1, 1, ldc);
+  if (st != FMM_OK) return st;
+  if (m == 0 || n == 0) return FMM_OK;
+  if (!C || !r || !s) return fail(FMM_ERR_INVALID_ARGUMENT, "null pointer");
+  DeviceGuard g(h->device);
+  if (!g.ok()) return fail(FMM_ERR_CUDA, "cudaSetDevice failed");
+  FMM_CUDA_TRY(fmm::scaling_postprocess_launch(C, ldc, (int)m, (int)n, r, s, h->stream, &h->launches),
+               "scaling postprocess");
+  return FMM_OK;
+}
+
+fmm_status fmm_diagonal_scaling_f32_host(fmm_handle h, float* A, int64_t lda, float* B, int64_t ldb, int64_t m,
+                                         int64_t k, int64_t n, int num_steps, int type, float* r, float* s) {
+  if (!h) return fail(FMM_ERR_INVALID_ARGUMENT, "null handle");
+  fmm_status st = check_dims(m, k, n, lda, ldb, m > 1 ? m : 1);
+  if (st != FMM_OK) return st;
+  if ((m > 0 && !r) || (n > 0 && !s)) return fail(FMM_ERR_INVALID_ARGUMENT, "null factor pointer");
+  if ((m * k > 0 && !A) || (k * n > 0 && !B)) return fail(FMM_ERR_INVALID_ARGUMENT, "null matrix pointer");
+  DeviceGuard g(h->device);
+  if (!g.ok()) return fail(FMM_ERR_CUDA, "cudaSetDevice failed");
+  const size_t na = pad32((size_t)m * (size_t)k), nb = pad32((size_t)k * (size_t)n);
+  if ((st = ensure_device_buffer(h, &h->narrow_io, &h->narrow_io_cap,
+                                 (na + nb + pad32((size_t)m) + pad32((size_t)n)) * sizeof(float),
+                                 "host-call operands")) != FMM_OK)
+    return st;
+  float* dA = static_cast<float*>(h->narrow_io);
+  float* dB = dA + na;
+  float* dr = dB + nb;
+  float* ds = dr + pad32((size_t)m);
+  const int64_t ldA = m > 1 ? m : 1, ldB = k > 1 ? k : 1;
+  if (m * k > 0)
+    FMM_CUDA_TRY(cudaMemcpy2DAsync(dA, ldA * sizeof(float), A, lda * sizeof(float), m * sizeof(float), k,
+                                   cudaMemcpyHostToDevice, h->stream),
+                 "copy A to device");
+  if (k * n > 0)
+    FMM_CUDA_TRY(cudaMemcpy2DAsync(dB, ldB * sizeof(float), B, ldb * sizeof(float), k * sizeof(float), n,
+                                   cudaMemcpyHostToDevice, h->stream),
+                 "copy B to device");
+  if (m) FMM_CUDA_TRY(cudaMemcpyAsync(dr, r, m * sizeof(float), cudaMemcpyHostToDevice, h->stream), "copy r");
+  if (n) FMM_CUDA_TRY(cudaMemcpyAsync(ds, s, n * sizeof(float), cudaMemcpyHostToDevice, h->stream), "copy s");
+  st = fmm_diagonal_scaling_f32(h, dA, ldA, dB, ldB, m, k, n, num_steps, type, dr, ds);
+  if (st != FMM_OK) return st;
+  if (m * k > 0)
+    FMM_CUDA_TRY(cudaMemcpy2DAsync(A, lda * sizeof(float), dA, ldA * sizeof(float), m * sizeof(float), k,
+                                   cudaMemcpyDeviceToHost, h->stream),
+                 "copy A to host");
+  if (k * n > 0)
+    FMM_CUDA_TRY(cudaMemcpy2DAsync(B, ldb * sizeof(float), dB, ldB * sizeof(float), k * sizeof(float), n,
+                                   cudaMemcpyDeviceToHost, h->stream),
+                 "copy B to host");
+  if (m) FMM_CUDA_TRY(cudaMemcpyAsync(r, dr, m * sizeof(float), cudaMemcpyDeviceToHost, h->stream), "copy r back");
+  if (n) FMM_CUDA_TRY(cudaMemcpyAsync(s, ds, n * sizeof(float), cudaMemcpyDeviceToHost, h->stream), "copy s back");
+  FMM_CUDA_TRY(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+  return FMM_OK;
+}
+
+fmm_status fmm_scaling_postprocess_f32_host(fmm_handle h, float* C, int64_t ldc, int64_t m, int64_t n,
+                                            const float* r, const float* s) {
+  if (!h) return fail(FMM_ERR_INVALID_ARGUMENT, "null handle");
+  fmm_status st = check_dims(m, 0, n, m > 1 ? m : 1, 1, ldc);
+  if (st != FMM_OK) return st;
+  if (m == 0 || n == 0) return FMM_OK;
+  if (!C || !r || !s) return fail(FMM_ERR_INVALID_ARGUMENT, "null pointer");
+  DeviceGuard g(h->device);
+  if (!g.ok()) return fail(FMM_ERR_CUDA, "cudaSetDevice failed");
+  const size_t nc = pad32((size_t)m * (size_t)n);
+  if ((st = ensure_device_buffer(h, &h->narrow_io, &h->narrow_io_cap,
+                                 (nc + pad32((size_t)m) + pad32((size_t)n)) * sizeof(float),
+                                 "host-call operands")) != FMM_OK)
+    return st;
+  float* dC = static_cast<float*>(h->narrow_io);
+  float* dr = dC + nc;
+  float* ds = dr + pad32((size_t)m);
+  FMM_CUDA_TRY(cudaMemcpy2DAsync(dC, m * sizeof(float), C, ldc * sizeof(float), m * sizeof(float), n,
+                                 cudaMemcpyHostToDevice, h->stream),
+               "copy C to device");
+  FMM_CUDA_TRY(cudaMemcpyAsync(dr, r, m * sizeof(float), cudaMemcpyHostToDevice, h->stream), "copy r");
+  FMM_CUDA_TRY(cudaMemcpyAsync(ds, s, n * sizeof(float), cudaMemcpyHostToDevice, h->stream), "copy s");
+  st = fmm_scaling_postprocess_f32(h, dC, m, m, n, dr, ds);
+  if (st != FMM_OK) return st;
+  FMM_CUDA_TRY(cudaMemcpy2DAsync(C, ldc * sizeof(float), dC, m * sizeof(float), m * sizeof(float), n,
+                                 cudaMemcpyDeviceToHost, h->stream),
+               "copy C to host");
+  FMM_CUDA_TRY(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+  return FMM_OK;
+}
+
+}  // extern "C"

@@ -196,6 +196,11 @@ cudaError_t scaling_launch(double* A, int64_t lda, double* B, int64_t ldb, int m
 // C(i,j) = (C(i,j) * r[i]) * s[j].
 cudaError_t scaling_postprocess_launch(double* C, int64_t ldc, int m, int n, const double* r, const double* s,
                                        cudaStream_t stream, int64_t* launches);
+// The same with Scalar = float (the reference's Scaling<float> arithmetic).
+cudaError_t scaling_launch(float* A, int64_t lda, float* B, int64_t ldb, int m, int k, int n, int num_steps,
+                           int type, float* r, float* s, void* scratch, cudaStream_t stream, int64_t* launches);
+cudaError_t scaling_postprocess_launch(float* C, int64_t ldc, int m, int n, const float* r, const float* s,
+                                       cudaStream_t stream, int64_t* launches);
 
 // ---------------------------------------------------------------------------
 // FP32 <-> FP64 conversions of column-major matrices (convert.cu).

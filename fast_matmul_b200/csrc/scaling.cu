@@ -13,9 +13,12 @@
 //
 // Every factor is the reference's own arithmetic: 1.0 / max (InverseVector,
 // :52-58), sqrt(max_col(A) / max_row(B)) (InnerScaling, :129-138), products
-// of two doubles (RowScale / ColScale / UpdateVals).  IEEE division, square
+// of two Scalars (RowScale / ColScale / UpdateVals).  IEEE division, square
 // root and multiplication are correctly rounded and a maximum is exact, so
-// the device result equals the reference's bit for bit.
+// the device result equals the reference's bit for bit.  With Scalar =
+// float the reference divides and takes the square root in double (its 1.0
+// is a double and MaxAbsRow / MaxAbsCol return double) and rounds the factor
+// to float on assignment; the float kernels do the same.
 
 #include <algorithm>
 
@@ -29,21 +32,46 @@ constexpr int kRows = 256;   // rows of a tile = threads of a block
 constexpr int kCols = 64;    // columns of a tile
 constexpr int kUnroll = 8;   // loads in flight per thread
 
-struct ScaleJob {
-  double* X;
-  int64_t ld;
-  int rows, cols;
-  const double* rowv;          // X(i,j) *= rowv[i] (null: none)
-  const double* colv;          // then X(i,j) *= colv[j] (null: none)
-  unsigned long long* rowmax;  // max_j |X(i,j)| of the result, as bits (null: not wanted)
-  unsigned long long* colmax;  // max_i |X(i,j)| of the result, as bits (null: not wanted)
-  int64_t tiles_r;             // ceil(rows / kRows)
-  int64_t tiles;               // tiles_r * ceil(cols / kCols)
+// Non-negative values order like their bit patterns: maxima are kept as
+// unsigned words of the same width and combined with atomicMax.
+template <class T>
+struct Bits;
+template <>
+struct Bits<double> {
+  using U = unsigned long long;
+};
+template <>
+struct Bits<float> {
+  using U = unsigned int;
 };
 
-ScaleJob make_job(double* X, int64_t ld, int rows, int cols, const double* rowv, const double* colv,
-                  unsigned long long* rowmax, unsigned long long* colmax) {
-  ScaleJob j;
+__device__ __forceinline__ unsigned long long to_bits(double x) { return (unsigned long long)__double_as_longlong(x); }
+__device__ __forceinline__ unsigned int to_bits(float x) { return __float_as_uint(x); }
+__device__ __forceinline__ double from_bits(unsigned long long b) { return __longlong_as_double((long long)b); }
+__device__ __forceinline__ float from_bits(unsigned int b) { return __uint_as_float(b); }
+__device__ __forceinline__ double vmax(double a, double b) { return fmax(a, b); }
+__device__ __forceinline__ float vmax(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ double vabs(double a) { return fabs(a); }
+__device__ __forceinline__ float vabs(float a) { return fabsf(a); }
+
+template <class T>
+struct ScaleJob {
+  using U = typename Bits<T>::U;
+  T* X;
+  int64_t ld;
+  int rows, cols;
+  const T* rowv;     // X(i,j) *= rowv[i] (null: none)
+  const T* colv;     // then X(i,j) *= colv[j] (null: none)
+  U* rowmax;         // max_j |X(i,j)| of the result, as bits (null: not wanted)
+  U* colmax;         // max_i |X(i,j)| of the result, as bits (null: not wanted)
+  int64_t tiles_r;   // ceil(rows / kRows)
+  int64_t tiles;     // tiles_r * ceil(cols / kCols)
+};
+
+template <class T>
+ScaleJob<T> make_job(T* X, int64_t ld, int rows, int cols, const T* rowv, const T* colv,
+                     typename Bits<T>::U* rowmax, typename Bits<T>::U* colmax) {
+  ScaleJob<T> j;
   j.X = X;
   j.ld = ld;
   j.rows = rows;
@@ -62,24 +90,25 @@ ScaleJob make_job(double* X, int64_t ld, int rows, int cols, const double* rowv,
 // each lane keeps 4 of the columns and trades the other 4, at 8 it keeps 2,
 // at 4 one, then two plain steps.  9 shuffles instead of 8 x 5.  Returns the
 // maximum of column column_of_lane(lane), valid in lanes with lane % 4 == 0.
-__device__ __forceinline__ double warp_max8(const double (&a)[8], int lane) {
+template <class T>
+__device__ __forceinline__ T warp_max8(const T (&a)[8], int lane) {
   const bool h16 = lane & 16, h8 = lane & 8, h4 = lane & 4;
-  double b4[4], b2[2];
+  T b4[4], b2[2];
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
-    const double keep = h16 ? a[j + 4] : a[j];
-    const double send = h16 ? a[j] : a[j + 4];
-    b4[j] = fmax(keep, __shfl_xor_sync(0xffffffffu, send, 16));
+    const T keep = h16 ? a[j + 4] : a[j];
+    const T send = h16 ? a[j] : a[j + 4];
+    b4[j] = vmax(keep, __shfl_xor_sync(0xffffffffu, send, 16));
   }
 #pragma unroll
   for (int j = 0; j < 2; ++j) {
-    const double keep = h8 ? b4[j + 2] : b4[j];
-    const double send = h8 ? b4[j] : b4[j + 2];
-    b2[j] = fmax(keep, __shfl_xor_sync(0xffffffffu, send, 8));
+    const T keep = h8 ? b4[j + 2] : b4[j];
+    const T send = h8 ? b4[j] : b4[j + 2];
+    b2[j] = vmax(keep, __shfl_xor_sync(0xffffffffu, send, 8));
   }
-  double b = fmax(h4 ? b2[1] : b2[0], __shfl_xor_sync(0xffffffffu, h4 ? b2[0] : b2[1], 4));
-  b = fmax(b, __shfl_xor_sync(0xffffffffu, b, 2));
-  return fmax(b, __shfl_xor_sync(0xffffffffu, b, 1));
+  T b = vmax(h4 ? b2[1] : b2[0], __shfl_xor_sync(0xffffffffu, h4 ? b2[0] : b2[1], 4));
+  b = vmax(b, __shfl_xor_sync(0xffffffffu, b, 2));
+  return vmax(b, __shfl_xor_sync(0xffffffffu, b, 1));
 }
 
 __device__ __forceinline__ int column_of_lane(int lane) {
@@ -89,11 +118,12 @@ __device__ __forceinline__ int column_of_lane(int lane) {
 // Blocks [0, j0.tiles) work on j0, the rest on j1.  A tile is kRows rows x
 // kCols columns; thread t owns row t of the tile, so every column load of a
 // warp is 32 consecutive doubles.
-__global__ void __launch_bounds__(kRows) scale_reduce_kernel(ScaleJob j0, ScaleJob j1) {
-  __shared__ double s_colv[kCols];
-  __shared__ double s_part[kRows / 32][kCols];
+template <class T>
+__global__ void __launch_bounds__(kRows) scale_reduce_kernel(ScaleJob<T> j0, ScaleJob<T> j1) {
+  __shared__ T s_colv[kCols];
+  __shared__ T s_part[kRows / 32][kCols];
   const bool second = (int64_t)blockIdx.x >= j0.tiles;
-  const ScaleJob J = second ? j1 : j0;
+  const ScaleJob<T> J = second ? j1 : j0;
   const int64_t t = second ? (int64_t)blockIdx.x - j0.tiles : (int64_t)blockIdx.x;
   const int64_t tr = t % J.tiles_r;
   const int c0 = (int)(t / J.tiles_r) * kCols;
@@ -101,138 +131,141 @@ __global__ void __launch_bounds__(kRows) scale_reduce_kernel(ScaleJob j0, ScaleJ
   const int64_t i = tr * kRows + threadIdx.x;
   const bool in = i < J.rows;
   const bool scales = J.rowv != nullptr || J.colv != nullptr;
-  if (threadIdx.x < kCols) s_colv[threadIdx.x] = (J.colv && (int)threadIdx.x < nc) ? J.colv[c0 + threadIdx.x] : 1.0;
+  if (threadIdx.x < kCols) s_colv[threadIdx.x] = (J.colv && (int)threadIdx.x < nc) ? J.colv[c0 + threadIdx.x] : T(1);
   __syncthreads();
-  const double rv = (J.rowv && in) ? J.rowv[i] : 1.0;
-  double* p = J.X + (in ? i : 0) + (int64_t)c0 * J.ld;
+  const T rv = (J.rowv && in) ? J.rowv[i] : T(1);
+  T* p = J.X + (in ? i : 0) + (int64_t)c0 * J.ld;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double rmax = 0.0;
+  T rmax = T(0);
   static_assert(kUnroll == 8, "warp_max8 reduces 8 columns");
   for (int cb = 0; cb < nc; cb += kUnroll) {
-    double v[kUnroll], a[kUnroll];
-    double* q = p + (int64_t)cb * J.ld;
+    T v[kUnroll], a[kUnroll];
+    T* q = p + (int64_t)cb * J.ld;
 #pragma unroll
-    for (int u = 0; u < kUnroll; ++u) v[u] = (in && cb + u < nc) ? q[(int64_t)u * J.ld] : 0.0;
+    for (int u = 0; u < kUnroll; ++u) v[u] = (in && cb + u < nc) ? q[(int64_t)u * J.ld] : T(0);
 #pragma unroll
     for (int u = 0; u < kUnroll; ++u) {
       const int c = cb + u;
       if (J.rowv) v[u] = v[u] * rv;
       if (J.colv) v[u] = v[u] * s_colv[c];
       if (scales && in && c < nc) q[(int64_t)u * J.ld] = v[u];
-      a[u] = fabs(v[u]);
-      rmax = fmax(rmax, a[u]);
+      a[u] = vabs(v[u]);
+      rmax = vmax(rmax, a[u]);
     }
     if (J.colmax) {
-      const double w = warp_max8(a, lane);
+      const T w = warp_max8(a, lane);
       if ((lane & 3) == 0) s_part[warp][cb + column_of_lane(lane)] = w;
     }
   }
-  if (J.rowmax && in && rmax > 0.0) atomicMax(&J.rowmax[i], (unsigned long long)__double_as_longlong(rmax));
+  if (J.rowmax && in && rmax > T(0)) atomicMax(&J.rowmax[i], to_bits(rmax));
   if (J.colmax) {
     __syncthreads();
     if ((int)threadIdx.x < nc) {
-      double mx = 0.0;
+      T mx = T(0);
 #pragma unroll
-      for (int w = 0; w < kRows / 32; ++w) mx = fmax(mx, s_part[w][threadIdx.x]);
-      if (mx > 0.0) atomicMax(&J.colmax[c0 + threadIdx.x], (unsigned long long)__double_as_longlong(mx));
+      for (int w = 0; w < kRows / 32; ++w) mx = vmax(mx, s_part[w][threadIdx.x]);
+      if (mx > T(0)) atomicMax(&J.colmax[c0 + threadIdx.x], to_bits(mx));
     }
   }
 }
 
+template <class T>
 struct Factors {
+  using U = typename Bits<T>::U;
   int m, k, n;
-  int inner;                    // 0: outer factors, 1: inner factors
-  unsigned long long* row_a;    // max |A(i,:)|   (m)
-  unsigned long long* col_a;    // max |A(:,l)|   (k)
-  unsigned long long* row_b;    // max |B(l,:)|   (k)
-  unsigned long long* col_b;    // max |B(:,j)|   (n)
-  double* fa;                   // outer: 1 / x (m); inner: 1 / z (k)
-  double* fb;                   // outer: 1 / y (n); inner: z (k)
-  double* r;                    // outer: r *= x (m)
-  double* s;                    // outer: s *= y (n)
+  int inner;  // 0: outer factors, 1: inner factors
+  U* row_a;   // max |A(i,:)|   (m)
+  U* col_a;   // max |A(:,l)|   (k)
+  U* row_b;   // max |B(l,:)|   (k)
+  U* col_b;   // max |B(:,j)|   (n)
+  T* fa;      // outer: 1 / x (m); inner: 1 / z (k)
+  T* fb;      // outer: 1 / y (n); inner: z (k)
+  T* r;       // outer: r *= x (m)
+  T* s;       // outer: s *= y (n)
 };
 
 // Turns the maxima into factors, then clears every maximum for the next
-// pass.  Thread t alone reads and clears entry t of each array.
-__global__ void scale_factors_kernel(Factors F) {
+// pass.  Thread t alone reads and clears entry t of each array.  The
+// quotient and the square root are taken in double and rounded to T, as
+// the reference's 1.0 / vals[k] and sqrt(MaxAbsCol / MaxAbsRow) are.
+template <class T>
+__global__ void scale_factors_kernel(Factors<T> F) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (!F.inner) {
     // OuterScaling (:105-124) and UpdateVals (:93-98)
     if (t < F.m) {
-      const double x = __longlong_as_double((long long)F.row_a[t]);
-      F.fa[t] = 1.0 / x;
+      const T x = from_bits(F.row_a[t]);
+      F.fa[t] = (T)(1.0 / (double)x);
       F.r[t] = F.r[t] * x;
     }
     if (t < F.n) {
-      const double y = __longlong_as_double((long long)F.col_b[t]);
-      F.fb[t] = 1.0 / y;
+      const T y = from_bits(F.col_b[t]);
+      F.fb[t] = (T)(1.0 / (double)y);
       F.s[t] = F.s[t] * y;
     }
   } else if (t < F.k) {
     // InnerScaling (:129-138)
-    const double z = sqrt(__longlong_as_double((long long)F.col_a[t]) / __longlong_as_double((long long)F.row_b[t]));
-    F.fa[t] = 1.0 / z;
+    const T z = (T)sqrt((double)from_bits(F.col_a[t]) / (double)from_bits(F.row_b[t]));
+    F.fa[t] = (T)(1.0 / (double)z);
     F.fb[t] = z;
   }
-  if (t < F.m) F.row_a[t] = 0ull;
+  if (t < F.m) F.row_a[t] = 0;
   if (t < F.k) {
-    F.col_a[t] = 0ull;
-    F.row_b[t] = 0ull;
+    F.col_a[t] = 0;
+    F.row_b[t] = 0;
   }
-  if (t < F.n) F.col_b[t] = 0ull;
+  if (t < F.n) F.col_b[t] = 0;
 }
 
 // Every maximum cleared.  r and s keep the caller's starting values
 // (Scaling's resize(m, 1.0), scaling.hpp:158-159, keeps the entries of
 // vectors that arrive sized).
-__global__ void scale_init_kernel(Factors F) {
+template <class T>
+__global__ void scale_init_kernel(Factors<T> F) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < F.m) F.row_a[t] = 0ull;
-  if (t < F.n) F.col_b[t] = 0ull;
+  if (t < F.m) F.row_a[t] = 0;
+  if (t < F.n) F.col_b[t] = 0;
   if (t < F.k) {
-    F.col_a[t] = 0ull;
-    F.row_b[t] = 0ull;
+    F.col_a[t] = 0;
+    F.row_b[t] = 0;
   }
 }
 
-cudaError_t launch_jobs(const ScaleJob& j0, const ScaleJob& j1, cudaStream_t stream, int64_t* launches) {
+template <class T>
+cudaError_t launch_jobs(const ScaleJob<T>& j0, const ScaleJob<T>& j1, cudaStream_t stream, int64_t* launches) {
   const int64_t blocks = j0.tiles + j1.tiles;
   if (blocks == 0) return cudaSuccess;
   if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
-  scale_reduce_kernel<<<(unsigned)blocks, kRows, 0, stream>>>(j0, j1);
+  scale_reduce_kernel<T><<<(unsigned)blocks, kRows, 0, stream>>>(j0, j1);
   ++*launches;
   return cudaGetLastError();
 }
 
-// Array lengths padded to 32 entries (256 bytes).
+// Array lengths padded to 32 entries (256 bytes at 8 bytes an entry).
 int64_t pad32(int64_t v) { return (v + 31) / 32 * 32; }
 
-}  // namespace
-
-size_t scaling_scratch_bytes(int64_t m, int64_t k, int64_t n) {
-  // four maxima arrays and two factor arrays, each rounded to 256 bytes
-  return (size_t)8 * (size_t)(pad32(m) + 2 * pad32(k) + pad32(n) + pad32(std::max(m, k)) + pad32(std::max(n, k)));
-}
-
-cudaError_t scaling_launch(double* A, int64_t lda, double* B, int64_t ldb, int m, int k, int n, int num_steps,
-                           int type, double* r, double* s, void* scratch, cudaStream_t stream, int64_t* launches) {
-  Factors F;
+template <class T>
+cudaError_t scaling_impl(T* A, int64_t lda, T* B, int64_t ldb, int m, int k, int n, int num_steps, int type, T* r,
+                         T* s, void* scratch, cudaStream_t stream, int64_t* launches) {
+  using U = typename Bits<T>::U;
+  Factors<T> F;
   F.m = m;
   F.k = k;
   F.n = n;
-  unsigned long long* base = static_cast<unsigned long long*>(scratch);
-  F.row_a = base;
-  F.col_a = F.row_a + pad32(m);
-  F.row_b = F.col_a + pad32(k);
-  F.col_b = F.row_b + pad32(k);
-  F.fa = reinterpret_cast<double*>(F.col_b + pad32(n));
-  F.fb = F.fa + pad32(std::max(m, k));
+  // entries of 8 bytes whatever T is: the layout of scaling_scratch_bytes
+  char* base = static_cast<char*>(scratch);
+  F.row_a = reinterpret_cast<U*>(base);
+  F.col_a = reinterpret_cast<U*>(base + 8 * pad32(m));
+  F.row_b = reinterpret_cast<U*>(base + 8 * (pad32(m) + pad32(k)));
+  F.col_b = reinterpret_cast<U*>(base + 8 * (pad32(m) + 2 * pad32(k)));
+  F.fa = reinterpret_cast<T*>(base + 8 * (pad32(m) + 2 * pad32(k) + pad32(n)));
+  F.fb = reinterpret_cast<T*>(base + 8 * (pad32(m) + 2 * pad32(k) + pad32(n) + pad32(std::max(m, k))));
   F.r = r;
   F.s = s;
   F.inner = 0;
   const int64_t span = std::max<int64_t>(std::max(m, n), std::max(k, 1));
   const unsigned vec_blocks = (unsigned)((span + 255) / 256);
-  scale_init_kernel<<<vec_blocks, 256, 0, stream>>>(F);
+  scale_init_kernel<T><<<vec_blocks, 256, 0, stream>>>(F);
   ++*launches;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
@@ -251,15 +284,15 @@ cudaError_t scaling_launch(double* A, int64_t lda, double* B, int64_t ldb, int m
   if (total == 0) return cudaSuccess;
 
   // Maxima for the first scaling, read-only over both operands.
-  auto want = [&](bool inner, ScaleJob* ja, ScaleJob* jb) {
+  auto want = [&](bool inner, ScaleJob<T>* ja, ScaleJob<T>* jb) {
     ja->rowmax = inner ? nullptr : F.row_a;
     ja->colmax = inner ? F.col_a : nullptr;
     jb->rowmax = inner ? F.row_b : nullptr;
     jb->colmax = inner ? nullptr : F.col_b;
   };
   {
-    ScaleJob ja = make_job(A, lda, m, k, nullptr, nullptr, nullptr, nullptr);
-    ScaleJob jb = make_job(B, ldb, k, n, nullptr, nullptr, nullptr, nullptr);
+    ScaleJob<T> ja = make_job<T>(A, lda, m, k, nullptr, nullptr, nullptr, nullptr);
+    ScaleJob<T> jb = make_job<T>(B, ldb, k, n, nullptr, nullptr, nullptr, nullptr);
     want(ops[0], &ja, &jb);
     e = launch_jobs(ja, jb, stream, launches);
     if (e != cudaSuccess) return e;
@@ -267,14 +300,14 @@ cudaError_t scaling_launch(double* A, int64_t lda, double* B, int64_t ldb, int m
   for (int64_t q = 0; q < total; ++q) {
     const bool inner = ops[q % per_step];
     F.inner = inner ? 1 : 0;
-    scale_factors_kernel<<<vec_blocks, 256, 0, stream>>>(F);
+    scale_factors_kernel<T><<<vec_blocks, 256, 0, stream>>>(F);
     ++*launches;
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     // outer: rows of A by 1 / x, columns of B by 1 / y;
     // inner: columns of A by 1 / z, rows of B by z
-    ScaleJob ja = make_job(A, lda, m, k, inner ? nullptr : F.fa, inner ? F.fa : nullptr, nullptr, nullptr);
-    ScaleJob jb = make_job(B, ldb, k, n, inner ? F.fb : nullptr, inner ? nullptr : F.fb, nullptr, nullptr);
+    ScaleJob<T> ja = make_job<T>(A, lda, m, k, inner ? nullptr : F.fa, inner ? F.fa : nullptr, nullptr, nullptr);
+    ScaleJob<T> jb = make_job<T>(B, ldb, k, n, inner ? F.fb : nullptr, inner ? nullptr : F.fb, nullptr, nullptr);
     if (q + 1 < total) want(ops[(q + 1) % per_step], &ja, &jb);
     e = launch_jobs(ja, jb, stream, launches);
     if (e != cudaSuccess) return e;
@@ -282,11 +315,39 @@ cudaError_t scaling_launch(double* A, int64_t lda, double* B, int64_t ldb, int m
   return cudaSuccess;
 }
 
+template <class T>
+cudaError_t postprocess_impl(T* C, int64_t ldc, int m, int n, const T* r, const T* s, cudaStream_t stream,
+                             int64_t* launches) {
+  const ScaleJob<T> jc = make_job<T>(C, ldc, m, n, r, s, nullptr, nullptr);
+  const ScaleJob<T> none = make_job<T>(nullptr, 1, 0, 0, nullptr, nullptr, nullptr, nullptr);
+  return launch_jobs(jc, none, stream, launches);
+}
+
+}  // namespace
+
+size_t scaling_scratch_bytes(int64_t m, int64_t k, int64_t n) {
+  // four maxima arrays and two factor arrays of 8-byte entries, each rounded to 256 bytes
+  return (size_t)8 * (size_t)(pad32(m) + 2 * pad32(k) + pad32(n) + pad32(std::max(m, k)) + pad32(std::max(n, k)));
+}
+
+cudaError_t scaling_launch(double* A, int64_t lda, double* B, int64_t ldb, int m, int k, int n, int num_steps,
+                           int type, double* r, double* s, void* scratch, cudaStream_t stream, int64_t* launches) {
+  return scaling_impl<double>(A, lda, B, ldb, m, k, n, num_steps, type, r, s, scratch, stream, launches);
+}
+
+cudaError_t scaling_launch(float* A, int64_t lda, float* B, int64_t ldb, int m, int k, int n, int num_steps,
+                           int type, float* r, float* s, void* scratch, cudaStream_t stream, int64_t* launches) {
+  return scaling_impl<float>(A, lda, B, ldb, m, k, n, num_steps, type, r, s, scratch, stream, launches);
+}
+
 cudaError_t scaling_postprocess_launch(double* C, int64_t ldc, int m, int n, const double* r, const double* s,
                                        cudaStream_t stream, int64_t* launches) {
-  const ScaleJob jc = make_job(C, ldc, m, n, r, s, nullptr, nullptr);
-  const ScaleJob none = make_job(nullptr, 1, 0, 0, nullptr, nullptr, nullptr, nullptr);
-  return launch_jobs(jc, none, stream, launches);
+  return postprocess_impl<double>(C, ldc, m, n, r, s, stream, launches);
+}
+
+cudaError_t scaling_postprocess_launch(float* C, int64_t ldc, int m, int n, const float* r, const float* s,
+                                       cudaStream_t stream, int64_t* launches) {
+  return postprocess_impl<float>(C, ldc, m, n, r, s, stream, launches);
 }
 
 }  // namespace fmm

@@ -2,7 +2,8 @@
  * fmm.h -- C ABI of the B200 fast-matrix-multiplication engine (libfmm.so).
  *
  * Plain pointers and sizes only; no exceptions cross this boundary.  All
- * matrices are column-major doubles, as in the reference's Matrix<Scalar>
+ * matrices are column-major doubles (floats for the _f32 entry points and
+ * fmm_sgemm), as in the reference's Matrix<Scalar>
  * view (linalg/linalg.hpp:41-192): element (i, j) of a matrix with leading
  * dimension ld is at ptr[i + j * ld].  Unless a function says "host", its
  * matrix pointers are CUDA device pointers on the handle's device.
@@ -64,7 +65,8 @@ typedef enum fmm_schedule {
  *               of two and split into `split_slices` BF16 digit slices of 8
  *               bits; the S(S+1)/2 leading slice products run on the BF16
  *               tensor cores (tcgen05) with exact FP32 accumulation over
- *               k-chunks of 128, recombined in FP64.  Error of one leaf
+ *               k groups of 128 (256 for the two leading diagonals at 3
+ *               slices or fewer), recombined in FP64.  Error of one leaf
  *               product: |C - AB|_ij <~ 3 * 2^-8S * k * max|A_i.| * max|B_.j|;
  *               S = 5 stays near 1e-14 relative for well-scaled operands. */
 typedef enum fmm_precision {
@@ -230,6 +232,19 @@ fmm_status fmm_diagonal_scaling_host(fmm_handle h, double* A, int64_t lda, doubl
                                      int64_t k, int64_t n, int num_steps, int type, double* r, double* s);
 fmm_status fmm_scaling_postprocess_host(fmm_handle h, double* C, int64_t ldc, int64_t m, int64_t n, const double* r,
                                         const double* s);
+
+/* The four calls above with Scalar = float (Scaling<float>, as the
+ * reference's scaling/fast_scaling.cpp uses it): maxima and products in
+ * float, each 1.0 / max and sqrt(max / max) taken in double and rounded to
+ * float as the reference's template does; bit for bit its result. */
+fmm_status fmm_diagonal_scaling_f32(fmm_handle h, float* A, int64_t lda, float* B, int64_t ldb, int64_t m, int64_t k,
+                                    int64_t n, int num_steps, int type, float* r, float* s);
+fmm_status fmm_scaling_postprocess_f32(fmm_handle h, float* C, int64_t ldc, int64_t m, int64_t n, const float* r,
+                                       const float* s);
+fmm_status fmm_diagonal_scaling_f32_host(fmm_handle h, float* A, int64_t lda, float* B, int64_t ldb, int64_t m,
+                                         int64_t k, int64_t n, int num_steps, int type, float* r, float* s);
+fmm_status fmm_scaling_postprocess_f32_host(fmm_handle h, float* C, int64_t ldc, int64_t m, int64_t n,
+                                            const float* r, const float* s);
 
 /* Waits for all work queued on the handle's stream.  FMM_ERR_TIMEOUT if a
  * tensor-core kernel of a split-BF16 product gave up one of its bounded

@@ -90,6 +90,10 @@ def ref_lib() -> Optional[ctypes.CDLL]:
         L.fmmref_fast_matmul_f32.restype = _D
         L.fmmref_matmul_f32.argtypes = [_PF, _I, _PF, _I, _PF, _I, _I, _I, _I, _F, _F]
         L.fmmref_matmul_f32.restype = None
+        L.fmmref_scaling_f32.argtypes = [_PF, _I, _PF, _I, _I, _I, _I, _I, _I, _PF, _PF]
+        L.fmmref_scaling_f32.restype = None
+        L.fmmref_scaling_postprocess_f32.argtypes = [_PF, _I, _I, _I, _PF, _PF]
+        L.fmmref_scaling_postprocess_f32.restype = None
         L.fmmref_set_threads.argtypes = [_I]
         L.fmmref_scaling.argtypes = [_P, _I, _P, _I, _I, _I, _I, _I, _I, _P, _P]
         L.fmmref_scaling.restype = None
@@ -204,6 +208,29 @@ def ref_matmul_f32(A, B, C, alpha=1.0, beta=0.0) -> None:
     m, k = A.shape
     n = B.shape[1]
     L.fmmref_matmul_f32(_pf(A), max(m, 1), _pf(B), max(k, 1), _pf(C), max(m, 1), m, k, n, alpha, beta)
+
+
+def ref_scaling_f32(A: np.ndarray, B: np.ndarray, num_steps: int, kind: int, r=None, s=None):
+    """The reference's Scaling<float> on Fortran-ordered float32 A, B in
+    place; returns (r, s) as float32 (fresh vectors of ones by default)."""
+    L = ref_lib()
+    m, k = A.shape
+    n = B.shape[1]
+    r = np.ones(m, dtype=np.float32) if r is None else np.array(r, dtype=np.float32)
+    s = np.ones(n, dtype=np.float32) if s is None else np.array(s, dtype=np.float32)
+    pf = ctypes.POINTER(ctypes.c_float)
+    L.fmmref_scaling_f32(_pf(A), max(m, 1), _pf(B), max(k, 1), m, k, n, num_steps, kind, r.ctypes.data_as(pf),
+                         s.ctypes.data_as(pf))
+    return r, s
+
+
+def ref_scaling_postprocess_f32(C: np.ndarray, r: np.ndarray, s: np.ndarray) -> None:
+    """The reference's PostProcessScaling on Fortran-ordered float32 C in place."""
+    m, n = C.shape
+    pf = ctypes.POINTER(ctypes.c_float)
+    r = np.ascontiguousarray(r, dtype=np.float32)
+    s = np.ascontiguousarray(s, dtype=np.float32)
+    ref_lib().fmmref_scaling_postprocess_f32(_pf(C), max(m, 1), m, n, r.ctypes.data_as(pf), s.ctypes.data_as(pf))
 
 
 def use_reference_leaf(enabled: bool) -> None:

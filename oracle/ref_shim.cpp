@@ -247,6 +247,23 @@ void fmmref_scaling(double* a, int lda, double* b, int ldb, int m, int k, int n,
   for (int j = 0; j < n; ++j) s[j] = sv[j];
 }
 
+// Scaling<float> / PostProcessScaling on float buffers (the same contract).
+void fmmref_scaling_f32(float* a, int lda, float* b, int ldb, int m, int k, int n, int num_steps, int type, float* r,
+                        float* s) {
+  Matrix<float> A(a, lda, m, k);
+  Matrix<float> B(b, ldb, k, n);
+  std::vector<float> rv(r, r + m), sv(s, s + n);
+  Scaling<float>(A, B, num_steps, rv, sv, type);
+  for (int i = 0; i < m; ++i) r[i] = rv[i];
+  for (int j = 0; j < n; ++j) s[j] = sv[j];
+}
+
+void fmmref_scaling_postprocess_f32(float* c, int ldc, int m, int n, const float* r, const float* s) {
+  Matrix<float> C(c, ldc, m, n);
+  std::vector<float> rv(r, r + m), sv(s, s + n);
+  PostProcessScaling(C, rv, sv);
+}
+
 // PostProcessScaling(C, r_vals, s_vals) from scaling/scaling.hpp.
 void fmmref_scaling_postprocess(double* c, int ldc, int m, int n, const double* r, const double* s) {
   Matrix<double> C(c, ldc, m, n);

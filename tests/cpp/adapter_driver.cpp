@@ -85,6 +85,14 @@ int main() {
     MatMul(A, B, C4, 0.5f);
     expect(MaxRelativeDiff(C3, C4) <= 1e-6, "float grey424 alpha=2 beta=0.5 vs MatMul<float>",
            MaxRelativeDiff(C3, C4));
+    // scaling/fast_scaling.cpp's pattern: Scaling<float> + FastMatmul<float>
+    // + PostProcessScaling back to the unscaled product
+    Matrix<float> As = A, Bs = B, C5(300, 280);
+    std::vector<float> r_vals, s_vals;
+    Scaling<float>(As, Bs, 10, r_vals, s_vals, OUTSIDE);
+    strassen::FastMatmul(As, Bs, C5, 2);
+    PostProcessScaling(C5, r_vals, s_vals);
+    expect(MaxRelativeDiff(C2, C5) <= 1e-5, "float Scaling + strassen + PostProcessScaling", MaxRelativeDiff(C2, C5));
   }
   // diagonal scaling (benchmarks/scaling_stability.cpp pattern): rows of A
   // and columns of B skewed by 2^-30..2^30; scaled Strassen back within the

@@ -224,3 +224,72 @@ def test_scaling_on_the_quadrant_case_costs_nothing():
     fmm.matmul(A, B, C1)
     e, _ = fmm.max_relative_diff(C1, scaled_product(A, B, steps, 50, fmm.INSIDE_OUTSIDE))
     assert e < 1e-13, e
+
+
+# ---------------------------------------------------------------------------
+# Scalar = float: against the reference's own Scaling<float> (oracle/_ref)
+
+
+def skewed32(m, n, seed, per):
+    return np.asfortranarray(skewed(m, n, seed, per).astype(np.float32))
+
+
+def dev32(a):
+    return torch.from_numpy(np.ascontiguousarray(a.T)).cuda().t()
+
+
+SHAPES32 = [(37, 53, 29), (300, 1000, 257), (1, 1, 1), (5, 0, 3), (513, 65, 700)]
+
+
+@pytest.mark.parametrize("kind", [0, 1, 2, 3])
+@pytest.mark.parametrize("shape", SHAPES32, ids=["%dx%dx%d" % s for s in SHAPES32])
+def test_scaling_f32_equals_the_references_bit_for_bit(kind, shape):
+    if not oracle.ref_available():
+        pytest.skip("reference build oracle/_ref not present")
+    m, k, n = shape
+    for steps in (0, 1, 2, 5):
+        A = skewed32(m, k, 3 * steps + kind, "row")
+        B = skewed32(k, n, 3 * steps + kind + 1, "col")
+        Ad, Bd = dev32(A), dev32(B)
+        r, s = fmm.diagonal_scaling(Ad, Bd, steps, kind)
+        fmm.synchronize()
+        Ar, Br = A.copy(order="F"), B.copy(order="F")
+        rr, sr = oracle.ref_scaling_f32(Ar, Br, steps, kind)
+        got = (np.asfortranarray(Ad.cpu().numpy()), np.asfortranarray(Bd.cpu().numpy()), r.cpu().numpy(),
+               s.cpu().numpy())
+        for name, g, w in zip("ABrs", got, (Ar, Br, rr, sr)):
+            assert g.dtype == np.float32 and np.array_equal(g, w, equal_nan=True), (kind, shape, steps, name)
+
+
+def test_postprocess_f32_and_host_entry_points_equal_the_references():
+    if not oracle.ref_available():
+        pytest.skip("reference build oracle/_ref not present")
+    import ctypes
+
+    from fast_matmul_b200._lib import check
+
+    m, k, n = 90, 70, 110
+    A = skewed32(m + 5, k, 11, "row")
+    B = skewed32(k + 3, n, 12, "col")
+    r = np.ones(m, dtype=np.float32)
+    s = np.ones(n, dtype=np.float32)
+    Ar, Br = A[:m].copy(order="F"), B[:k].copy(order="F")
+    rr, sr = oracle.ref_scaling_f32(Ar, Br, 3, 0)
+    P = ctypes.c_void_p
+    h = fmm.default_handle()
+    check(fmm.lib().fmm_diagonal_scaling_f32_host(h.ptr, P(A.ctypes.data), m + 5, P(B.ctypes.data), k + 3, m, k, n,
+                                                  3, 0, P(r.ctypes.data), P(s.ctypes.data)))
+    assert np.array_equal(A[:m], Ar) and np.array_equal(B[:k], Br)
+    assert np.array_equal(r, rr) and np.array_equal(s, sr)
+    C = skewed32(m + 2, n, 13, "row")
+    want = C[:m].copy(order="F")
+    oracle.ref_scaling_postprocess_f32(want, r, s)
+    check(fmm.lib().fmm_scaling_postprocess_f32_host(h.ptr, P(C.ctypes.data), m + 2, m, n, P(r.ctypes.data),
+                                                     P(s.ctypes.data)))
+    assert np.array_equal(C[:m], want)
+    Cd = dev32(C[:m].copy(order="F"))
+    fmm.scaling_postprocess(Cd, torch.from_numpy(r).cuda(), torch.from_numpy(s).cuda())
+    fmm.synchronize()
+    want2 = C[:m].copy(order="F")
+    oracle.ref_scaling_postprocess_f32(want2, r, s)
+    assert np.array_equal(np.asfortranarray(Cd.cpu().numpy()), want2)
