@@ -1128,7 +1128,8 @@ def run_fp32_workload(a):
     clocks = ClockSampler(0)
     clocks.start()
     configs = [("classical (fmm_sgemm)", None, 0, 4), ("strassen", "strassen", 1, 4), ("strassen", "strassen", 2, 4),
-               ("strassen", "strassen", 2, 3), ("grey424_26_206", "grey424_26_206", 2, 4)]
+               ("strassen", "strassen", 2, 3), ("strassen", "strassen", 3, 3), ("grey424_26_206", "grey424_26_206", 2, 4),
+               ("grey424_26_206", "grey424_26_206", 2, 3)]
     for label, alg, steps, sl in configs:
         if alg is None:
             fn = lambda: fmm.matmul(A, B, C, handle=h)  # noqa: E731
