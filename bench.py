@@ -54,14 +54,16 @@ def parse_args(argv=None):
     ap.add_argument("--cpu-sample", type=int, default=4096, help="edge of the CPU baseline sample")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU work budget of the baseline sample")
     ap.add_argument("--workload", default="product",
-                    choices=["product", "batch", "serve", "precision", "scaling", "fp32"],
+                    choices=["product", "batch", "serve", "precision", "scaling", "fp32", "int8"],
                     help="product: one large FastMatmul (the headline); batch: 4096 independent products "
                          "with log-uniform dimensions in [64, 1024] in one CUDA-graph plan; serve: a Poisson "
                          "request stream through the continuous-batching server; precision: split-BF16 leaf "
                          "products (Strassen, Bini) against the FP64 oracle; scaling: diagonal scaling "
                          "(Scaling + FastMatmul + PostProcessScaling) on skewed operands; fp32: "
-                         "FastMatmul<float> against cuBLAS SGEMM")
+                         "FastMatmul<float> against cuBLAS SGEMM; int8: split-INT8 leaf products beside "
+                         "split-BF16 and FP64")
     ap.add_argument("--fp32-size", type=int, default=16384, help="square size of the fp32 workload")
+    ap.add_argument("--int8-size", type=int, default=16384, help="square size of the int8 workload")
     ap.add_argument("--scaling-size", type=int, default=16384, help="square size of the scaling workload")
     ap.add_argument("--precision-sizes", default="8192,16384",
                     help="square sizes of the precision workload")
@@ -1075,6 +1077,109 @@ def run_scaling_workload(a):
     return 0
 
 
+def run_int8_workload(a):
+    """Split-INT8 leaf products (7-bit digits on the INT8 tensor cores, exact
+    int32 sums) beside split-BF16 and FP64 at n^3 on seeded uniform [0, 1)
+    inputs: Strassen with 2 and 3 steps, fast424 with 2 steps and the
+    classical split product, each timed (CUDA events, inputs resident, L2
+    flushed by the inputs' size) and checked against the engine's FP64
+    classical product; the engine's DGEMM and cuBLAS DGEMM give the ratios.
+    The headline is the fastest configuration within 1e-12 (elementwise)."""
+    import torch
+
+    import fast_matmul_b200 as fmm
+
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    h = fmm.default_handle(0)
+    n = a.int8_size
+    flops = 2.0 * n ** 3
+    A = fmm.random_matrix(n, n, 31, 1, handle=h)
+    B = fmm.random_matrix(n, n, 31, 2, handle=h)
+
+    def timed(fn, reps):
+        for _ in range(max(a.warmup, 3)):
+            fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    ref = fmm.colmajor_empty(n, n, dev)
+    ms = timed(lambda: fmm.matmul(A, B, ref, handle=h), 2)
+    engine = flops / (ms * 1e-3) / 1e12
+    Ct = torch.matmul(A, B)
+    msb = timed(lambda: torch.matmul(A, B, out=Ct), 2)
+    cublas = flops / (msb * 1e-3) / 1e12
+    del Ct
+    absAB = fmm.colmajor_empty(n, n, dev)
+    fmm.matmul(A.abs(), B.abs(), absAB, handle=h)
+    C = fmm.colmajor_empty(n, n, dev)
+    clocks = ClockSampler(0)
+    clocks.start()
+    configs = [("strassen", 2, "split_bf16", 5), ("strassen", 2, "split_int8", 6), ("strassen", 2, "split_int8", 7),
+               ("strassen", 3, "split_int8", 6), ("grey424_26_206", 2, "split_int8", 6),
+               ("classical", 0, "split_int8", 6), ("classical", 0, "split_bf16", 5)]
+    rows = []
+    for alg, steps, prec, sl in configs:
+        if alg == "classical":
+            mm = fmm.matmul_split_int8 if prec == "split_int8" else fmm.matmul_split_bf16
+            fn = lambda: mm(A, B, C, slices=sl, handle=h)  # noqa: E731
+        else:
+            fn = lambda: fmm.fast_matmul(alg, A, B, C, steps, precision=prec, split_slices=sl,  # noqa: E731
+                                         handle=h)
+        ms = timed(fn, a.steps)
+        h.profile(True)
+        h.profile_reset()
+        fn()
+        prof = h.profile_read()
+        h.profile(False)
+        fmm.synchronize(h)
+        err = precision_errors(fmm, A, B, C, ref, absAB, h)
+        leaf_ms = prof["gemm_ms"] - prof["split_ms"]
+        rows.append({"algorithm": alg, "num_steps": steps, "precision": "%s x%d" % (prec, sl), "ms": ms,
+                     "effective_tflops": flops / (ms * 1e-3) / 1e12, "error": err,
+                     "split_kernel_ms": prof["split_ms"], "product_kernel_ms": leaf_ms,
+                     "slice_product_tensor_tops": (prof["split_bf16_flops"] / (leaf_ms * 1e-3) / 1e12
+                                                   if leaf_ms > 0 else None)})
+        print(json.dumps({"int8_row": rows[-1]}), file=sys.stderr, flush=True)
+    clk = clocks.stop()
+    ok = [r for r in rows if r["error"]["max_rel_elementwise"] <= 1e-12]
+    head = max(ok, key=lambda r: r["effective_tflops"]) if ok else None
+    peaks, peak_src = measured_peaks()
+    roofline = None
+    if head and head["slice_product_tensor_tops"] and "int8" in head["precision"]:
+        # no INT8 figure is measured: the INT8 tensor rate is twice the BF16 one on
+        # B200 (4.5 against 2.25 dense POPS nominal), so twice the sustained cuBLAS
+        # BF16 figure stands in as the denominator
+        pk = 2.0 * peaks.get("bf16_tflops_sustained", 1400.0)
+        ach = head["slice_product_tensor_tops"]
+        roofline = {"kernel": "split_gemm_kernel<2, true> (tcgen05 kind::i8 slice products)", "bound": "tensor",
+                    "achieved": ach, "peak": pk, "unit": "TOP/s", "frac": ach / pk,
+                    "peak_source": "2 x bf16_tflops_sustained of MEASURED_PEAKS.json (%s): INT8 dense is twice "
+                                   "BF16 dense on B200" % peak_src, "traffic": None}
+    out = {
+        "metric": "effective TFLOP/s (2MNK/t) fast vs classical GEMM, same B200, at stated error",
+        "value": head["effective_tflops"] if head else None, "unit": "TFLOP/s", "n_gpus": 1, "steps": a.steps,
+        "warmup": max(a.warmup, 3), "ms_per_step": head["ms"] if head else None, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int8 slices (FP64 in and out)", "data": "synthetic",
+        "config": {"workload": "int8: split-INT8 leaf products at %d^3, uniform [0, 1); headline = fastest "
+                               "configuration within 1e-12 (elementwise) of the FP64 classical product" % n,
+                   "headline": head, "l2": "inputs larger than L2"},
+        "classical": {"engine_dgemm_tflops": engine, "cublas_dgemm_tflops": cublas},
+        "speedup_vs_engine_classical": head["effective_tflops"] / engine if head else None,
+        "speedup_vs_cublas": head["effective_tflops"] / cublas if head else None,
+        "roofline": roofline, "clocks": clk, "rows": rows,
+    }
+    print(json.dumps(out))
+    return 0
+
+
 def run_fp32_workload(a):
     """FastMatmul<float> (fmm_fast_matmul_f32): FP32 operands widened to FP64
     on the device, split-BF16 leaf products (4 slices by default), rounded to
@@ -1198,6 +1303,8 @@ def main(argv=None):
         return run_precision_workload(a)
     if a.workload == "scaling":
         return run_scaling_workload(a)
+    if a.workload == "int8":
+        return run_int8_workload(a)
     if a.workload == "fp32":
         return run_fp32_workload(a)
     return run_ours(a)

@@ -31,6 +31,7 @@ from .api import (  # noqa: F401
     fast_matmul_host,
     matmul,
     matmul_split_bf16,
+    matmul_split_int8,
     max_relative_diff,
     num_algorithms,
     random_matrix,

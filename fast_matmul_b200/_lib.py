@@ -32,7 +32,7 @@ STATUS_NAMES = {
 }
 
 SCHEDULES = {"auto": 0, "dfs": 1, "bfs": 2, "hybrid": 3}
-PRECISIONS = {"fp64": 0, "split_bf16": 1}
+PRECISIONS = {"fp64": 0, "split_bf16": 1, "split_int8": 2}
 
 
 class FmmError(RuntimeError):
@@ -143,6 +143,10 @@ SIGNATURES = {
                                        ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
                                        ctypes.c_int64, ctypes.c_int64, ctypes.c_double, ctypes.c_double]),
     "fmm_dgemm_split_bf16": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+                                             ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
+                                             ctypes.c_int64, ctypes.c_int64, ctypes.c_double, ctypes.c_double,
+                                             ctypes.c_int]),
+    "fmm_dgemm_split_int8": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
                                              ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
                                              ctypes.c_int64, ctypes.c_int64, ctypes.c_double, ctypes.c_double,
                                              ctypes.c_int]),

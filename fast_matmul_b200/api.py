@@ -184,7 +184,8 @@ def fast_matmul(alg, A, B, C, num_steps: int, x: float = 1e-8, alpha: float = 1.
     """C := alpha * A * B + beta * C with `num_steps` levels of algorithm
     `alg` -- <alg>::FastMatmul(A, B, C, num_steps, x, alpha, beta).
     precision "split_bf16" runs the leaf products on the BF16 tensor cores
-    over `split_slices` slices (0 = 5).  Queued on torch's current stream.
+    over `split_slices` slices (0 = 5), "split_int8" on the INT8 tensor cores
+    over 7-bit slices (0 = 6).  Queued on torch's current stream.
 
     float32 operands (all three) select FastMatmul<float>
     (fmm_fast_matmul_f32): computed on FP64 copies and rounded to FP32 once;
@@ -291,6 +292,19 @@ def matmul_split_bf16(A, B, C, alpha: float = 1.0, beta: float = 0.0, slices: in
     pc, ldc = _mat(C, m, n, "C")
     h = handle or default_handle(C.device.index)
     check(lib().fmm_dgemm_split_bf16(h.ptr, pa, lda, pb, ldb, pc, ldc, m, k, n, alpha, beta, slices))
+
+
+def matmul_split_int8(A, B, C, alpha: float = 1.0, beta: float = 0.0, slices: int = 0,
+                      handle: Optional[Handle] = None) -> None:
+    """Classical C := alpha * A * B + beta * C with split-INT8 tensor-core
+    products (fmm_dgemm_split_int8; `slices` 0 = 6)."""
+    m, k = A.shape
+    n = B.shape[1]
+    pa, lda = _mat(A, m, k, "A")
+    pb, ldb = _mat(B, k, n, "B")
+    pc, ldc = _mat(C, m, n, "C")
+    h = handle or default_handle(C.device.index)
+    check(lib().fmm_dgemm_split_int8(h.ptr, pa, lda, pb, ldb, pc, ldc, m, k, n, alpha, beta, slices))
 
 
 def synchronize(handle: Optional[Handle] = None) -> None:

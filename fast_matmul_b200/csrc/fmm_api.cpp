@@ -121,6 +121,13 @@ void resolve_options(const fmm_options* opts, fmm_options* out) {
 fmm_status split_slices_for(int precision, int requested, int* slices) {
   *slices = 0;
   if (precision == FMM_PRECISION_FP64) return FMM_OK;
+  if (precision == FMM_PRECISION_SPLIT_INT8) {
+    const int s = requested == 0 ? FMM_SPLIT_INT8_DEFAULT_SLICES : requested;
+    if (s < FMM_SPLIT_MIN_SLICES || s > FMM_SPLIT_INT8_MAX_SLICES)
+      return fail(FMM_ERR_INVALID_ARGUMENT, "split_slices must be in [2, 8] for SPLIT_INT8");
+    *slices = fmm::kSplitInt8Code + s;
+    return FMM_OK;
+  }
   if (precision != FMM_PRECISION_SPLIT_BF16) return fail(FMM_ERR_INVALID_ARGUMENT, "unknown precision");
   const int s = requested == 0 ? FMM_SPLIT_DEFAULT_SLICES : requested;
   if (s < FMM_SPLIT_MIN_SLICES || s > FMM_SPLIT_MAX_SLICES)
@@ -488,14 +495,15 @@ fmm_status fmm_dgemm_host(fmm_handle h, const double* A, int64_t lda, const doub
   return FMM_OK;
 }
 
-fmm_status fmm_dgemm_split_bf16(fmm_handle h, const double* A, int64_t lda, const double* B, int64_t ldb,
-                                double* C, int64_t ldc, int64_t m, int64_t k, int64_t n, double alpha, double beta,
-                                int slices) {
+// One classical split product (BF16 or INT8 digits, by `precision`).
+static fmm_status dgemm_split(fmm_handle h, int precision, const double* A, int64_t lda, const double* B, int64_t ldb,
+                       double* C, int64_t ldc, int64_t m, int64_t k, int64_t n, double alpha, double beta,
+                       int slices) {
   if (!h) return fail(FMM_ERR_INVALID_ARGUMENT, "null handle");
   fmm_status s = check_dims(m, k, n, lda, ldb, ldc);
   if (s != FMM_OK) return s;
   int sl = 0;
-  if ((s = split_slices_for(FMM_PRECISION_SPLIT_BF16, slices, &sl)) != FMM_OK) return s;
+  if ((s = split_slices_for(precision, slices, &sl)) != FMM_OK) return s;
   if (m == 0 || n == 0) return FMM_OK;
   if (!C || (k > 0 && (!A || !B))) return fail(FMM_ERR_INVALID_ARGUMENT, "null matrix pointer");
   DeviceGuard g(h->device);
@@ -532,6 +540,18 @@ fmm_status fmm_dgemm_split_bf16(fmm_handle h, const double* A, int64_t lda, cons
   prog.ops.push_back(op);
   if ((s = stage_descriptors(h, prog)) != FMM_OK) return s;
   return run_staged(h, prog);
+}
+
+fmm_status fmm_dgemm_split_bf16(fmm_handle h, const double* A, int64_t lda, const double* B, int64_t ldb,
+                                double* C, int64_t ldc, int64_t m, int64_t k, int64_t n, double alpha, double beta,
+                                int slices) {
+  return dgemm_split(h, FMM_PRECISION_SPLIT_BF16, A, lda, B, ldb, C, ldc, m, k, n, alpha, beta, slices);
+}
+
+fmm_status fmm_dgemm_split_int8(fmm_handle h, const double* A, int64_t lda, const double* B, int64_t ldb,
+                                double* C, int64_t ldc, int64_t m, int64_t k, int64_t n, double alpha, double beta,
+                                int slices) {
+  return dgemm_split(h, FMM_PRECISION_SPLIT_INT8, A, lda, B, ldb, C, ldc, m, k, n, alpha, beta, slices);
 }
 
 fmm_status fmm_fill_uniform(fmm_handle h, double* out, int64_t rows, int64_t cols, int64_t ld, uint64_t seed,

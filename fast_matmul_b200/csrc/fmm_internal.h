@@ -46,6 +46,24 @@ constexpr int kSplitPairRows = 2 * kSplitTile;  // rows of the tile of a CTA pai
 constexpr int kSplitKBlock = 64;  // k-depth of one TMA box (128 bytes of BF16)
 constexpr int kSplitChunk = 128;  // k-depth accumulated exactly in FP32 (two k-blocks)
 
+// Split-INT8 leaf products: the same scaling, signed 8-bit digits of 7 bits
+// (|d| <= 64), products on the INT8 tensor cores with exact int32 sums.  A
+// 128-byte row then holds 128 k values and a chunk (two rows, one pipeline
+// stage) 256; a diagonal is accumulated over up to kSplitI8GroupChunks
+// chunks: at most 8 slices give at most 8 * 64 * 64 = 2^15 per k, so a sum
+// over 32768 k stays below 2^30.
+constexpr int kSplitI8MaxSlices = 8;
+constexpr int kSplitI8DefaultSlices = 6;
+constexpr int kSplitI8KBlock = 128;
+constexpr int kSplitI8Chunk = 256;
+constexpr int kSplitI8GroupChunks = 128;
+
+// A split form travels through the planner as one int, the split code:
+// 0 = FP64 leaves, s = s BF16 slices, kSplitInt8Code + s = s INT8 slices.
+constexpr int kSplitInt8Code = 16;
+__host__ __device__ inline int split_code_slices(int code) { return code >= kSplitInt8Code ? code - kSplitInt8Code : code; }
+__host__ __device__ inline bool split_code_int8(int code) { return code >= kSplitInt8Code; }
+
 // Accumulation groups of one output tile, in order: for each pair of
 // 128-deep k-chunks, diagonal 0 over both chunks, diagonal 1 over both, then
 // diagonals 2..S-1 of the first chunk and of the second (a last single chunk
@@ -88,10 +106,10 @@ struct SplitDesc {
   int64_t lda, ldb, ldc;
   double alpha, beta;
   int m, n, k;
-  int kblocks;          // padded k / kSplitKBlock
+  int kblocks;          // 128-byte rows of k per padded row / column (padded k / 64 BF16 or / 128 INT8)
   int tiles_m, tiles_n; // padded m / kSplitTile (even: m is padded to kSplitPairRows), padded n / kSplitTile
   int64_t tile_begin;   // first output tile (kSplitPairRows x kSplitTile, one CTA pair) of this problem
-  int64_t sa_begin;     // first A-splitting work tile (32 rows x one k-block)
+  int64_t sa_begin;     // first A-splitting work tile (32 rows x 64 k)
   int64_t a_row;        // first 128-byte row of this problem's A slices
   int64_t b_row;        // first 128-byte row of this problem's B slices
   int64_t e_off;        // first row exponent (tiles_m * 128 entries)
@@ -100,7 +118,8 @@ struct SplitDesc {
 
 // Scratch layout of one split launch (offsets from the scratch base).
 struct SplitPlan {
-  int slices = 0;
+  int slices = 0;        // slice count
+  bool int8 = false;     // INT8 digits (else BF16)
   int64_t tiles = 0;     // output tiles (one per CTA pair) over all problems
   int64_t sa_work = 0;   // A-splitting work tiles
   int64_t rows_a = 0, rows_b = 0;  // 128-byte slice rows
@@ -108,16 +127,18 @@ struct SplitPlan {
   size_t off_b = 0, off_e = 0, off_f = 0, bytes = 0;
 };
 
-// Fills the derived fields of descs[0..n) for `slices` slices and returns the
-// scratch layout.  Problems with m == 0 or n == 0 get no tiles.
-SplitPlan split_prepare(SplitDesc* descs, int n, int slices);
+// Fills the derived fields of descs[0..n) for split code `code` and returns
+// the scratch layout.  Problems with m == 0 or n == 0 get no tiles.
+SplitPlan split_prepare(SplitDesc* descs, int n, int code);
 // Adds `count` problems of m x k x n to the sizes of *plan (before
 // split_finish), the same arithmetic split_prepare applies per descriptor.
 void split_accumulate(SplitPlan* plan, int64_t m, int64_t k, int64_t n, int64_t count);
 // Computes the region offsets and total bytes of *plan from its sizes.
 void split_finish(SplitPlan* plan);
 // Scratch bytes split_prepare would report for `count` problems of m x k x n.
-size_t split_scratch_bytes(int64_t m, int64_t k, int64_t n, int64_t count, int slices);
+size_t split_scratch_bytes(int64_t m, int64_t k, int64_t n, int64_t count, int code);
+// The plan of split code `code` with no problems yet.
+SplitPlan split_plan_for(int code);
 // Launches splitting and the tensor-core product.  `scratch` holds plan.bytes
 // bytes (256-byte aligned); *d_err (device) receives a nonzero code if a
 // bounded wait inside the product kernel gave up.  Returns the kernel count

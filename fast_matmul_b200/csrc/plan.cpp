@@ -296,7 +296,8 @@ void emit_gemm(Program* prog, int level, std::vector<GemmDesc>& g, bool leaves) 
   prog->ops.push_back(op);
 }
 
-// Leaf products of one launch as split-BF16 products with `slices` slices.
+// Leaf products of one launch as split products of split code `slices`
+// (BF16 or INT8 digits, fmm_internal.h).
 // All split launches of a program run in order on one stream, so they share
 // one scratch region sized for the largest (Program::split_bytes).
 void emit_split_gemm(Program* prog, int level, const std::vector<GemmDesc>& g, int slices) {
@@ -517,8 +518,9 @@ void BatchFootprint::add(const BatchItem& it) {
     fp64_ += (size_t)round_up((int64_t)end, 256);  // items are laid out back to back, 256-byte aligned
   }
   if (it.split_slices <= 0) return;
-  SplitPlan& p = split_[it.split_slices];
-  p.slices = it.split_slices;
+  auto f = split_.find(it.split_slices);
+  if (f == split_.end()) f = split_.emplace(it.split_slices, split_plan_for(it.split_slices)).first;
+  SplitPlan& p = f->second;
   if (it.classical) {
     split_accumulate(&p, it.m, it.k, it.n, 1);
     return;

@@ -63,7 +63,7 @@ struct Program {
   double leaf_flops = 0.0;  // 2 * m * n * k summed over leaf products
   double peel_flops = 0.0;
   int64_t leaf_count = 0;
-  int split_slices = 0;         // > 0: leaf products run split-BF16 with this many slices
+  int split_slices = 0;         // > 0: split code of the leaf products (slices, BF16 or INT8 digits)
   char* split_scratch = nullptr;  // scratch shared by the split launches (inside the workspace)
   size_t split_bytes = 0;       // its size
   void clear();
@@ -78,13 +78,13 @@ struct LevelDims {
 std::vector<LevelDims> level_dims(const fmm_alg_table& t, int64_t m, int64_t k, int64_t n, int steps);
 
 // Workspace bytes for `dfs_levels` depth-first levels (0 = all breadth-first);
-// split_slices > 0 adds the scratch of split-BF16 leaf products.
+// split_slices > 0 (a split code) adds the scratch of split leaf products.
 size_t workspace_bytes(const fmm_alg_table& t, int64_t m, int64_t k, int64_t n, int steps, int dfs_levels,
                        int split_slices = 0);
 
 // Builds the launch program of one call.  ws must hold workspace_bytes(...) bytes.
-// split_slices > 0 runs the leaf products (not the fringe products of
-// dynamic peeling) split-BF16 with that many slices.
+// split_slices > 0 (a split code: slice count, BF16 or INT8 digits) runs
+// the leaf products (not the fringe products of dynamic peeling) split.
 void build_program(int alg, int64_t m, int64_t k, int64_t n, int steps, double x, double alpha, double beta,
                    int dfs_levels, Operand A, Operand B, Operand C, void* ws, Program* out, int split_slices = 0);
 
@@ -98,7 +98,7 @@ struct BatchItem {
   Operand A, B, C;
   double x, alpha, beta;
   bool classical;
-  int split_slices = 0;  // > 0: this item's leaf products run split-BF16
+  int split_slices = 0;  // > 0: split code of this item's leaf products
 };
 
 // Workspace of a batch (every item planned breadth-first, regions back to back).
@@ -114,7 +114,7 @@ class BatchFootprint {
 
  private:
   size_t fp64_ = 0;                 // FP64 temporaries of the items, 256-byte aligned each
-  std::map<int, SplitPlan> split_;  // split-BF16 leaves per slice count (one launch each)
+  std::map<int, SplitPlan> split_;  // split leaves per split code (one launch each)
 };
 
 // Builds one program for the whole batch: operand formations level by level
@@ -127,7 +127,7 @@ void build_batch_program(const BatchItem* items, int count, void* ws, Program* o
 // d_desc (which must hold prog.desc.size() bytes), then the launches in order.
 // Adds the number of kernels launched to *launches (may be null).
 // When prof is non-null every launch is bracketed by CUDA events.  d_err
-// (device int) collects the error codes of split-BF16 launches.
+// (device int) collects the error codes of split launches.
 cudaError_t run_program(const Program& prog, const void* h_desc, void* d_desc, int num_sms, cudaStream_t stream,
                         int64_t* launches, Profiler* prof = nullptr, int* d_err = nullptr);
 

@@ -1,8 +1,8 @@
 // sm_100a building blocks written directly in PTX for CTA pairs (clusters of
 // two, the two-SM MMA): mbarriers with bounded waits, cluster barriers and
 // remote arrives, TMA tile loads (cp.async.bulk.tensor.cta_group::2),
-// tensor-memory allocation, tcgen05 MMA issue / commit and tensor-memory
-// loads.
+// tensor-memory allocation, tcgen05 MMA issue (BF16 and INT8) / commit and
+// tensor-memory loads.
 //
 // Every wait gives up after kWaitLimitNs of wall-clock time (the device's
 // global timer): it records a code in the caller's error word and returns
@@ -193,6 +193,13 @@ __host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
+// Instruction descriptor of tcgen05.mma kind::i8: S32 accumulator [4,6) = 2,
+// A = signed 8-bit [7,10) = 1, B = signed 8-bit [10,13) = 1, both K-major,
+// N >> 3 at [17,23), M >> 4 at [24,29).
+__host__ __device__ constexpr uint32_t idesc_s8_s32(int M, int N) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
 // D[tmem] (+)= A[smem] * B[smem]^T in the two-SM form, issued by one thread
 // of the pair leader: A rows 0-127 from the leader's shared memory and
 // 128-255 from the peer's at the same offset, B columns split in halves the
@@ -202,6 +209,17 @@ __device__ __forceinline__ void mma_bf16_pair(uint32_t d_tmem, uint64_t a_desc, 
   asm volatile(
       "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
       " tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d_tmem),
+      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"((uint32_t)accumulate)
+      : "memory");
+}
+
+// The same with signed 8-bit operands and an int32 accumulator (kind::i8):
+// one instruction covers 32 bytes of k per row, K = 32.
+__device__ __forceinline__ void mma_s8_pair(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                            bool accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, p;\n}\n" ::"r"(d_tmem),
       "l"(a_desc), "l"(b_desc), "r"(idesc), "r"((uint32_t)accumulate)
       : "memory");
 }

@@ -20,6 +20,18 @@
 // Error: |x - sum_t d_t 2^-8t| <= 2^-(8S+1) 2^e per operand entry plus the
 // dropped diagonals, so |C - AB| <~ 3 * 2^-8S * k * max|a_i.| * max|b_.j|.
 //
+// Split-INT8 (the same kernels, instantiated for 8-bit digits): the scaled x
+// is split into signed bytes d_0 = rint(64 x), d_t = rint(128 r_{t-1}), so
+// x = sum_t d_t 2^-(6+7t) + r 2^-(7S-1) with |d_t| <= 64 and |r| <= 1/2; the
+// slice products run as tcgen05.mma kind::i8 (M256 N128 K32, twice the BF16
+// rate) and accumulate in int32, exactly, over up to kSplitI8GroupChunks
+// 256-deep chunks per diagonal, so a tile drains each diagonal once instead
+// of once per chunk.  Each diagonal sum is scaled by 2^-(12+7D) and added
+// into the FP64 accumulator in diagonal order.  A 128-byte slice row holds
+// 128 k values, so the tensor maps, TMA boxes, shared-memory descriptors and
+// MMA count per stage are those of the BF16 form byte for byte.
+// Error: |C - AB| <~ (S + 2) * 2^-7S * k * max|a_i.| * max|b_.j|.
+//
 // Product kernel: persistent CTA pairs (clusters of 2) over the 256 x 128
 // output tiles of every problem, with the two-SM MMA: one thread of the
 // pair leader issues tcgen05.mma.cta_group::2 (M256 N128 K16), which reads
@@ -173,13 +185,33 @@ __device__ __forceinline__ void store_digits(double (&x)[8], int slices, __nv_bf
   }
 }
 
-// A slices: one work tile = 32 rows x one 64-deep k-block, read column-major
+// INT8 digits of 8 scaled values, one 8-byte store per slice: d_0 = rint(64 x),
+// then d_t = rint(128 r), by the same FP64-pipe rounding; |d_t| <= 64, and
+// the low byte of the sum's low word is the digit's two's complement.
+__device__ __forceinline__ void store_digits_i8(double (&x)[8], int slices, uint8_t* dst, int64_t slice_stride) {
+  const double kRound = 6755399441055744.0;  // 1.5 * 2^52
+  double radix = 64.0;
+  for (int t = 0; t < slices; ++t) {
+    uint32_t w[2] = {0u, 0u};
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const double y = fma(x[c], radix, kRound);
+      x[c] = fma(x[c], radix, -(y - kRound));
+      w[c >> 2] |= ((uint32_t)__double2loint(y) & 0xFFu) << (8 * (c & 3));
+    }
+    *reinterpret_cast<uint2*>(dst + t * slice_stride) = make_uint2(w[0], w[1]);
+    radix = 128.0;
+  }
+}
+
+// A slices: one work tile = 32 rows x 64 k (one BF16 k-block, half an INT8 one), read column-major
 // (coalesced along rows) into shared memory, written as 128-byte k-block rows
 // for every slice (8 threads per row, 16 bytes each).  The tile's row index
 // is XOR-swizzled by k so that both the column-wise fill and the row-wise
 // read-out touch every bank pair at most twice per warp.
+template <bool kInt8>
 __global__ void __launch_bounds__(256) split_a(const SplitDesc* __restrict__ d, int nd, int64_t total, int slices,
-                                               const int* __restrict__ ea, __nv_bfloat16* __restrict__ out) {
+                                               const int* __restrict__ ea, uint8_t* __restrict__ out) {
   __shared__ double tile[64 * 32];
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
   const int row = threadIdx.x >> 3, kc = (threadIdx.x & 7) * 8;
@@ -216,16 +248,24 @@ __global__ void __launch_bounds__(256) split_a(const SplitDesc* __restrict__ d, 
     double x[8];
 #pragma unroll
     for (int c = 0; c < 8; ++c) x[c] = scale_pow2(tile[at(kc + c, row)], e);
-    const int64_t orow = s.a_row + kb * mp + i0 + row;
-    store_digits(x, slices, out + orow * kBK + kc, (int64_t)s.kblocks * mp * kBK);
+    const int64_t slice_bytes = (int64_t)s.kblocks * mp * 128;
+    if constexpr (kInt8) {
+      const int64_t orow = s.a_row + (kb >> 1) * mp + i0 + row;
+      store_digits_i8(x, slices, out + orow * 128 + (kb & 1) * 64 + kc, slice_bytes);
+    } else {
+      const int64_t orow = s.a_row + kb * mp + i0 + row;
+      store_digits(x, slices, reinterpret_cast<__nv_bfloat16*>(out + orow * 128) + kc, slice_bytes / 2);
+    }
   }
 }
 
 // B: one block per padded column: the column maximum, then the slices, 8
 // consecutive k per thread (B's columns are contiguous in k, so they are
 // written as they are read).
+template <bool kInt8>
 __global__ void __launch_bounds__(256) split_b(const SplitDesc* __restrict__ d, int nd, int64_t total, int slices,
-                                               int* __restrict__ fb, __nv_bfloat16* __restrict__ out) {
+                                               int* __restrict__ fb, uint8_t* __restrict__ out) {
+  constexpr int kRowValues = kInt8 ? kSplitI8KBlock : kBK;  // k values per 128-byte slice row
   __shared__ double red[8];
   __shared__ int e_sh;
   for (int64_t x = blockIdx.x; x < total; x += gridDim.x) {
@@ -236,7 +276,7 @@ __global__ void __launch_bounds__(256) split_b(const SplitDesc* __restrict__ d, 
     const double* b = s.B + j * s.ldb;
     const bool live = j < s.n;
     const bool vec = (reinterpret_cast<uintptr_t>(b) & 15) == 0;
-    const int k = s.k, kp = s.kblocks * kBK;
+    const int k = s.k, kp = s.kblocks * kRowValues;
     auto load8 = [&](int p0, double (&v)[8]) {
       if (vec && p0 + 8 <= k) {
 #pragma unroll
@@ -279,8 +319,13 @@ __global__ void __launch_bounds__(256) split_b(const SplitDesc* __restrict__ d, 
       }
 #pragma unroll
       for (int c = 0; c < 8; ++c) v[c] = scale_pow2(v[c], f);
-      const int64_t orow = s.b_row + (int64_t)(p0 / kBK) * np + j;
-      store_digits(v, slices, out + orow * kBK + (p0 % kBK), (int64_t)s.kblocks * np * kBK);
+      const int64_t orow = s.b_row + (int64_t)(p0 / kRowValues) * np + j;
+      const int64_t slice_bytes = (int64_t)s.kblocks * np * 128;
+      if constexpr (kInt8)
+        store_digits_i8(v, slices, out + orow * 128 + (p0 % kRowValues), slice_bytes);
+      else
+        store_digits(v, slices, reinterpret_cast<__nv_bfloat16*>(out + orow * 128) + (p0 % kRowValues),
+                     slice_bytes / 2);
     }
     __syncthreads();  // e_sh and red are reused by the next column
   }
@@ -330,10 +375,17 @@ __device__ __forceinline__ TileCoord tile_coord(const GemmParams& g, int64_t til
 
 // Calls fn(D, c0, c1) for the accumulation groups of a tile in order
 // (split_group), until fn returns false; returns whether all ran.  With one
-// chunk per group the loops are the plain chunk-then-diagonal order.
-template <int kSpan, class Fn>
+// chunk per group the loops are the plain chunk-then-diagonal order.  INT8
+// digits: each diagonal over up to kSplitI8GroupChunks chunks (exact int32).
+template <int kSpan, bool kInt8, class Fn>
 __device__ __forceinline__ bool for_each_group(int chunks, int S, Fn&& fn) {
-  if constexpr (kSpan == 1) {
+  if constexpr (kInt8) {
+    for (int c0 = 0; c0 < chunks; c0 += kSplitI8GroupChunks) {
+      const int c1 = min(c0 + kSplitI8GroupChunks, chunks);
+      for (int D = 0; D < S; ++D)
+        if (!fn(D, c0, c1)) return false;
+    }
+  } else if constexpr (kSpan == 1) {
     for (int c = 0; c < chunks; ++c)
       for (int D = 0; D < S; ++D)
         if (!fn(D, c, c + 1)) return false;
@@ -349,7 +401,23 @@ __device__ __forceinline__ bool for_each_group(int chunks, int S, Fn&& fn) {
   return true;
 }
 
-template <int kEpiGroups>
+// A drained accumulator value as a double (exact either way) and the weight
+// of diagonal D: FP32 sums of BF16 digits weigh 2^-8(D+2), int32 sums of
+// INT8 digits 2^-(12+7D).
+template <bool kInt8>
+__device__ __forceinline__ double acc_value(uint32_t r) {
+  if constexpr (kInt8)
+    return (double)(int32_t)r;
+  else
+    return (double)__uint_as_float(r);
+}
+
+template <bool kInt8>
+__device__ __forceinline__ double diagonal_weight(int D) {
+  return kInt8 ? ldexp(1.0, -(12 + 7 * D)) : ldexp(1.0, -8 * (D + 2));
+}
+
+template <int kEpiGroups, bool kInt8>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(gemm_threads(kEpiGroups), 1)
     split_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                       const GemmParams g) {
@@ -404,7 +472,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(gemm_threads(kEpiGro
         const int64_t ya_tile = s.a_row + (int64_t)tc.tm * kSplitPairRows + rank * kBM;
         const int64_t yb_tile = s.b_row + (int64_t)tc.tn * kBN + rank * kBHalf;
         const int chunks = s.kblocks / kChunkBlocks;
-        ok = for_each_group<kSpan>(chunks, S, [&](int D, int c0, int c1) {
+        ok = for_each_group<kSpan, kInt8>(chunks, S, [&](int D, int c0, int c1) {
           for (int c = c0; c < c1; ++c)
             for (int t = 0; t <= D; ++t)
               for (int h = 0; h < kChunkBlocks; h += kStageKBlocks) {
@@ -443,13 +511,13 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(gemm_threads(kEpiGro
     }
   } else if (warp == 1) {
     if (lane == 0 && leader) {
-      const uint32_t idesc = idesc_bf16_f32(kSplitPairRows, kBN);
+      const uint32_t idesc = kInt8 ? idesc_s8_s32(kSplitPairRows, kBN) : idesc_bf16_f32(kSplitPairRows, kBN);
       uint32_t st = 0, ph = 0, ai = 0;
       bool ok = true;
       for (int64_t tile = pair; tile < g.tiles && ok; tile += pairs) {
         const TileCoord tc = tile_coord(g, tile);
         const int chunks = g.desc[tc.q].kblocks / kChunkBlocks;
-        ok = for_each_group<kSpan>(chunks, S, [&](int D, int c0, int c1) {
+        ok = for_each_group<kSpan, kInt8>(chunks, S, [&](int D, int c0, int c1) {
           const uint32_t buf = ai % kAccBufs;
           if (ai >= (uint32_t)kAccBufs && !mbar_wait(&acc_empty[buf], ((ai / kAccBufs) - 1) & 1, g.err, 2))
             return false;
@@ -463,11 +531,15 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(gemm_threads(kEpiGro
                 const uint32_t a = smem_addr(base + st * kStageBytes);
                 const uint32_t b = a + kStageKBlocks * kATileBytes;
 #pragma unroll
-                for (int kk = 0; kk < kStageKBlocks * kBK / 16; ++kk) {
+                for (int kk = 0; kk < kStageKBlocks * kBK / 16; ++kk) {  // 32 bytes of each row per MMA
                   const uint32_t koff = (kk & 3) * 32;
-                  mma_bf16_pair(d_tmem, smem_desc_sw128(a + (kk >> 2) * kATileBytes + koff),
-                                smem_desc_sw128(b + (kk >> 2) * kBTileBytes + koff), idesc,
-                                c > c0 || t > 0 || h > 0 || kk > 0);
+                  const uint64_t ad = smem_desc_sw128(a + (kk >> 2) * kATileBytes + koff);
+                  const uint64_t bd = smem_desc_sw128(b + (kk >> 2) * kBTileBytes + koff);
+                  const bool accumulate = c > c0 || t > 0 || h > 0 || kk > 0;
+                  if constexpr (kInt8)
+                    mma_s8_pair(d_tmem, ad, bd, idesc, accumulate);
+                  else
+                    mma_bf16_pair(d_tmem, ad, bd, idesc, accumulate);
                 }
                 mma_commit_pair(&empty[st], kPairMask);
                 if (++st == (uint32_t)kStages) {
@@ -498,11 +570,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(gemm_threads(kEpiGro
       double acc[kEpiCols];
 #pragma unroll
       for (int j = 0; j < kEpiCols; ++j) acc[j] = 0.0;
-      ok = for_each_group<kSpan>(chunks, S, [&](int D, int, int) {
+      ok = for_each_group<kSpan, kInt8>(chunks, S, [&](int D, int, int) {
           const int buf = ai % kAccBufs;
           if (!mbar_wait(&acc_full[buf], (ai / kAccBufs) & 1, g.err, 4)) return false;
           tc_fence_after();
-          const double scale = ldexp(1.0, -8 * (D + 2));
+          const double scale = diagonal_weight<kInt8>(D);
           const uint32_t taddr = tmem + ((uint32_t)(qd * 32) << 16) + buf * kBN + wg * kEpiCols;
           // eight pieces of 8 columns, software-pipelined: the load of piece
           // g + 1 is in flight while piece g is converted and accumulated
@@ -514,7 +586,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(gemm_threads(kEpiGro
             tmem_ld_32x32b_x8(taddr + (g8 + 1) * 8, r1);
 #pragma unroll
             for (int j = 0; j < 8; ++j)
-              acc[g8 * 8 + j] = fma((double)__uint_as_float(r0[j]), scale, acc[g8 * 8 + j]);
+              acc[g8 * 8 + j] = fma(acc_value<kInt8>(r0[j]), scale, acc[g8 * 8 + j]);
             tmem_ld_wait();
             if (g8 + 2 < kEpiCols / 8) tmem_ld_32x32b_x8(taddr + (g8 + 2) * 8, r0);
             if (g8 + 2 == kEpiCols / 8) {  // the accumulator is free once the last piece is in registers
@@ -524,7 +596,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(gemm_threads(kEpiGro
             }
 #pragma unroll
             for (int j = 0; j < 8; ++j)
-              acc[(g8 + 1) * 8 + j] = fma((double)__uint_as_float(r1[j]), scale, acc[(g8 + 1) * 8 + j]);
+              acc[(g8 + 1) * 8 + j] = fma(acc_value<kInt8>(r1[j]), scale, acc[(g8 + 1) * 8 + j]);
             if (g8 + 2 < kEpiCols / 8) tmem_ld_wait();
           }
           ++ai;
@@ -578,16 +650,18 @@ EncodeTiledFn encode_fn() {
   return fn;
 }
 
-// {64 BF16, rows} view of a slice buffer; boxes of `box_rows` 128-byte rows.
-bool encode_slices(CUtensorMap* map, void* base, int64_t rows, int box_rows) {
+// {64 BF16 or 128 INT8, rows} view of a slice buffer; boxes of `box_rows`
+// 128-byte rows.
+bool encode_slices(CUtensorMap* map, void* base, int64_t rows, int box_rows, bool int8) {
   EncodeTiledFn enc = encode_fn();
   if (!enc) return false;
-  const cuuint64_t dims[2] = {(cuuint64_t)kBK, (cuuint64_t)rows};
-  const cuuint64_t strides[1] = {(cuuint64_t)kBK * 2};
-  const cuuint32_t box[2] = {(cuuint32_t)kBK, (cuuint32_t)box_rows};
+  const cuuint64_t row_values = int8 ? 128 : 64;
+  const cuuint64_t dims[2] = {row_values, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {128};
+  const cuuint32_t box[2] = {(cuuint32_t)row_values, (cuuint32_t)box_rows};
   const cuuint32_t es[2] = {1, 1};
-  return enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-             CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+  return enc(map, int8 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box,
+             es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
@@ -614,26 +688,31 @@ cudaError_t wait_probe_launch(int* d_err, uint64_t limit_ns, int code, cudaStrea
 cudaError_t split_gemm_launch(const SplitDesc* d_descs, int n, const SplitPlan& plan, void* scratch, int* d_err,
                               int num_sms, cudaStream_t stream, int64_t* launches, cudaEvent_t split_done) {
   if (plan.tiles == 0) return cudaSuccess;
-  if (plan.slices < kSplitMinSlices || plan.slices > kSplitMaxSlices || !d_err || !scratch ||
-      reinterpret_cast<uintptr_t>(scratch) % 256 != 0)
+  if (plan.slices < kSplitMinSlices || plan.slices > (plan.int8 ? kSplitI8MaxSlices : kSplitMaxSlices) || !d_err ||
+      !scratch || reinterpret_cast<uintptr_t>(scratch) % 256 != 0)
     return cudaErrorInvalidValue;
   // tensor-map row coordinates are 32-bit
   if (plan.rows_a >= (int64_t(1) << 31) || plan.rows_b >= (int64_t(1) << 31)) return cudaErrorInvalidValue;
   char* base = static_cast<char*>(scratch);
-  __nv_bfloat16* as = reinterpret_cast<__nv_bfloat16*>(base);
-  __nv_bfloat16* bs = reinterpret_cast<__nv_bfloat16*>(base + plan.off_b);
+  uint8_t* as = reinterpret_cast<uint8_t*>(base);
+  uint8_t* bs = reinterpret_cast<uint8_t*>(base + plan.off_b);
   int* ea = reinterpret_cast<int*>(base + plan.off_e);
   int* fb = reinterpret_cast<int*>(base + plan.off_f);
   const int64_t cap = (int64_t)num_sms * 16;
   split_row_exponents<<<grid_for(plan.n_e / 32, (int64_t)num_sms * 4), kExpWarps * 32, 0, stream>>>(d_descs, n,
                                                                                              plan.n_e / 32, ea);
-  split_a<<<grid_for(plan.sa_work, cap), 256, 0, stream>>>(d_descs, n, plan.sa_work, plan.slices, ea, as);
-  split_b<<<grid_for(plan.n_f, cap), 256, 0, stream>>>(d_descs, n, plan.n_f, plan.slices, fb, bs);
+  if (plan.int8) {
+    split_a<true><<<grid_for(plan.sa_work, cap), 256, 0, stream>>>(d_descs, n, plan.sa_work, plan.slices, ea, as);
+    split_b<true><<<grid_for(plan.n_f, cap), 256, 0, stream>>>(d_descs, n, plan.n_f, plan.slices, fb, bs);
+  } else {
+    split_a<false><<<grid_for(plan.sa_work, cap), 256, 0, stream>>>(d_descs, n, plan.sa_work, plan.slices, ea, as);
+    split_b<false><<<grid_for(plan.n_f, cap), 256, 0, stream>>>(d_descs, n, plan.n_f, plan.slices, fb, bs);
+  }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   if (split_done && (e = cudaEventRecord(split_done, stream)) != cudaSuccess) return e;
   CUtensorMap tA, tB;
-  if (!encode_slices(&tA, as, plan.rows_a, kBM) || !encode_slices(&tB, bs, plan.rows_b, kBHalf))
+  if (!encode_slices(&tA, as, plan.rows_a, kBM, plan.int8) || !encode_slices(&tB, bs, plan.rows_b, kBHalf, plan.int8))
     return cudaErrorInvalidValue;
   GemmParams gp;
   gp.desc = d_descs;
@@ -650,9 +729,14 @@ cudaError_t split_gemm_launch(const SplitDesc* d_descs, int n, const SplitPlan& 
   {
     std::lock_guard<std::mutex> lock(mu);
     if (dev < 0 || dev >= 64 || !opted_in[dev]) {
-      e = cudaFuncSetAttribute(split_gemm_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem);
+      e = cudaFuncSetAttribute(split_gemm_kernel<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kGemmSmem);
       if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(split_gemm_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem);
+        e = cudaFuncSetAttribute(split_gemm_kernel<4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kGemmSmem);
+      if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(split_gemm_kernel<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kGemmSmem);
       if (e != cudaSuccess) return e;
       if (dev >= 0 && dev < 64) opted_in[dev] = true;
     }
@@ -660,10 +744,12 @@ cudaError_t split_gemm_launch(const SplitDesc* d_descs, int n, const SplitPlan& 
   // CTA pairs: the grid is even and a pair's CTAs are consecutive blocks
   const unsigned pairs = grid_for(plan.tiles, num_sms / 2 > 0 ? num_sms / 2 : 1);
   if (split_chunk_span(plan.slices) != (plan.slices <= 3 ? 2 : 1)) return cudaErrorInvalidValue;
-  if (plan.slices <= 3)
-    split_gemm_kernel<4><<<2 * pairs, gemm_threads(4), kGemmSmem, stream>>>(tA, tB, gp);
+  if (plan.int8)  // one drain per diagonal and tile: two epilogue warpgroups suffice
+    split_gemm_kernel<2, true><<<2 * pairs, gemm_threads(2), kGemmSmem, stream>>>(tA, tB, gp);
+  else if (plan.slices <= 3)
+    split_gemm_kernel<4, false><<<2 * pairs, gemm_threads(4), kGemmSmem, stream>>>(tA, tB, gp);
   else
-    split_gemm_kernel<2><<<2 * pairs, gemm_threads(2), kGemmSmem, stream>>>(tA, tB, gp);
+    split_gemm_kernel<2, false><<<2 * pairs, gemm_threads(2), kGemmSmem, stream>>>(tA, tB, gp);
   e = cudaGetLastError();
   if (e == cudaSuccess && launches) *launches += 4;
   return e;

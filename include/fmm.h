@@ -68,22 +68,33 @@ typedef enum fmm_schedule {
  *               k groups of 128 (256 for the two leading diagonals at 3
  *               slices or fewer), recombined in FP64.  Error of one leaf
  *               product: |C - AB|_ij <~ 3 * 2^-8S * k * max|A_i.| * max|B_.j|;
- *               S = 5 stays near 1e-14 relative for well-scaled operands. */
+ *               S = 5 stays near 1e-14 relative for well-scaled operands.
+ *   SPLIT_INT8  the same scaling, split into `split_slices` signed 8-bit
+ *               digit slices of 7 bits (|digit| <= 64); the S(S+1)/2 leading
+ *               slice products run on the INT8 tensor cores (tcgen05
+ *               kind::i8, twice the BF16 rate) with exact int32
+ *               accumulation over k groups of up to 32768, recombined in
+ *               FP64.  Error of one leaf product:
+ *               |C - AB|_ij <~ (S + 2) * 2^-7S * k * max|A_i.| * max|B_.j|;
+ *               6 slices are about as accurate as 5 BF16 slices. */
 typedef enum fmm_precision {
   FMM_PRECISION_FP64 = 0,
-  FMM_PRECISION_SPLIT_BF16 = 1
+  FMM_PRECISION_SPLIT_BF16 = 1,
+  FMM_PRECISION_SPLIT_INT8 = 2
 } fmm_precision;
 
 #define FMM_SPLIT_MIN_SLICES 2
 #define FMM_SPLIT_MAX_SLICES 6
 #define FMM_SPLIT_DEFAULT_SLICES 5
+#define FMM_SPLIT_INT8_MAX_SLICES 8
+#define FMM_SPLIT_INT8_DEFAULT_SLICES 6
 
 typedef struct fmm_handle_s* fmm_handle;
 
 typedef struct fmm_options {
   fmm_schedule schedule;    /* default FMM_SCHEDULE_AUTO */
   fmm_precision precision;  /* default FMM_PRECISION_FP64 */
-  int split_slices;         /* BF16 slices per operand for SPLIT_BF16, 2..6 (0 = default 5) */
+  int split_slices;         /* slices per operand: SPLIT_BF16 2..6 (0 = default 5), SPLIT_INT8 2..8 (0 = 6) */
   int dfs_levels;           /* HYBRID only: depth-first levels; -1 = choose */
   size_t workspace_limit;   /* bytes; 0 = the handle's limit */
 } fmm_options;
@@ -145,6 +156,12 @@ fmm_status fmm_dgemm(fmm_handle h, const double* A, int64_t lda, const double* B
  * `slices` slices (0 = default) on the BF16 tensor cores (no counterpart in
  * the reference).  Device pointers; queued on the handle's stream. */
 fmm_status fmm_dgemm_split_bf16(fmm_handle h, const double* A, int64_t lda, const double* B, int64_t ldb,
+                                double* C, int64_t ldc, int64_t m, int64_t k, int64_t n, double alpha, double beta,
+                                int slices);
+
+/* The same product computed split-INT8 (FMM_PRECISION_SPLIT_INT8) with
+ * `slices` slices (0 = default 6) on the INT8 tensor cores. */
+fmm_status fmm_dgemm_split_int8(fmm_handle h, const double* A, int64_t lda, const double* B, int64_t ldb,
                                 double* C, int64_t ldc, int64_t m, int64_t k, int64_t n, double alpha, double beta,
                                 int slices);
 
@@ -274,9 +291,10 @@ typedef struct fmm_profile {
   double form_ms, gemm_ms, peel_ms, combine_ms;
   double form_bytes, combine_bytes;
   double gemm_flops, peel_flops;
-  /* split-BF16 leaf products (counted in gemm_* above as well): time of the
-   * scale / split kernels within gemm_ms, and the BF16 tensor-core FLOPs of
-   * the slice products (2 m n k per product, S(S+1)/2 products per leaf) */
+  /* split leaf products (counted in gemm_* above as well): time of the
+   * scale / split kernels within gemm_ms, and the tensor-core operations of
+   * the slice products (2 m n k per product, S(S+1)/2 products per leaf;
+   * BF16 FLOPs for SPLIT_BF16, INT8 operations for SPLIT_INT8) */
   double split_ms;
   double split_bf16_flops;
 } fmm_profile;
@@ -307,7 +325,7 @@ typedef struct fmm_batch_item {
   int64_t m, k, n;
   double x, alpha, beta; /* as in fmm_fast_matmul */
   int precision;         /* fmm_precision of the item's leaf products (0 = FP64) */
-  int split_slices;      /* SPLIT_BF16 slices, 2..6 (0 = default) */
+  int split_slices;      /* slices: SPLIT_BF16 2..6, SPLIT_INT8 2..8 (0 = default) */
 } fmm_batch_item;
 
 /* Independent products in one program: the operand formations of all items
@@ -382,7 +400,7 @@ typedef struct fmm_request {
   int64_t ldc;
   int64_t m, k, n;
   double x, alpha, beta;
-  int split_slices; /* SPLIT_BF16 slices, 2..6 (0 = default) */
+  int split_slices; /* slices: SPLIT_BF16 2..6, SPLIT_INT8 2..8 (0 = default) */
 } fmm_request;
 
 typedef struct fmm_request_info {

@@ -148,11 +148,26 @@ void digits(double x, int slices, double* out) {
   }
 }
 
-// One split-BF16 product C = alpha * A * B + beta * C, in the device's order.
-void split_product(const fmm::SplitDesc& d, int slices) {
+// INT8 digits of x (|x| < 1): d_0 = rint(64 x), d_t = rint(128 r_{t-1}),
+// |d_t| <= 64.
+void digits_i8(double x, int slices, double* out) {
+  double radix = 64.0;
+  for (int t = 0; t < slices; ++t) {
+    const double y = x * radix;
+    const double dg = std::rint(y);
+    x = y - dg;
+    out[t] = dg;
+    radix = 128.0;
+  }
+}
+
+// One split product C = alpha * A * B + beta * C (split code `code`: BF16
+// or INT8 digits), in the device's order.
+void split_product(const fmm::SplitDesc& d, int code) {
   const int m = d.m, n = d.n, k = d.k;
   if (m <= 0 || n <= 0) return;
-  const int S = slices;
+  const int S = fmm::split_code_slices(code);
+  const bool int8 = fmm::split_code_int8(code);
   std::vector<int> ea((size_t)m), fb((size_t)n);
   for (int i = 0; i < m; ++i) {
     double mx = 0.0;
@@ -169,30 +184,49 @@ void split_product(const fmm::SplitDesc& d, int slices) {
   double dg[8];
   for (int p = 0; p < k; ++p) {
     for (int i = 0; i < m; ++i) {
-      digits(std::ldexp(d.A[i + (int64_t)p * d.lda], -ea[(size_t)i]), S, dg);
+      (int8 ? digits_i8 : digits)(std::ldexp(d.A[i + (int64_t)p * d.lda], -ea[(size_t)i]), S, dg);
       for (int t = 0; t < S; ++t) dA[((size_t)t * k + p) * m + i] = dg[t];
     }
     for (int j = 0; j < n; ++j) {
-      digits(std::ldexp(d.B[p + (int64_t)j * d.ldb], -fb[(size_t)j]), S, dg);
+      (int8 ? digits_i8 : digits)(std::ldexp(d.B[p + (int64_t)j * d.ldb], -fb[(size_t)j]), S, dg);
       for (int t = 0; t < S; ++t) dB[((size_t)t * k + p) * n + j] = dg[t];
     }
   }
   std::vector<double> acc((size_t)m * n, 0.0), part((size_t)m * n);
+  // part[j * m + i] += sum over t <= D, p in [p0, p1) of dA_t[i, p] dB_{D-t}[p, j] (exact integers)
+  auto diagonal_sum = [&](int D, int p0, int p1) {
+    std::fill(part.begin(), part.end(), 0.0);
+    for (int t = 0; t <= D; ++t)
+      for (int p = p0; p < p1; ++p) {
+        const double* a = &dA[((size_t)t * k + p) * m];
+        const double* b = &dB[((size_t)(D - t) * k + p) * n];
+        for (int j = 0; j < n; ++j)
+          for (int i = 0; i < m; ++i) part[(size_t)j * m + i] += a[i] * b[j];
+      }
+  };
+  if (int8) {
+    // each diagonal over groups of up to kSplitI8GroupChunks 256-deep chunks,
+    // summed in int32 (exact: |sum| < 2^30), weighted 2^-(12 + 7D)
+    const int chunks = std::max(1, (k + fmm::kSplitI8Chunk - 1) / fmm::kSplitI8Chunk);
+    for (int c0 = 0; c0 < chunks; c0 += fmm::kSplitI8GroupChunks) {
+      const int c1 = std::min(chunks, c0 + fmm::kSplitI8GroupChunks);
+      for (int D = 0; D < S; ++D) {
+        diagonal_sum(D, c0 * fmm::kSplitI8Chunk, std::min(k, c1 * fmm::kSplitI8Chunk));
+        const double scale = std::ldexp(1.0, -(12 + 7 * D));
+        for (size_t x = 0; x < part.size(); ++x) {
+          const int32_t v = (int32_t)part[x];  // the int32 accumulator (exact)
+          acc[x] = std::fma((double)v, scale, acc[x]);
+        }
+      }
+    }
+  }
   const int chunks = std::max(1, (k + fmm::kSplitChunk - 1) / fmm::kSplitChunk);
-  for (int cp = 0; cp < chunks; cp += fmm::split_chunk_span(S)) {
+  for (int cp = 0; !int8 && cp < chunks; cp += fmm::split_chunk_span(S)) {
     const int nch = std::min(fmm::split_chunk_span(S), chunks - cp);
     for (int gi = 0; gi < fmm::split_groups_in_pair(nch, S); ++gi) {
       const fmm::SplitGroup G = fmm::split_group(cp, nch, S, gi);
       const int D = G.D;
-      const int p0 = G.c0 * fmm::kSplitChunk, p1 = std::min(k, G.c1 * fmm::kSplitChunk);
-      std::fill(part.begin(), part.end(), 0.0);
-      for (int t = 0; t <= D; ++t)
-        for (int p = p0; p < p1; ++p) {
-          const double* a = &dA[((size_t)t * k + p) * m];
-          const double* b = &dB[((size_t)(D - t) * k + p) * n];
-          for (int j = 0; j < n; ++j)
-            for (int i = 0; i < m; ++i) part[(size_t)j * m + i] += a[i] * b[j];  // exact integers
-        }
+      diagonal_sum(D, G.c0 * fmm::kSplitChunk, std::min(k, G.c1 * fmm::kSplitChunk));
       const double scale = std::ldexp(1.0, -8 * (D + 2));
       for (size_t x = 0; x < part.size(); ++x) {
         const float f = (float)part[x];  // the FP32 accumulator (exact)
@@ -211,7 +245,8 @@ void split_product(const fmm::SplitDesc& d, int slices) {
 
 void run_split(const fmm::Op& op, const unsigned char* desc) {
   const fmm::SplitDesc* g = reinterpret_cast<const fmm::SplitDesc*>(desc + op.desc_off);
-  for (int p = 0; p < op.n; ++p) split_product(g[p], op.split.slices);
+  const int code = op.split.int8 ? fmm::kSplitInt8Code + op.split.slices : op.split.slices;
+  for (int p = 0; p < op.n; ++p) split_product(g[p], code);
 }
 
 void run_ops(const fmm::Program& prog) {

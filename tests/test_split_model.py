@@ -172,3 +172,100 @@ def test_split_batch_items_equal_their_single_calls():
         else:
             split_fast(E, alg, As[i], Bs[i], want, s, 1e-8, 1.0, 0.75, 0, sl)
         assert np.array_equal(got, want), i
+
+
+# ---------------------------------------------------------------------------
+# Split-INT8: the same scaling, 7-bit signed digits, exact int32 sums per
+# diagonal over up to 32768 k, FP64 recombination.  The model passes the
+# planner's split code (16 + slices) through every entry point.
+
+I8 = 16
+
+
+@pytest.mark.parametrize("slices", [2, 3, 4, 5, 6, 7, 8])
+def test_int8_product_within_its_error_bound(slices):
+    E = emulator()
+    rng = np.random.default_rng(100 + slices)
+    m, k, n = 70, 300, 45
+    A = np.asfortranarray(rng.standard_normal((m, k)) * np.exp2(rng.uniform(-16, 16, (m, 1))))
+    B = np.asfortranarray(rng.standard_normal((k, n)) * np.exp2(rng.uniform(-16, 16, (1, n))))
+    got = np.zeros((m, n), order="F")
+    split_gemm(E, A, B, got, 1.0, 0.0, I8 + slices)
+    err = scaled_error(A, B, got, A @ B)
+    # representation error 2^-7S per operand (relative to the row / column
+    # maximum) on both sides, the dropped diagonals (S - 1 terms of at most
+    # 2^-7S), and the FP64 rounding
+    assert err <= (slices + 2) * 2.0 ** (-7 * slices) + 1e-15, (slices, err)
+
+
+def test_int8_six_slices_match_five_bf16_slices():
+    E = emulator()
+    A = oracle.uniform(64, 512, 21, 1)
+    B = oracle.uniform(512, 48, 21, 2)
+    want = A @ B
+    errs = {}
+    for code in (5, I8 + 6, I8 + 7):
+        got = np.zeros((64, 48), order="F")
+        split_gemm(E, A, B, got, 1.0, 0.0, code)
+        errs[code] = float(np.abs(got - want).max() / np.abs(want).max())
+    assert errs[I8 + 6] < 2.0 * errs[5] and errs[I8 + 6] < 1e-12, errs
+    assert errs[I8 + 7] < errs[I8 + 6] / 16, errs
+
+
+def test_int8_sum_groups_past_32768_k():
+    """k beyond one int32 group (128 chunks of 256): the second group is summed
+    separately, and the result stays within the bound."""
+    E = emulator()
+    m, k, n = 6, 32768 + 300, 5
+    A = oracle.uniform(m, k, 4, 1)
+    B = oracle.uniform(k, n, 4, 2)
+    got = np.zeros((m, n), order="F")
+    split_gemm(E, A, B, got, 1.0, 0.0, I8 + 6)
+    assert scaled_error(A, B, got, A @ B) <= 8 * 2.0 ** -42 + 1e-15
+
+
+def test_int8_alpha_beta_and_ragged_shapes():
+    E = emulator()
+    for (m, k, n) in [(1, 1, 1), (3, 0, 2), (129, 257, 130), (5, 513, 1)]:
+        A = oracle.uniform(m, k, 8, 1) if k else np.zeros((m, 0), order="F")
+        B = oracle.uniform(k, n, 8, 2) if k else np.zeros((0, n), order="F")
+        C0 = oracle.uniform(m, n, 8, 3)
+        got = C0.copy(order="F")
+        split_gemm(E, A, B, got, -1.5, 0.25, I8 + 8)
+        want = -1.5 * (A @ B) + 0.25 * C0
+        assert np.allclose(got, want, rtol=1e-13, atol=1e-13 * max(k, 1)), (m, k, n)
+
+
+@pytest.mark.parametrize("alg,steps", [("strassen", 2), ("grey424_26_206", 1)])
+def test_int8_fast_matmul_every_schedule_identical_and_close_to_oracle(alg, steps):
+    E = emulator()
+    m, k, n = 133, 150, 97
+    A = oracle.uniform(m, k, 13, 1)
+    B = oracle.uniform(k, n, 13, 2)
+    C0 = oracle.uniform(m, n, 13, 3)
+    want = C0.copy(order="F")
+    oracle.fast_matmul(alg, A, B, want, steps, 1e-8, 1.0, 0.5)
+    # 6 INT8 slices are about as accurate as 5 BF16 ones, 7 as 6
+    for slices, tol in [(6, 1e-11), (7, 1e-12)]:
+        results = []
+        for d in range(steps + 1):
+            got = C0.copy(order="F")
+            split_fast(E, alg, A, B, got, steps, 1e-8, 1.0, 0.5, d, I8 + slices)
+            results.append(got)
+        for r in results[1:]:
+            assert np.array_equal(results[0], r)
+        assert float(np.abs(results[0] - want).max() / np.abs(want).max()) <= tol, slices
+
+
+def test_int8_workspace_query_covers_the_program():
+    E = emulator()
+    idx = NAMES.index("strassen")
+    for d in range(3):
+        q = E.emu_workspace_bytes_split(idx, 300, 600, 280, 2, d, I8 + 6)
+        A = oracle.uniform(300, 600, 2, 1)
+        B = oracle.uniform(600, 280, 2, 2)
+        C = np.zeros((300, 280), order="F")
+        st = split_fast(E, "strassen", A, B, C, 2, 1e-8, 1.0, 0.0, d, I8 + 6)
+        assert st[4] == q, (d, st[4], q)
+        # six one-byte slices take less scratch than five two-byte ones
+        assert q < E.emu_workspace_bytes_split(idx, 300, 600, 280, 2, d, 5)
