@@ -1232,18 +1232,22 @@ def run_fp32_workload(a):
     del Cb
     clocks = ClockSampler(0)
     clocks.start()
-    configs = [("classical (fmm_sgemm)", None, 0, 4), ("strassen", "strassen", 1, 4), ("strassen", "strassen", 2, 4),
-               ("strassen", "strassen", 2, 3), ("strassen", "strassen", 3, 3), ("grey424_26_206", "grey424_26_206", 2, 4),
-               ("grey424_26_206", "grey424_26_206", 2, 3)]
-    for label, alg, steps, sl in configs:
+    # split-INT8 with 4 slices (27 bits) is as accurate as split-BF16 with 3-4
+    # once the result is rounded to FP32
+    configs = [("classical (fmm_sgemm)", None, 0, "split_bf16", 4), ("strassen", "strassen", 1, "split_bf16", 4),
+               ("strassen", "strassen", 2, "split_bf16", 4), ("strassen", "strassen", 2, "split_bf16", 3),
+               ("strassen", "strassen", 3, "split_bf16", 3), ("grey424_26_206", "grey424_26_206", 2, "split_bf16", 4),
+               ("grey424_26_206", "grey424_26_206", 2, "split_bf16", 3), ("strassen", "strassen", 2, "split_int8", 4),
+               ("strassen", "strassen", 3, "split_int8", 4), ("grey424_26_206", "grey424_26_206", 2, "split_int8", 4)]
+    for label, alg, steps, prec, sl in configs:
         if alg is None:
             fn = lambda: fmm.matmul(A, B, C, handle=h)  # noqa: E731
         else:
-            fn = lambda: fmm.fast_matmul(alg, A, B, C, steps, precision="split_bf16", split_slices=sl,  # noqa: E731
+            fn = lambda: fmm.fast_matmul(alg, A, B, C, steps, precision=prec, split_slices=sl,  # noqa: E731
                                          handle=h)
         ms = timed(fn, a.steps)
         fmm.synchronize(h)
-        rows.append({"product": label, "num_steps": steps, "precision": "split_bf16 x%d" % sl, "ms": ms,
+        rows.append({"product": label, "num_steps": steps, "precision": "%s x%d" % (prec, sl), "ms": ms,
                      "tflops": flops / (ms * 1e-3) / 1e12, "max_rel_vs_exact_32_sampled": errors(C)})
         print(json.dumps({"fp32_row": rows[-1]}), file=sys.stderr, flush=True)
     clk = clocks.stop()

@@ -148,6 +148,8 @@ fmm_status fmm_sgemm(fmm_handle h, const float* A, int64_t lda, const float* B, 
   const int64_t lm = m > 1 ? m : 1, lk = k > 1 ? k : 1;
   if (o.precision == FMM_PRECISION_SPLIT_BF16)
     s = fmm_dgemm_split_bf16(h, a, lm, b, lk, c, lm, m, k, n, (double)alpha, (double)beta, o.split_slices);
+  else if (o.precision == FMM_PRECISION_SPLIT_INT8)
+    s = fmm_dgemm_split_int8(h, a, lm, b, lk, c, lm, m, k, n, (double)alpha, (double)beta, o.split_slices);
   else
     s = fmm_dgemm(h, a, lm, b, lk, c, lm, m, k, n, (double)alpha, (double)beta);
   if (s != FMM_OK) return s;

@@ -87,10 +87,9 @@ def test_alpha_beta_and_fp64_leaves():
     Cr = C0.copy(order="F")
     oracle.ref_fast_matmul_f32("strassen", A, B, Cr, 2, 1e-8, 1.5, -0.75)
     e_ref = rel_err(Cr, want)
-    for prec in (None, "fp64", "split_bf16"):
+    for prec, sl in ((None, 0), ("fp64", 0), ("split_bf16", 5), ("split_int8", 4)):
         Cd = dev(C0)
-        fmm.fast_matmul("strassen", dev(A), dev(B), Cd, 2, alpha=1.5, beta=-0.75, precision=prec,
-                        split_slices=5 if prec == "split_bf16" else 0)
+        fmm.fast_matmul("strassen", dev(A), dev(B), Cd, 2, alpha=1.5, beta=-0.75, precision=prec, split_slices=sl)
         fmm.synchronize()
         e = rel_err(host(Cd), want)
         assert e <= min(2.0 * e_ref, 2.0 ** -22), (prec, e, e_ref)
