@@ -209,41 +209,91 @@ __device__ __forceinline__ void store_digits_i8(double (&x)[8], int slices, uint
 // for every slice (8 threads per row, 16 bytes each).  The tile's row index
 // is XOR-swizzled by k so that both the column-wise fill and the row-wise
 // read-out touch every bank pair at most twice per warp.
+// Position of an A-splitting work tile: its problem q, row tile rt (32
+// rows) and 64-deep k-block kb.  A block's tiles advance by a fixed stride
+// (the grid size), which within one problem is a fixed step in (rt, kb): no
+// search and no division unless the tile enters another problem.  A
+// problem's tiles number (padded rows / 32) * (64-deep k-blocks) < 2^32.
+struct ATile {
+  int q;
+  int64_t end;              // first work tile after problem q
+  uint32_t rows;            // row tiles of problem q
+  uint32_t rt, kb;          // position within problem q
+  uint32_t step_rt, step_kb;  // the stride in row tiles and k-blocks
+};
+
+__device__ __forceinline__ void atile_seek(const SplitDesc* __restrict__ d, int nd, int64_t total, int64_t w,
+                                           uint32_t stride, ATile& t) {
+  t.q = find_desc(d, nd, w, [](const SplitDesc& s) { return s.sa_begin; });
+  const SplitDesc& s = d[t.q];
+  t.end = t.q + 1 < nd ? d[t.q + 1].sa_begin : total;
+  t.rows = (uint32_t)s.tiles_m * (kBM / 32);
+  const uint32_t local = (uint32_t)(w - s.sa_begin);
+  t.rt = local % t.rows;
+  t.kb = local / t.rows;
+  t.step_rt = stride % t.rows;
+  t.step_kb = stride / t.rows;
+}
+
+__device__ __forceinline__ void atile_next(const SplitDesc* __restrict__ d, int nd, int64_t total, int64_t w,
+                                           uint32_t stride, ATile& t) {
+  if (w < t.end) {
+    t.rt += t.step_rt;
+    t.kb += t.step_kb;
+    if (t.rt >= t.rows) {
+      t.rt -= t.rows;
+      ++t.kb;
+    }
+  } else {
+    atile_seek(d, nd, total, w, stride, t);
+  }
+}
+
 template <bool kInt8>
 __global__ void __launch_bounds__(256) split_a(const SplitDesc* __restrict__ d, int nd, int64_t total, int slices,
                                                const int* __restrict__ ea, uint8_t* __restrict__ out) {
   __shared__ double tile[64 * 32];
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
   const int row = threadIdx.x >> 3, kc = (threadIdx.x & 7) * 8;
+  const uint32_t stride = gridDim.x;
   auto at = [](int k, int r) { return k * 32 + (r ^ (((k >> 3) & 3) << 2)); };
   // The next tile's loads are issued before this tile's digits are computed
   // and stored, so each thread keeps a tile of loads in flight.
-  auto load = [&](int64_t w, double (&v)[8]) {
-    const int q = find_desc(d, nd, w, [](const SplitDesc& s) { return s.sa_begin; });
-    const SplitDesc& s = d[q];
-    const int64_t mp = (int64_t)s.tiles_m * kBM;
-    const int64_t local = w - s.sa_begin;
-    const int64_t i = (local % (mp / 32)) * 32 + tx, p0 = (local / (mp / 32)) * kBK;
+  auto load = [&](const ATile& t, double (&v)[8]) {
+    const SplitDesc& s = d[t.q];
+    const int64_t i = (int64_t)t.rt * 32 + tx, p0 = (int64_t)t.kb * kBK;
+    const double* a = s.A + i + p0 * s.lda;
+    if (i < s.m && p0 + kBK <= s.k) {
 #pragma unroll
-    for (int r = 0; r < 8; ++r) {
-      const int64_t p = p0 + ty + 8 * r;
-      v[r] = (i < s.m && p < s.k) ? s.A[i + p * s.lda] : 0.0;
+      for (int r = 0; r < 8; ++r) v[r] = a[(int64_t)(ty + 8 * r) * s.lda];
+    } else {
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        const int64_t p = p0 + ty + 8 * r;
+        v[r] = (i < s.m && p < s.k) ? a[(int64_t)(ty + 8 * r) * s.lda] : 0.0;
+      }
     }
   };
   double pre[8];
-  if ((int64_t)blockIdx.x < total) load(blockIdx.x, pre);
-  for (int64_t w = blockIdx.x; w < total; w += gridDim.x) {
-    const int q = find_desc(d, nd, w, [](const SplitDesc& s) { return s.sa_begin; });
-    const SplitDesc& s = d[q];
+  ATile next;
+  if ((int64_t)blockIdx.x < total) {
+    atile_seek(d, nd, total, blockIdx.x, stride, next);
+    load(next, pre);
+  }
+  for (int64_t w = blockIdx.x; w < total; w += stride) {
+    const ATile cur = next;
+    const SplitDesc& s = d[cur.q];
     const int64_t mp = (int64_t)s.tiles_m * kBM;
-    const int64_t local = w - s.sa_begin;
-    const int64_t rt = local % (mp / 32), kb = local / (mp / 32);
-    const int64_t i0 = rt * 32;
+    const int64_t kb = cur.kb;
+    const int64_t i0 = (int64_t)cur.rt * 32;
     __syncthreads();  // previous tile's readers are done
 #pragma unroll
     for (int r = 0; r < 8; ++r) tile[at(ty + 8 * r, tx)] = pre[r];
     __syncthreads();
-    if (w + gridDim.x < total) load(w + gridDim.x, pre);
+    if (w + stride < total) {
+      atile_next(d, nd, total, w + stride, stride, next);
+      load(next, pre);
+    }
     const int e = ea[s.e_off + i0 + row];
     double x[8];
 #pragma unroll
@@ -259,17 +309,27 @@ __global__ void __launch_bounds__(256) split_a(const SplitDesc* __restrict__ d, 
   }
 }
 
-// B: one block per padded column: the column maximum, then the slices, 8
-// consecutive k per thread (B's columns are contiguous in k, so they are
-// written as they are read).
+// B: one warp per padded column: the column maximum (a warp butterfly), then
+// the slices, 8 consecutive k per lane (B's columns are contiguous in k, so
+// they are written as they are read; the second read hits L2).  A warp's
+// columns advance by a fixed stride, so the problem search runs only when a
+// column enters another problem, and no block barrier is involved.
+constexpr int kSplitBWarps = 8;
+
 template <bool kInt8>
-__global__ void __launch_bounds__(256) split_b(const SplitDesc* __restrict__ d, int nd, int64_t total, int slices,
-                                               int* __restrict__ fb, uint8_t* __restrict__ out) {
+__global__ void __launch_bounds__(32 * kSplitBWarps) split_b(const SplitDesc* __restrict__ d, int nd, int64_t total,
+                                                             int slices, int* __restrict__ fb,
+                                                             uint8_t* __restrict__ out) {
   constexpr int kRowValues = kInt8 ? kSplitI8KBlock : kBK;  // k values per 128-byte slice row
-  __shared__ double red[8];
-  __shared__ int e_sh;
-  for (int64_t x = blockIdx.x; x < total; x += gridDim.x) {
-    const int q = find_desc(d, nd, x, [](const SplitDesc& s) { return s.f_off; });
+  const int lane = threadIdx.x & 31;
+  const int64_t stride = (int64_t)gridDim.x * kSplitBWarps;
+  int q = -1;
+  int64_t q_end = 0;  // first column after problem q
+  for (int64_t x = (int64_t)blockIdx.x * kSplitBWarps + (threadIdx.x >> 5); x < total; x += stride) {
+    if (q < 0 || x >= q_end) {
+      q = find_desc(d, nd, x, [](const SplitDesc& s) { return s.f_off; });
+      q_end = q + 1 < nd ? d[q + 1].f_off : total;
+    }
     const SplitDesc& s = d[q];
     const int64_t j = x - s.f_off;
     const int64_t np = (int64_t)s.tiles_n * kBN;
@@ -291,25 +351,21 @@ __global__ void __launch_bounds__(256) split_b(const SplitDesc* __restrict__ d, 
       }
     };
     double mx = 0.0;
-    if (live)
-      for (int p0 = threadIdx.x * 8; p0 < k; p0 += blockDim.x * 8) {
+    if (live) {
+#pragma unroll 4
+      for (int p0 = lane * 8; p0 < k; p0 += 256) {
         double v[8];
         load8(p0, v);
 #pragma unroll
         for (int c = 0; c < 8; ++c) mx = fmax(mx, fabs(v[c]));
       }
-    for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double v = 0.0;
-      for (int w = 0; w < 8; ++w) v = fmax(v, red[w]);
-      e_sh = exponent_above(v);
-      fb[x] = e_sh;
     }
-    __syncthreads();
-    const int f = e_sh;
-    for (int p0 = threadIdx.x * 8; p0 < kp; p0 += blockDim.x * 8) {
+    for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+    const int f = exponent_above(mx);
+    if (lane == 0) fb[x] = f;
+    const int64_t slice_bytes = (int64_t)s.kblocks * np * 128;
+#pragma unroll 2
+    for (int p0 = lane * 8; p0 < kp; p0 += 256) {
       double v[8];
       if (live) {
         load8(p0, v);
@@ -320,14 +376,12 @@ __global__ void __launch_bounds__(256) split_b(const SplitDesc* __restrict__ d, 
 #pragma unroll
       for (int c = 0; c < 8; ++c) v[c] = scale_pow2(v[c], f);
       const int64_t orow = s.b_row + (int64_t)(p0 / kRowValues) * np + j;
-      const int64_t slice_bytes = (int64_t)s.kblocks * np * 128;
       if constexpr (kInt8)
         store_digits_i8(v, slices, out + orow * 128 + (p0 % kRowValues), slice_bytes);
       else
         store_digits(v, slices, reinterpret_cast<__nv_bfloat16*>(out + orow * 128) + (p0 % kRowValues),
                      slice_bytes / 2);
     }
-    __syncthreads();  // e_sh and red are reused by the next column
   }
 }
 
@@ -703,10 +757,12 @@ cudaError_t split_gemm_launch(const SplitDesc* d_descs, int n, const SplitPlan& 
                                                                                              plan.n_e / 32, ea);
   if (plan.int8) {
     split_a<true><<<grid_for(plan.sa_work, cap), 256, 0, stream>>>(d_descs, n, plan.sa_work, plan.slices, ea, as);
-    split_b<true><<<grid_for(plan.n_f, cap), 256, 0, stream>>>(d_descs, n, plan.n_f, plan.slices, fb, bs);
+    split_b<true><<<grid_for((plan.n_f + kSplitBWarps - 1) / kSplitBWarps, cap), 32 * kSplitBWarps, 0, stream>>>(
+        d_descs, n, plan.n_f, plan.slices, fb, bs);
   } else {
     split_a<false><<<grid_for(plan.sa_work, cap), 256, 0, stream>>>(d_descs, n, plan.sa_work, plan.slices, ea, as);
-    split_b<false><<<grid_for(plan.n_f, cap), 256, 0, stream>>>(d_descs, n, plan.n_f, plan.slices, fb, bs);
+    split_b<false><<<grid_for((plan.n_f + kSplitBWarps - 1) / kSplitBWarps, cap), 32 * kSplitBWarps, 0, stream>>>(
+        d_descs, n, plan.n_f, plan.slices, fb, bs);
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
