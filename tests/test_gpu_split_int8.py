@@ -164,3 +164,37 @@ def test_int8_slice_count_out_of_range_is_rejected():
         fmm.matmul_split_int8(A, B, C, slices=9)
     with pytest.raises(fmm.FmmError):
         fmm.fast_matmul("strassen", A, B, C, 1, precision="split_int8", split_slices=1)
+
+
+def test_int8_requests_in_the_server_equal_alone():
+    """Split-INT8, split-BF16 and FP64 requests mixed in one server: each
+    result equals the same product computed alone."""
+    import torch
+
+    rng = np.random.default_rng(5)
+    reqs = []
+    for i in range(12):
+        m, k, n = (int(v) for v in rng.integers(100, 700, 3))
+        A = fmm.random_matrix(m, k, 23, 3 * i)
+        B = fmm.random_matrix(k, n, 23, 3 * i + 1)
+        prec, sl = [("split_int8", 6), ("split_bf16", 5), ("fp64", 0)][i % 3]
+        reqs.append((A, B, prec, sl))
+    alone = []
+    for A, B, prec, sl in reqs:
+        C = fmm.colmajor_empty(A.shape[0], B.shape[1], A.device)
+        fmm.fast_matmul("strassen", A, B, C, 1, precision=prec, split_slices=sl)
+        alone.append(C)
+    fmm.synchronize()
+    srv = fmm.Server(workspace_bytes=4 << 30, max_inflight=3)
+    try:
+        outs, tickets = [], []
+        for A, B, prec, sl in reqs:
+            C = fmm.colmajor_empty(A.shape[0], B.shape[1], A.device)
+            tickets.append(srv.submit(A, B, C, alg="strassen", num_steps=1, precision=prec, split_slices=sl))
+            outs.append(C)
+        for t in tickets:
+            assert srv.wait(t, 60000.0)["status"] == 0
+    finally:
+        srv.close()
+    for a, o in zip(alone, outs):
+        assert torch.equal(a, o)
