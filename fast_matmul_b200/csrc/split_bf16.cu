@@ -166,8 +166,10 @@ __global__ void __launch_bounds__(kExpWarps * 32) split_row_exponents(const Spli
 // low word of the sum.  |d| <= 256, so its BF16 pattern is the top half of
 // the FP32 value (1.5 * 2^23 + d) - 1.5 * 2^23 (exact).  No conversion-unit
 // instruction is involved.
-__device__ __forceinline__ uint32_t bf16_bits_of_small_int(int d) {
-  return __float_as_uint(__int_as_float(0x4B400000 + d) - 12582912.0f) >> 16;
+// The FP32 value of a small integer d (|d| <= 2^22), whose top half is the
+// BF16 pattern of d when d has at most 8 significant bits.
+__device__ __forceinline__ uint32_t f32_bits_of_small_int(int d) {
+  return __float_as_uint(__int_as_float(0x4B400000 + d) - 12582912.0f);
 }
 
 __device__ __forceinline__ void store_digits(double (&x)[8], int slices, __nv_bfloat16* dst, int64_t slice_stride) {
@@ -179,7 +181,9 @@ __device__ __forceinline__ void store_digits(double (&x)[8], int slices, __nv_bf
       const double y0 = fma(x[c], 256.0, kRound), y1 = fma(x[c + 1], 256.0, kRound);
       x[c] = fma(x[c], 256.0, -(y0 - kRound));
       x[c + 1] = fma(x[c + 1], 256.0, -(y1 - kRound));
-      w[c / 2] = bf16_bits_of_small_int(__double2loint(y0)) | (bf16_bits_of_small_int(__double2loint(y1)) << 16);
+      // top halves of the two FP32 values: one byte permute
+      w[c / 2] = __byte_perm(f32_bits_of_small_int(__double2loint(y0)), f32_bits_of_small_int(__double2loint(y1)),
+                             0x7632);
     }
     *reinterpret_cast<uint4*>(dst + t * slice_stride) = make_uint4(w[0], w[1], w[2], w[3]);
   }
@@ -192,14 +196,17 @@ __device__ __forceinline__ void store_digits_i8(double (&x)[8], int slices, uint
   const double kRound = 6755399441055744.0;  // 1.5 * 2^52
   double radix = 64.0;
   for (int t = 0; t < slices; ++t) {
-    uint32_t w[2] = {0u, 0u};
+    uint32_t lo[8];
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
       const double y = fma(x[c], radix, kRound);
       x[c] = fma(x[c], radix, -(y - kRound));
-      w[c >> 2] |= ((uint32_t)__double2loint(y) & 0xFFu) << (8 * (c & 3));
+      lo[c] = (uint32_t)__double2loint(y);
     }
-    *reinterpret_cast<uint2*>(dst + t * slice_stride) = make_uint2(w[0], w[1]);
+    // the low bytes of lo[0..3] (lo[4..7]) in order: three byte permutes each
+    const uint32_t w0 = __byte_perm(__byte_perm(lo[0], lo[1], 0x0040), __byte_perm(lo[2], lo[3], 0x0040), 0x5410);
+    const uint32_t w1 = __byte_perm(__byte_perm(lo[4], lo[5], 0x0040), __byte_perm(lo[6], lo[7], 0x0040), 0x5410);
+    *reinterpret_cast<uint2*>(dst + t * slice_stride) = make_uint2(w0, w1);
     radix = 128.0;
   }
 }
