@@ -1151,6 +1151,24 @@ def run_int8_workload(a):
     clk = clocks.stop()
     ok = [r for r in rows if r["error"]["max_rel_elementwise"] <= 1e-12]
     head = max(ok, key=lambda r: r["effective_tflops"]) if ok else None
+    # N(0, 1) entries with per-row (A) / per-column (B) scales 2^U{-16..16}:
+    # errors only (elementwise relative errors are unbounded there for every
+    # Strassen variant, FP64 included; normwise ones are comparable)
+    del A, B, ref, absAB
+    torch.cuda.empty_cache()
+    A = scaled_normal(n, n, 41, "row", dev)
+    B = scaled_normal(n, n, 42, "col", dev)
+    ref = fmm.colmajor_empty(n, n, dev)
+    fmm.matmul(A, B, ref, handle=h)
+    absAB = fmm.colmajor_empty(n, n, dev)
+    fmm.matmul(A.abs(), B.abs(), absAB, handle=h)
+    scaled_rows = []
+    for prec, sl in (("fp64", 0), ("split_bf16", 6), ("split_int8", 6), ("split_int8", 7)):
+        fmm.fast_matmul("strassen", A, B, C, 2, precision=prec, split_slices=sl, handle=h)
+        fmm.synchronize(h)
+        scaled_rows.append({"algorithm": "strassen", "num_steps": 2, "precision": "%s x%d" % (prec, sl) if sl else prec,
+                            "error": precision_errors(fmm, A, B, C, ref, absAB, h)})
+        print(json.dumps({"int8_scaled_row": scaled_rows[-1]}), file=sys.stderr, flush=True)
     peaks, peak_src = measured_peaks()
     roofline = None
     if head and head["slice_product_tensor_tops"] and "int8" in head["precision"]:
@@ -1175,6 +1193,7 @@ def run_int8_workload(a):
         "speedup_vs_engine_classical": head["effective_tflops"] / engine if head else None,
         "speedup_vs_cublas": head["effective_tflops"] / cublas if head else None,
         "roofline": roofline, "clocks": clk, "rows": rows,
+        "scaled_normal_inputs": scaled_rows,
     }
     print(json.dumps(out))
     return 0

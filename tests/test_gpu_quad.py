@@ -10,6 +10,7 @@ against their __float128 values:
   step) and the engine's classical GEMM: max relative error <= 1e-13;
 * split-BF16 leaf products: <= 1e-12 at 6 slices, <= 1e-11 at 5 slices
   (uniform [0, 1) inputs, where elementwise relative errors are meaningful);
+  split-INT8: <= 1e-12 at 7 slices, <= 1e-11 at 6;
 * Bini's approximate <3,2,2;10> at lambda = 2^-13: the same error in FP64 and
   split-BF16 (6 slices), within a factor 2.
 """
@@ -53,6 +54,11 @@ CASES = [
      lambda A, B, C: fmm.fast_matmul("strassen", A, B, C, 2, precision="split_bf16", split_slices=6), 1e-12),
     ("strassen s2 split x5",
      lambda A, B, C: fmm.fast_matmul("strassen", A, B, C, 2, precision="split_bf16", split_slices=5), 1e-11),
+    ("classical int8 x7", lambda A, B, C: fmm.matmul_split_int8(A, B, C, slices=7), 1e-12),
+    ("strassen s2 int8 x7",
+     lambda A, B, C: fmm.fast_matmul("strassen", A, B, C, 2, precision="split_int8", split_slices=7), 1e-12),
+    ("strassen s2 int8 x6",
+     lambda A, B, C: fmm.fast_matmul("strassen", A, B, C, 2, precision="split_int8", split_slices=6), 1e-11),
 ]
 
 
@@ -72,7 +78,11 @@ def test_approximate_algorithm_same_error_in_fp64_and_split(operands):
     C64 = run(A, B, lambda a, b, c: fmm.fast_matmul("bini322_10_52_approx", a, b, c, 1, x))
     Cs = run(A, B, lambda a, b, c: fmm.fast_matmul("bini322_10_52_approx", a, b, c, 1, x, precision="split_bf16",
                                                    split_slices=6))
+    Ci = run(A, B, lambda a, b, c: fmm.fast_matmul("bini322_10_52_approx", a, b, c, 1, x, precision="split_int8",
+                                                   split_slices=7))
     e64, _ = oracle.quad_errors(A, B, rows, cols, C64[rows, cols])
     es, _ = oracle.quad_errors(A, B, rows, cols, Cs[rows, cols])
+    ei, _ = oracle.quad_errors(A, B, rows, cols, Ci[rows, cols])
     assert 1e-8 < e64 < 1e-2  # lambda dominates the error
     assert es <= 2.0 * e64 and e64 <= 2.0 * es
+    assert ei <= 2.0 * e64 and e64 <= 2.0 * ei
