@@ -67,7 +67,7 @@ def parse_args(argv=None):
     ap.add_argument("--scaling-size", type=int, default=16384, help="square size of the scaling workload")
     ap.add_argument("--precision-sizes", default="8192,16384",
                     help="square sizes of the precision workload")
-    ap.add_argument("--batch-precision", default="fp64", choices=["fp64", "split_bf16"])
+    ap.add_argument("--batch-precision", default="fp64", choices=["fp64", "split_bf16", "split_int8"])
     ap.add_argument("--batch-count", type=int, default=4096)
     ap.add_argument("--serve-requests", type=int, default=300)
     ap.add_argument("--serve-slots", type=int, default=6)
@@ -578,6 +578,8 @@ def run_batch_workload(a):
             if alg == fmm.CLASSICAL:
                 if a.batch_precision == "split_bf16":
                     fmm.matmul_split_bf16(p["A"], p["B"], p["C"], slices=6, handle=h)
+                elif a.batch_precision == "split_int8":
+                    fmm.matmul_split_int8(p["A"], p["B"], p["C"], slices=6, handle=h)
                 else:
                     fmm.matmul(p["A"], p["B"], p["C"], handle=h)
             else:
@@ -589,10 +591,12 @@ def run_batch_workload(a):
     out = {
         "metric": METRIC, "value": flops / (ms * 1e-3) / 1e12, "unit": "TFLOP/s", "n_gpus": 1, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if a.batch_precision == "fp64" else "bf16 slices (FP64 in and out)", "data": "synthetic",
+        "dtype": {"fp64": "f64", "split_bf16": "bf16 slices (FP64 in and out)",
+                  "split_int8": "int8 slices (FP64 in and out)"}[a.batch_precision], "data": "synthetic",
         "config": {"workload": "batch of %d independent %s products, M,K,N log-uniform in [64,1024], "
                                "uniform[-1,1), autotuned per shape bucket, one CUDA-graph plan"
-                               % (a.batch_count, "FP64" if a.batch_precision == "fp64" else "split-BF16 (6 slices)"),
+                               % (a.batch_count, {"fp64": "FP64", "split_bf16": "split-BF16 (6 slices)",
+                                                  "split_int8": "split-INT8 (6 slices)"}[a.batch_precision]),
                    "total_gflop": flops / 1e9, "autotune_seconds": tune_s,
                    "choices": {("classical" if k[0] == fmm.CLASSICAL else "%s/%d" % (fmm.algorithm_names()[k[0]], k[1])): v
                                for k, v in choices.items()}},
@@ -1201,8 +1205,8 @@ def run_int8_workload(a):
 
 def run_fp32_workload(a):
     """FastMatmul<float> (fmm_fast_matmul_f32): FP32 operands widened to FP64
-    on the device, split-BF16 leaf products (4 slices by default), rounded to
-    FP32 once.  At n^3: Strassen with 1 and 2 steps and the classical
+    on the device, split leaf products (5 INT8 slices by default; BF16 and
+    other INT8 slice counts as rows), rounded to FP32 once.  At n^3: Strassen with 1 and 2 steps and the classical
     product (fmm_sgemm) against cuBLAS SGEMM (torch.matmul in float32, TF32
     off) on the same inputs, errors against the exact product of the FP32
     inputs on sampled entries, and the reference's own FastMatmul<float>
@@ -1253,11 +1257,12 @@ def run_fp32_workload(a):
     clocks.start()
     # split-INT8 with 4 slices (27 bits) is as accurate as split-BF16 with 3-4
     # once the result is rounded to FP32
-    configs = [("classical (fmm_sgemm)", None, 0, "split_bf16", 4), ("strassen", "strassen", 1, "split_bf16", 4),
+    configs = [("classical (fmm_sgemm)", None, 0, "split_int8", 5), ("strassen", "strassen", 1, "split_bf16", 4),
                ("strassen", "strassen", 2, "split_bf16", 4), ("strassen", "strassen", 2, "split_bf16", 3),
                ("strassen", "strassen", 3, "split_bf16", 3), ("grey424_26_206", "grey424_26_206", 2, "split_bf16", 4),
                ("grey424_26_206", "grey424_26_206", 2, "split_bf16", 3), ("strassen", "strassen", 2, "split_int8", 4),
-               ("strassen", "strassen", 3, "split_int8", 4), ("grey424_26_206", "grey424_26_206", 2, "split_int8", 4)]
+               ("strassen", "strassen", 3, "split_int8", 4), ("grey424_26_206", "grey424_26_206", 2, "split_int8", 4),
+               ("strassen", "strassen", 2, "split_int8", 5)]
     for label, alg, steps, prec, sl in configs:
         if alg is None:
             fn = lambda: fmm.matmul(A, B, C, handle=h)  # noqa: E731

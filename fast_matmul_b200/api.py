@@ -151,7 +151,7 @@ def colmajor_empty(m: int, n: int, device="cuda"):
     return torch.empty((n, m), dtype=torch.float64, device=device).t()
 
 
-F32_DEFAULT_SLICES = 4  # FMM_F32_DEFAULT_SLICES of include/fmm.h
+F32_DEFAULT_SLICES = 5  # FMM_F32_DEFAULT_SLICES of include/fmm.h (split-INT8 slices)
 
 
 def _mat(t, rows: int, cols: int, name: str, dtype=None) -> Tuple[int, int]:
@@ -189,7 +189,7 @@ def fast_matmul(alg, A, B, C, num_steps: int, x: float = 1e-8, alpha: float = 1.
 
     float32 operands (all three) select FastMatmul<float>
     (fmm_fast_matmul_f32): computed on FP64 copies and rounded to FP32 once;
-    precision None there means split-BF16 leaves with 4 slices."""
+    precision None there means split-INT8 leaves with 5 slices."""
     torch = _torch()
     idx = algorithm_index(alg)
     m, k = A.shape
@@ -201,8 +201,8 @@ def fast_matmul(alg, A, B, C, num_steps: int, x: float = 1e-8, alpha: float = 1.
         pa, lda = _mat(A, m, k, "A", torch.float32)
         pb, ldb = _mat(B, k, n, "B", torch.float32)
         pc, ldc = _mat(C, m, n, "C", torch.float32)
-        if precision is None:  # the FP32 default: split-BF16 leaves, FMM_F32_DEFAULT_SLICES slices
-            o = _options(schedule, dfs_levels, workspace_limit, "split_bf16", split_slices or F32_DEFAULT_SLICES)
+        if precision is None:  # the FP32 default: split-INT8 leaves, FMM_F32_DEFAULT_SLICES slices
+            o = _options(schedule, dfs_levels, workspace_limit, "split_int8", split_slices or F32_DEFAULT_SLICES)
         else:
             o = _options(schedule, dfs_levels, workspace_limit, precision, split_slices)
         check(lib().fmm_fast_matmul_f32(h.ptr, idx, pa, lda, pb, ldb, pc, ldc, m, k, n, num_steps, x, alpha, beta,
@@ -263,7 +263,7 @@ def fast_matmul_host(alg, A, B, C, num_steps: int, x: float = 1e-8, alpha: float
 def matmul(A, B, C, alpha: float = 1.0, beta: float = 0.0, handle: Optional[Handle] = None) -> None:
     """Classical C := alpha * A * B + beta * C on the engine's FP64 GEMM
     (MatMul with C's multiplier as alpha).  float32 operands: MatMul<float>
-    (fmm_sgemm: FP64 copies, split-BF16 with 4 slices, rounded to FP32)."""
+    (fmm_sgemm: FP64 copies, split-INT8 with 5 slices, rounded to FP32)."""
     torch = _torch()
     m, k = A.shape
     n = B.shape[1]

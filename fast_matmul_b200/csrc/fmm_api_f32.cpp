@@ -1,7 +1,7 @@
 // FP32 entry points: <ns>::FastMatmul and MatMul with Scalar = float.
 //
 // The operands are widened to FP64 once (exact), the FP64 engine runs on
-// them -- by default with split-BF16 leaf products of 4 slices, 32 bits per
+// them -- by default with split-INT8 leaf products of 5 slices, 34 bits per
 // operand entry against FP32's 24 -- and the result is rounded to FP32 once.
 // The reference computes every addition and leaf product in FP32
 // (Scalar = float, algorithms/*.hpp; sgemm, linalg/blas_wrap.hpp:116-120),
@@ -30,7 +30,7 @@ void f32_options(const fmm_options* opts, fmm_options* o) {
   if (opts) {
     *o = *opts;
   } else {
-    o->precision = FMM_PRECISION_SPLIT_BF16;
+    o->precision = FMM_PRECISION_SPLIT_INT8;
     o->split_slices = FMM_F32_DEFAULT_SLICES;
   }
 }

@@ -179,12 +179,13 @@ fmm_status fmm_dgemm_host(fmm_handle h, const double* A, int64_t lda, const doub
  * (exact), the product runs on the FP64 engine, and C is rounded to FP32
  * once (round to nearest), so every result is at least as accurate as the
  * reference's, which rounds in FP32 at every addition and leaf product.
- * opts == NULL selects split-BF16 leaf products with FMM_F32_DEFAULT_SLICES
- * slices (32 bits per operand entry, beyond FP32's 24); other options are
- * taken as given (FMM_PRECISION_FP64 runs FP64 leaves).  Device pointers,
+ * opts == NULL selects split-INT8 leaf products with FMM_F32_DEFAULT_SLICES
+ * slices (34 bits per operand entry, beyond FP32's 24); other options are
+ * taken as given (FMM_PRECISION_FP64 runs FP64 leaves, SPLIT_BF16 BF16
+ * slices).  Device pointers,
  * the handle's stream; FP64 staging of m*k + k*n + m*n doubles is held by
  * the handle.  num_steps == 0 ignores beta, as FastMatmul does. */
-#define FMM_F32_DEFAULT_SLICES 4
+#define FMM_F32_DEFAULT_SLICES 5
 fmm_status fmm_fast_matmul_f32(fmm_handle h, int alg, const float* A, int64_t lda, const float* B, int64_t ldb,
                                float* C, int64_t ldc, int64_t m, int64_t k, int64_t n, int num_steps, double x,
                                float alpha, float beta, const fmm_options* opts);

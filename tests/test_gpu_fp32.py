@@ -3,7 +3,7 @@ fmm_sgemm and their host forms).
 
 The reference computes these in FP32 throughout (Scalar = float, sgemm
 leaves); the engine widens the operands to FP64, multiplies there (by
-default with split-BF16 leaves of 4 slices) and rounds once.  Each case
+default with split-INT8 leaves of 5 slices) and rounds once.  Each case
 runs the reference itself (oracle/_ref, the reference's headers with
 Scalar = float) on the same FP32 inputs and checks, against the exact
 product of those inputs:
