@@ -832,6 +832,8 @@ def run_precision_workload(a):
     rows = []
     classical = {}
     head = None
+    clocks = ClockSampler(0)
+    clocks.start()
     for n in sizes:
         flops = 2.0 * n ** 3
         for dist in ("uniform[0,1)", "N(0,1)*2^U(-16,16)"):
@@ -894,6 +896,7 @@ def run_precision_workload(a):
             del A, B, C, ref, absAB
             torch.cuda.empty_cache()
 
+    clk = clocks.stop()
     peaks, peak_src = measured_peaks()
     n_head = max(sizes)
     base = classical[n_head]
@@ -925,6 +928,7 @@ def run_precision_workload(a):
         "speedup_vs_engine_classical": value / base["engine_dgemm_tflops"] if value else None,
         "speedup_vs_cublas": value / base["cublas_dgemm_tflops"] if value else None,
         "roofline": roofline,
+        "clocks": clk,
         "rows": rows,
     }
     print(json.dumps(out))
