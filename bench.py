@@ -569,7 +569,10 @@ def run_batch_workload(a):
     for _ in range(a.warmup):
         plan.execute()
     launches0 = h.launches()
+    clocks = ClockSampler(0)
+    clocks.start()
     ms = timed(plan.execute, a.steps)
+    clk = clocks.stop()
     launches = (h.launches() - launches0) // max(a.steps, 1)
 
     def one_at_a_time():
@@ -602,6 +605,7 @@ def run_batch_workload(a):
                                for k, v in choices.items()}},
         "one_at_a_time": {"value": flops / (ms_single * 1e-3) / 1e12, "ms": ms_single,
                           "speedup_of_batched": ms_single / ms},
+        "clocks": clk,
         "gpu_launches": launches,
     }
     print(json.dumps(out))
@@ -688,10 +692,13 @@ def run_serve_workload(a):
             tickets[i] = srv.submit(A, B, C, fmm.AUTO, precision="split_bf16" if wants_split[i] else "fp64",
                                     split_slices=split_slices)
 
+    clocks = ClockSampler(0)
+    clocks.start()
     th = threading.Thread(target=client)
     th.start()
     th.join()
     srv.drain()
+    clk = clocks.stop()
     infos = [srv.wait(t) for t in tickets]
     stats = srv.stats()
     srv.close()
@@ -718,6 +725,7 @@ def run_serve_workload(a):
                                 "what": "classical FP64 GEMM per request, launch + synchronize each"},
         "server": stats,
         "results_identical_to_alone": bool(same),
+        "clocks": clk,
         "gpu_launches": stats["launches"],
     }
     print(json.dumps(out))
