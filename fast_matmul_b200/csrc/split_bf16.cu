@@ -81,7 +81,12 @@ constexpr uint16_t kPairMask = 0x3;  // both CTAs of the cluster
 // warpgroups of 32 columns (measured +6-8% at 3 slices), more slices two of
 // 64 (four were 2% slower at 5).
 constexpr int gemm_threads(int epi_groups) { return 32 * (2 + 4 * epi_groups); }
+// INT8 digits pair the diagonals (D, D + 1): a stage holds A_t with B_{D-t}
+// and B_{D+1-t} (64 KB, two products from one A tile), 3 stages.
+constexpr int kI8StageBytes = kStageKBlocks * (kATileBytes + 2 * kBTileBytes);
+constexpr int kI8Stages = 3;
 constexpr size_t kGemmSmem = (size_t)kStages * kStageBytes + 1024;
+static_assert((size_t)kI8Stages * kI8StageBytes + 1024 <= kGemmSmem && kI8Stages <= kStages, "INT8 ring fits");
 static_assert(kChunkBlocks == 2 && kChunkBlocks % kStageKBlocks == 0, "stages tile the chunk");
 static_assert(kBK * 2 == 128, "one k-block row is one 128-byte swizzle row");
 static_assert(kATileBytes % 1024 == 0 && kBTileBytes % 1024 == 0, "128-byte-swizzled tiles start 1024-aligned");
@@ -517,6 +522,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(gemm_threads(kEpiGro
   cluster_sync();  // barriers of both CTAs initialised, tensor memory allocated
   tc_fence_after();
   const uint32_t tmem = tmem_slot;
+  // the stage ring: 4 stages of one slice product (BF16), 3 of a diagonal pair (INT8)
+  constexpr int kSt = kInt8 ? kI8Stages : kStages;
+  constexpr int kStB = kInt8 ? kI8StageBytes : kStageBytes;
 
   if (warp == 0) {
     if (lane == 0) {
@@ -533,6 +541,53 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(gemm_threads(kEpiGro
         const int64_t ya_tile = s.a_row + (int64_t)tc.tm * kSplitPairRows + rank * kBM;
         const int64_t yb_tile = s.b_row + (int64_t)tc.tn * kBN + rank * kBHalf;
         const int chunks = s.kblocks / kChunkBlocks;
+        if constexpr (kInt8) {
+          // one stage: A_t with B_u1 and, for a paired product, B_u2, over
+          // one 256-deep chunk starting at k-block blk
+          auto load_stage = [&](int t, int u1, int u2, int64_t blk) -> bool {
+            if (n >= (uint32_t)kSt && !mbar_wait(&empty[st], ph ^ 1u, g.err, 1)) return false;
+            uint8_t* dst = base + st * kStB;
+            const uint32_t bar = cluster_addr(&full[st], 0);  // the leader's
+            const uint32_t bytes = kStageKBlocks * (kATileBytes + (u2 >= 0 ? 2 : 1) * kBTileBytes);
+            if (leader) mbar_arrive_expect_tx(&full[st], 2 * bytes);
+            const int64_t ya = ya_tile + ((int64_t)t * s.kblocks + blk) * mp;
+            const int64_t yb1 = yb_tile + ((int64_t)u1 * s.kblocks + blk) * np;
+#pragma unroll
+            for (int b = 0; b < kStageKBlocks; ++b) {
+              tma_load_2d_pair(dst + b * kATileBytes, &tmA, bar, 0, (int)(ya + b * mp));
+              tma_load_2d_pair(dst + kStageKBlocks * kATileBytes + b * kBTileBytes, &tmB, bar, 0,
+                               (int)(yb1 + b * np));
+            }
+            if (u2 >= 0) {
+              const int64_t yb2 = yb_tile + ((int64_t)u2 * s.kblocks + blk) * np;
+#pragma unroll
+              for (int b = 0; b < kStageKBlocks; ++b)
+                tma_load_2d_pair(dst + kStageKBlocks * (kATileBytes + kBTileBytes) + b * kBTileBytes, &tmB, bar, 0,
+                                 (int)(yb2 + b * np));
+            }
+            ++n;
+            if (++st == (uint32_t)kSt) {
+              st = 0;
+              ph ^= 1u;
+            }
+            return true;
+          };
+          // per group of chunks, the diagonal pairs (D0, D0 + 1) in order;
+          // per chunk the stages t = 0..D0 (products (t, D0 - t) and
+          // (t, D0 + 1 - t)) and the lone (D0 + 1, 0); an odd last diagonal
+          // alone
+          for (int cg = 0; cg < chunks && ok; cg += kSplitI8GroupChunks) {
+            const int cend = min(cg + kSplitI8GroupChunks, chunks);
+            for (int D0 = 0; D0 < S && ok; D0 += 2) {
+              const bool two = D0 + 1 < S;
+              for (int c = cg; c < cend && ok; ++c)
+                for (int t = 0; t <= D0 + (two ? 1 : 0) && ok; ++t)
+                  ok = load_stage(t, t <= D0 ? D0 - t : 0, (two && t <= D0) ? D0 + 1 - t : -1,
+                                  (int64_t)c * kChunkBlocks);
+            }
+          }
+          continue;
+        }
         ok = for_each_group<kSpan, kInt8>(chunks, S, [&](int D, int c0, int c1) {
           for (int c = c0; c < c1; ++c)
             for (int t = 0; t <= D; ++t)
@@ -564,8 +619,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(gemm_threads(kEpiGro
       // the copies.  After an error the releases may never come; the wait
       // is then bounded and a short pause lets copies in flight land.
       bool drained = true;
-      for (uint32_t sx = 0; sx < (uint32_t)kStages && sx < n; ++sx) {
-        const uint32_t last = (n - 1 - sx) / kStages;  // round of stage sx
+      for (uint32_t sx = 0; sx < (uint32_t)kSt && sx < n; ++sx) {
+        const uint32_t last = (n - 1 - sx) / kSt;  // round of stage sx
         drained = mbar_drain(&empty[sx], last & 1, 1000000ull) && drained;
       }
       if (!drained) spin_ns(100000ull);
@@ -578,6 +633,68 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(gemm_threads(kEpiGro
       for (int64_t tile = pair; tile < g.tiles && ok; tile += pairs) {
         const TileCoord tc = tile_coord(g, tile);
         const int chunks = g.desc[tc.q].kblocks / kChunkBlocks;
+        if constexpr (kInt8) {
+          // the producer's order: per group of chunks, per diagonal pair
+          // (D0, D0 + 1) in accumulators b0, b1, per chunk the stages
+          // t = 0..D0 (8 MMAs into b0 from B_{D0-t}, 8 into b1 from
+          // B_{D0+1-t}) and the lone (D0 + 1, 0) into b1
+          for (int cg = 0; cg < chunks && ok; cg += kSplitI8GroupChunks) {
+            const int cend = min(cg + kSplitI8GroupChunks, chunks);
+            for (int D0 = 0; D0 < S && ok; D0 += 2) {
+              const bool two = D0 + 1 < S;
+              const uint32_t b0 = ai % kAccBufs, b1 = (ai + 1) % kAccBufs;
+              if (ai >= (uint32_t)kAccBufs && !mbar_wait(&acc_empty[b0], ((ai / kAccBufs) - 1) & 1, g.err, 2)) {
+                ok = false;
+                break;
+              }
+              if (two && ai + 1 >= (uint32_t)kAccBufs &&
+                  !mbar_wait(&acc_empty[b1], (((ai + 1) / kAccBufs) - 1) & 1, g.err, 2)) {
+                ok = false;
+                break;
+              }
+              tc_fence_after();
+              for (int c = cg; c < cend && ok; ++c)
+                for (int t = 0; t <= D0 + (two ? 1 : 0); ++t) {
+                  if (!mbar_wait(&full[st], ph, g.err, 3)) {
+                    ok = false;
+                    break;
+                  }
+                  tc_fence_after();
+                  const bool paired = two && t <= D0;
+                  const uint32_t d_first = tmem + ((two && t > D0) ? b1 : b0) * kBN;
+                  const uint32_t a = smem_addr(base + st * kStB);
+                  const uint32_t bb1 = a + kStageKBlocks * kATileBytes;
+                  const uint32_t bb2 = bb1 + kStageKBlocks * kBTileBytes;
+#pragma unroll
+                  for (int kk = 0; kk < kStageKBlocks * kBK / 16; ++kk) {
+                    const uint32_t koff = (kk & 3) * 32;
+                    mma_s8_pair(d_first, smem_desc_sw128(a + (kk >> 2) * kATileBytes + koff),
+                                smem_desc_sw128(bb1 + (kk >> 2) * kBTileBytes + koff), idesc,
+                                c > cg || t > 0 || kk > 0);
+                  }
+                  if (paired) {
+#pragma unroll
+                    for (int kk = 0; kk < kStageKBlocks * kBK / 16; ++kk) {
+                      const uint32_t koff = (kk & 3) * 32;
+                      mma_s8_pair(tmem + b1 * kBN, smem_desc_sw128(a + (kk >> 2) * kATileBytes + koff),
+                                  smem_desc_sw128(bb2 + (kk >> 2) * kBTileBytes + koff), idesc,
+                                  c > cg || t > 0 || kk > 0);
+                    }
+                  }
+                  mma_commit_pair(&empty[st], kPairMask);
+                  if (++st == (uint32_t)kSt) {
+                    st = 0;
+                    ph ^= 1u;
+                  }
+                }
+              if (!ok) break;
+              mma_commit_pair(&acc_full[b0], kPairMask);
+              if (two) mma_commit_pair(&acc_full[b1], kPairMask);
+              ai += two ? 2 : 1;
+            }
+          }
+          continue;
+        }
         ok = for_each_group<kSpan, kInt8>(chunks, S, [&](int D, int c0, int c1) {
           const uint32_t buf = ai % kAccBufs;
           if (ai >= (uint32_t)kAccBufs && !mbar_wait(&acc_empty[buf], ((ai / kAccBufs) - 1) & 1, g.err, 2))
