@@ -28,8 +28,10 @@
 // 256-deep chunks per diagonal, so a tile drains each diagonal once instead
 // of once per chunk.  Each diagonal sum is scaled by 2^-(12+7D) and added
 // into the FP64 accumulator in diagonal order.  A 128-byte slice row holds
-// 128 k values, so the tensor maps, TMA boxes, shared-memory descriptors and
-// MMA count per stage are those of the BF16 form byte for byte.
+// 128 k values, so the tensor maps, TMA boxes and shared-memory descriptors
+// are those of the BF16 form byte for byte.  The diagonals run in pairs
+// (D, D + 1) in two accumulators: a stage holds A_t with B_{D-t} and
+// B_{D+1-t}, so one A tile feeds two products (a third fewer bytes per MMA).
 // Error: |C - AB| <~ (S + 2) * 2^-7S * k * max|a_i.| * max|b_.j|.
 //
 // Product kernel: persistent CTA pairs (clusters of 2) over the 256 x 128
