@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 
 #include "fmm_internal.h"
 
@@ -337,15 +338,20 @@ cudaError_t gemm_launch_cfg(const GemmDesc* d_descs, int n, int64_t total_tiles,
   if (total_tiles <= 0 || n <= 0) return cudaSuccess;
   // the shared-memory opt-in is per device; set it once so launches can be
   // captured into CUDA graphs without other API calls in between
+  // (handles on several host threads may launch concurrently)
   static bool opted_in[64] = {};
+  static std::mutex mu;
   int dev = 0;
   cudaError_t err = cudaGetDevice(&dev);
   if (err != cudaSuccess) return err;
-  if (dev < 0 || dev >= 64 || !opted_in[dev]) {
-    err = cudaFuncSetAttribute(grouped_dgemm_kernel<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)Cfg::SMEM_BYTES);
-    if (err != cudaSuccess) return err;
-    if (dev >= 0 && dev < 64) opted_in[dev] = true;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev < 0 || dev >= 64 || !opted_in[dev]) {
+      err = cudaFuncSetAttribute(grouped_dgemm_kernel<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)Cfg::SMEM_BYTES);
+      if (err != cudaSuccess) return err;
+      if (dev >= 0 && dev < 64) opted_in[dev] = true;
+    }
   }
   const int64_t slots = (int64_t)num_sms * Cfg::MINB;
   const int64_t grid = total_tiles < slots ? total_tiles : slots;
