@@ -269,3 +269,41 @@ def test_int8_workspace_query_covers_the_program():
         assert st[4] == q, (d, st[4], q)
         # six one-byte slices take less scratch than five two-byte ones
         assert q < E.emu_workspace_bytes_split(idx, 300, 600, 280, 2, d, 5)
+
+
+def test_batch_mixing_int8_bf16_and_fp64_items_equals_single_calls():
+    """One batch with INT8, BF16 and FP64 leaf products: one split launch per
+    split code, each item equal to its own planner run."""
+    E = emulator()
+    items = [("strassen", 1, (90, 300, 80), I8 + 6), ("strassen", 1, (70, 260, 66), 5), (None, 0, (40, 520, 30), I8 + 7),
+             ("grey424_26_206", 1, (64, 64, 64), 0)]
+    algs = (ctypes.c_int * len(items))(*[NAMES.index(a) if a else -1 for a, _, _, _ in items])
+    steps = (ctypes.c_int * len(items))(*[s for _, s, _, _ in items])
+    dims = (ctypes.c_int64 * (3 * len(items)))(*[v for _, _, d, _ in items for v in d])
+    codes = (ctypes.c_int * len(items))(*[c for _, _, _, c in items])
+    As, Bs, Cs = [], [], []
+    for i, (_, _, (m, k, n), _) in enumerate(items):
+        As.append(oracle.uniform(m, k, 12, 3 * i))
+        Bs.append(oracle.uniform(k, n, 12, 3 * i + 1))
+        Cs.append(oracle.uniform(m, n, 12, 3 * i + 2))
+    Acat = np.concatenate([a.ravel(order="F") for a in As])
+    Bcat = np.concatenate([b.ravel(order="F") for b in Bs])
+    Ccat = np.concatenate([c.ravel(order="F") for c in Cs])
+    off = lambda arrs: (ctypes.c_int64 * len(arrs))(*np.cumsum([0] + [a.size for a in arrs[:-1]]).tolist())
+    stats = (ctypes.c_int64 * 5)()
+    rc = E.emu_fast_matmul_batch_split(len(items), algs, steps, dims, Acat.ctypes.data_as(P), off(As),
+                                       Bcat.ctypes.data_as(P), off(Bs), Ccat.ctypes.data_as(P), off(Cs), 1e-8, 1.0,
+                                       0.5, codes, stats)
+    assert rc == 0
+    # one FP64 grouped GEMM and one split launch per split code (three codes)
+    assert stats[1] == 4
+    pos = 0
+    for i, (alg, s, (m, k, n), code) in enumerate(items):
+        got = Ccat[pos:pos + m * n].reshape((m, n), order="F")
+        pos += m * n
+        want = Cs[i].copy(order="F")
+        if alg is None:
+            split_gemm(E, As[i], Bs[i], want, 1.0, 0.5, code)
+        else:
+            split_fast(E, alg, As[i], Bs[i], want, s, 1e-8, 1.0, 0.5, 0, code)
+        assert np.array_equal(got, want), i
