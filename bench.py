@@ -54,14 +54,20 @@ def parse_args(argv=None):
     ap.add_argument("--cpu-sample", type=int, default=4096, help="edge of the CPU baseline sample")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU work budget of the baseline sample")
     ap.add_argument("--workload", default="product",
-                    choices=["product", "batch", "serve", "precision", "scaling", "fp32", "int8"],
+                    choices=["product", "batch", "serve", "precision", "scaling", "fp32", "int8", "profile"],
                     help="product: one large FastMatmul (the headline); batch: 4096 independent products "
                          "with log-uniform dimensions in [64, 1024] in one CUDA-graph plan; serve: a Poisson "
                          "request stream through the continuous-batching server; precision: split-BF16 leaf "
                          "products (Strassen, Bini) against the FP64 oracle; scaling: diagonal scaling "
                          "(Scaling + FastMatmul + PostProcessScaling) on skewed operands; fp32: "
                          "FastMatmul<float> against cuBLAS SGEMM; int8: split-INT8 leaf products beside "
-                         "split-BF16 and FP64")
+                         "split-BF16 and FP64; profile: one product configuration (--alg or classical, --m/--k/--n, "
+                         "--num-steps, --precision, --split-slices) called --steps times untimed, as a profiler "
+                         "target (each call launches the same kernels, so a capture skips the first call's "
+                         "launches with ncu -s)")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "split_bf16", "split_int8"],
+                    help="leaf products of the profile workload")
+    ap.add_argument("--split-slices", type=int, default=5, help="slices of the profile workload's split leaves")
     ap.add_argument("--fp32-size", type=int, default=16384, help="square size of the fp32 workload")
     ap.add_argument("--int8-size", type=int, default=16384, help="square size of the int8 workload")
     ap.add_argument("--scaling-size", type=int, default=16384, help="square size of the scaling workload")
@@ -1329,6 +1335,31 @@ def run_fp32_workload(a):
     return 0
 
 
+def run_profile_workload(a):
+    """One product configuration called a.steps times, untimed (a profiler target)."""
+    import fast_matmul_b200 as fmm
+
+    A = fmm.random_matrix(a.m, a.k, 1, 1)
+    B = fmm.random_matrix(a.k, a.n, 1, 2)
+    C = fmm.colmajor_empty(a.m, a.n, A.device)
+    for _ in range(a.steps):
+        if a.alg == "classical":
+            if a.precision == "split_int8":
+                fmm.matmul_split_int8(A, B, C, slices=a.split_slices)
+            elif a.precision == "split_bf16":
+                fmm.matmul_split_bf16(A, B, C, slices=a.split_slices)
+            else:
+                fmm.matmul(A, B, C)
+        else:
+            fmm.fast_matmul(a.alg, A, B, C, a.num_steps, schedule=a.schedule, precision=a.precision,
+                            split_slices=a.split_slices)
+    fmm.synchronize()
+    print(json.dumps({"workload": "profile", "alg": a.alg, "m": a.m, "k": a.k, "n": a.n, "num_steps": a.num_steps,
+                      "precision": a.precision, "split_slices": a.split_slices, "calls": a.steps,
+                      "c00": float(C[0, 0])}))
+    return 0
+
+
 def main(argv=None):
     a = parse_args(argv)
     if a.impl == "reference":
@@ -1347,6 +1378,8 @@ def main(argv=None):
         return run_int8_workload(a)
     if a.workload == "fp32":
         return run_fp32_workload(a)
+    if a.workload == "profile":
+        return run_profile_workload(a)
     return run_ours(a)
 
 

@@ -86,8 +86,24 @@ extern "C" fmm_status fmm_fast_matmul_noalloc(int alg, const double* A, int64_t 
                     "its static scratch holds " + std::to_string(cap) + " (FMM_NOALLOC_SCRATCH_BYTES less " +
                     std::to_string(kDescBytes) + " for launch descriptors)");
 
+  // The launch descriptors are copied from a host buffer that the next call
+  // on this thread rewrites.  An ordinary cudaMemcpyAsync from pageable
+  // memory has consumed the source when it returns; a copy recorded into a
+  // graph would read the buffer again at every replay.  So a stream in
+  // capture mode is refused before anything is queued on it.
+  cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+  cudaError_t e = cudaStreamIsCapturing(static_cast<cudaStream_t>(stream), &capture);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(FMM_ERR_CUDA, std::string("cudaStreamIsCapturing: ") + cudaGetErrorString(e));
+  }
+  if (capture != cudaStreamCaptureStatusNone)
+    return fail(FMM_ERR_NOT_SUPPORTED,
+                "fmm_fast_matmul_noalloc stages its launch descriptors from reused host memory and does not run "
+                "on a stream in capture mode");
+
   int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
+  e = cudaGetDevice(&dev);
   if (e != cudaSuccess) {
     cudaGetLastError();
     return fail(FMM_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));

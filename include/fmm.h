@@ -450,6 +450,9 @@ fmm_status fmm_server_destroy(fmm_server s);
  *    Strassen with one step: dimensions up to about 1400).
  *  - The first call on a device looks up the array's device address (with
  *    that device current); make that first call before any stream capture.
+ *  - The launch descriptors are copied from a host buffer that the next call
+ *    reuses, so a stream in capture mode is refused with
+ *    FMM_ERR_NOT_SUPPORTED before anything is queued on it.
  *  - Every call shares the array and it keeps the last call's contents;
  *    nothing in it has to start at zero.  Calls that overlap on the GPU
  *    (different streams, or several host threads) race on it.

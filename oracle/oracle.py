@@ -33,11 +33,26 @@ _oracle = None
 _ref = None
 
 
+def reference_tree() -> Optional[str]:
+    """The reference checkout: $FMM_REFERENCE, else the tree _ref/ was built
+    from (recorded by the Makefile); None where neither exists."""
+    cands = [os.environ.get("FMM_REFERENCE")]
+    rec = os.path.join(HERE, "_ref", "REFERENCE_TREE")
+    if os.path.exists(rec):
+        with open(rec) as fh:
+            cands.append(fh.read().strip())
+    for c in cands:
+        if c and os.path.isdir(os.path.join(c, "algorithms")):
+            return c
+    return None
+
+
 def build(ref: bool = True) -> None:
-    """Builds liboracle.so and, when the reference tree exists, _ref/libfmm_ref.so."""
+    """Builds liboracle.so and, when a reference tree is known, _ref/libfmm_ref.so."""
     subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
-    if ref and os.path.isdir("/root/reference/algorithms"):
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+    tree = reference_tree() if ref else None
+    if tree:
+        subprocess.run(["make", "-s", "-C", HERE, "ref", "REF=" + tree], check=True)
 
 
 def oracle_lib() -> ctypes.CDLL:

@@ -20,6 +20,7 @@ from helpers import REPO
 
 sys.path.insert(0, os.path.join(REPO, "fast_matmul_b200", "codegen"))
 import coeffs  # noqa: E402
+import oracle  # noqa: E402
 
 JSON = os.path.join(REPO, "fast_matmul_b200", "generated", "algorithms.json")
 
@@ -109,12 +110,12 @@ def test_slot_expressions_evaluate_like_c():
             assert np.isfinite(v)
 
 
-@pytest.mark.skipif(not os.path.isdir("/root/reference/codegen/algorithms"), reason="reference tree not present")
+@pytest.mark.skipif(oracle.reference_tree() is None, reason="reference tree not present")
 def test_generated_files_are_current():
     gen = os.path.join(REPO, "fast_matmul_b200", "codegen", "gen_cuda.py")
+    coeff_dir = os.path.join(oracle.reference_tree(), "codegen", "algorithms")
     with tempfile.TemporaryDirectory() as tmp:
-        subprocess.run([sys.executable, gen, "/root/reference/codegen/algorithms", tmp], check=True,
-                       capture_output=True)
+        subprocess.run([sys.executable, gen, coeff_dir, tmp], check=True, capture_output=True)
         for rel in ("fast_matmul_b200/csrc/generated/fmm_algorithms.h",
                     "fast_matmul_b200/csrc/generated/fmm_alg_kernels.cuh",
                     "include/fmm/algorithms.hpp",
