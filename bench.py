@@ -51,6 +51,8 @@ def parse_args(argv=None):
     ap.add_argument("--schedule", default="auto", choices=["auto", "dfs", "bfs", "hybrid"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the precision, batch and serve sub-records of the headline line")
     ap.add_argument("--cpu-sample", type=int, default=4096, help="edge of the CPU baseline sample")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU work budget of the baseline sample")
     ap.add_argument("--workload", default="product",
@@ -288,6 +290,101 @@ class Replicas:
             self.dist.destroy_process_group()
 
 
+def reference_digest_diff(alg, m, k, n, steps, seed, C):
+    """Max relative difference of C from the reference's own result for this
+    product, over the committed digest of that result (sampled entries, fringe
+    rows and columns included, and band sums; tests/golden/reference_baseline.json,
+    written by tests/golden/make_reference_digests.py), or None without one."""
+    gold = os.path.join(REPO, "tests", "golden")
+    path = os.path.join(gold, "reference_baseline.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as fh:
+        cases = json.load(fh)["cases"]
+    hit = [c for c in cases if (c["alg"], c["m"], c["k"], c["n"], c["steps"], c["seed"]) == (alg, m, k, n, steps, seed)]
+    if not hit:
+        return None
+    c = hit[0]
+    sys.path.insert(0, gold)
+    import digest as dg
+
+    import fast_matmul_b200 as fmm
+
+    info = fmm.algorithm_info(alg)
+    rows, cols = dg.positions(m, n, info["m0"], info["n0"], steps, c["samples_count"], seed)
+    got = dg.digest_torch(C, rows, cols, c["groups"])
+    diff = dg.rel_diffs({key: dg.dec(c[key]) for key in ("samples", "rowsum", "colsum")}, got)
+    return {"max": diff["max"], "sampled_entries": diff["samples"], "row_band_sums": diff["rowsum"],
+            "column_band_sums": diff["colsum"], "entries": c["samples_count"], "bands": c["groups"],
+            "reference_max_rel_diff_vs_its_classical": c["ref_err"],
+            "source": "digest of the reference's own FastMatmul result on the same seeded inputs "
+                      "(tests/golden/reference_baseline.json)"}
+
+
+def precision_record(a, fmm, h, A, B, ref, classical_tf, cublas_tf, slices=5, steps=2):
+    """The split-BF16 precision target on the headline's operands: Strassen
+    with `steps` steps, leaf products split into `slices` BF16 slices (FP64 in
+    and out), timed with CUDA events (3 calls after one warm-up, clocks
+    sampled meanwhile), its error against the engine's FP64 classical product
+    `ref` of the same inputs, and the ratios to the engine's DGEMM and to
+    cuBLAS DGEMM measured in the same run."""
+    import torch
+
+    m, k = A.shape
+    n = B.shape[1]
+    flops = 2.0 * m * n * k
+    C = fmm.colmajor_empty(m, n, A.device)
+
+    def call():
+        fmm.fast_matmul("strassen", A, B, C, steps, precision="split_bf16", split_slices=slices, handle=h)
+
+    call()
+    torch.cuda.synchronize()
+    reps = 3
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    time.sleep(0.2)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        call()
+    e1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / reps
+    h.profile(True)
+    h.profile_reset()
+    call()
+    prof = h.profile_read()
+    h.profile(False)
+    fmm.synchronize(h)
+    rel, absd = fmm.max_relative_diff(ref, C, handle=h)
+    ex_rel, ex_scaled = exact_sample_errors(A, B, C, count=16)
+    leaf_ms = prof["gemm_ms"] - prof["split_ms"]
+    tf = flops / (ms * 1e-3) / 1e12
+    peaks, peak_src = measured_peaks()
+    pk = peaks.get("bf16_tflops_sustained", 1400.0)
+    prod_tf = prof["split_bf16_flops"] / (leaf_ms * 1e-3) / 1e12 if leaf_ms > 0 else None
+    del C
+    return {
+        "workload": "strassen %dx%dx%d, %d recursive steps, split-BF16 leaf products (%d slices), FP64 in and out, "
+                    "uniform[0,1) (the headline's operands)" % (m, k, n, steps, slices),
+        "value": tf, "unit": "TFLOP/s", "ms_per_call": ms, "calls": reps,
+        "error": {"max_rel_elementwise_vs_fp64_classical": rel,
+                  "max_rel_normwise_vs_fp64_classical": absd / float(ref.abs().max()),
+                  "max_rel_vs_exact_16_sampled_entries": ex_rel,
+                  "max_vs_exact_over_absAB_16_sampled_entries": ex_scaled, "target": 1e-12},
+        "speedup_vs_engine_dgemm": tf / classical_tf, "speedup_vs_cublas_dgemm": tf / cublas_tf,
+        "phases_ms": {"splitting": prof["split_ms"], "slice_products": leaf_ms, "form": prof["form_ms"],
+                      "combine": prof["combine_ms"], "peel": prof["peel_ms"]},
+        "roofline": {"kernel": "split_gemm_kernel (tcgen05 BF16 slice products)", "bound": "tensor",
+                     "achieved": prod_tf, "peak": pk, "unit": "TFLOP/s", "frac": prod_tf / pk if prod_tf else None,
+                     "peak_source": "bf16_tflops_sustained (%s)" % peak_src},
+        "clocks": clk,
+    }
+
+
 def run_ours(a):
     import torch
 
@@ -354,12 +451,11 @@ def run_ours(a):
     classical_tf = flops * reps / (e0.elapsed_time(e1) * 1e-3) / 1e12
     rel, absd = fmm.max_relative_diff(Cc, C, handle=h)
     ex_rel, ex_scaled = exact_sample_errors(A, B, C, count=32)
-    At, Bt = A, B
-    Ct = torch.matmul(At, Bt)
+    Ct = torch.matmul(A, B)
     torch.cuda.synchronize()
     e0.record()
     for _ in range(reps):
-        torch.matmul(At, Bt, out=Ct)
+        torch.matmul(A, B, out=Ct)
     e1.record()
     torch.cuda.synchronize()
     cublas_tf = flops * reps / (e0.elapsed_time(e1) * 1e-3) / 1e12
@@ -368,8 +464,13 @@ def run_ours(a):
     rel_cublas, _ = fmm.max_relative_diff(Ct_cm, C, handle=h)
     del Ct_cm
     del Ct
+    vs_ref = reference_digest_diff(a.alg, m, k, n, a.num_steps, 1234 + rank, C) if world == 1 else None
 
-    # ---- end to end through the host-memory C entry point
+    # ---- end to end through the host-memory C entry points: every step copies
+    # its A and B from pinned host memory to the device and its C back.  The
+    # pipelined entry point (fmm_fast_matmul_host_async) overlaps one step's
+    # copies with the neighbouring steps' products; the synchronous one
+    # (fmm_fast_matmul_host) runs them strictly one after the other.
     e2e = None
     if not a.no_e2e:
         Ah = torch.empty((k, m), dtype=torch.float64, pin_memory=True).t()
@@ -378,16 +479,31 @@ def run_ours(a):
         Ah.copy_(A)
         Bh.copy_(B)
         fmm.fast_matmul_host(a.alg, Ah, Bh, Ch, a.num_steps, schedule=a.schedule, handle=h)  # warm
-        e2e_steps = max(2, min(a.steps, 3))
+        for _ in range(2):
+            fmm.fast_matmul_host_async(a.alg, Ah, Bh, Ch, a.num_steps, schedule=a.schedule, handle=h)
+        fmm.host_sync(h)
+        e2e_steps = max(3, a.steps)
         barrier()
         t0 = time.perf_counter()
         for _ in range(e2e_steps):
+            fmm.fast_matmul_host_async(a.alg, Ah, Bh, Ch, a.num_steps, schedule=a.schedule, handle=h)
+        fmm.host_sync(h)
+        e2e_s = rep.max(time.perf_counter() - t0)
+        e2e_ok = bool(torch.equal(Ch.to(C.device), C))
+        sync_steps = max(2, min(a.steps, 3))
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(sync_steps):
             fmm.fast_matmul_host(a.alg, Ah, Bh, Ch, a.num_steps, schedule=a.schedule, handle=h)
-        e2e_s = time.perf_counter() - t0
-        e2e_s = rep.max(e2e_s)
+        sync_s = rep.max(time.perf_counter() - t0)
         e2e = {"value": rep.whole_job_rate(flops * e2e_steps, e2e_s) / 1e12, "unit": "TFLOP/s",
                "h2d_bytes_per_step": 8 * (m * k + k * n), "d2h_bytes_per_step": 8 * m * n,
-               "ms_per_step": e2e_s * 1e3 / e2e_steps, "api": "fmm_fast_matmul_host (include/fmm.h)"}
+               "ms_per_step": e2e_s * 1e3 / e2e_steps, "steps": e2e_steps,
+               "api": "fmm_fast_matmul_host_async + fmm_host_sync (include/fmm.h), pinned host buffers",
+               "result_equals_device_call": e2e_ok,
+               "one_call_at_a_time": {"value": rep.whole_job_rate(flops * sync_steps, sync_s) / 1e12,
+                                      "ms_per_step": sync_s * 1e3 / sync_steps, "steps": sync_steps,
+                                      "api": "fmm_fast_matmul_host (include/fmm.h)"}}
         del Ah, Bh, Ch
 
     # ---- roofline of the dominant kernel (grouped leaf FP64 GEMM)
@@ -441,7 +557,9 @@ def run_ours(a):
                        "m": m, "k": k, "n": n, "num_steps": a.num_steps, "schedule": a.schedule,
                        "precision": "fp64", "parallelism": "replicas" if world > 1 else "single GPU",
                        "l2": "inputs larger than L2 (each operand %.1f GiB > 126 MB)" % (8.0 * m * k / 2**30)},
-            "error": {"max_rel_diff_vs_classical": rel, "max_abs_diff_vs_classical": absd,
+            "error": {"max_rel_diff_vs_reference": vs_ref["max"] if vs_ref else None,
+                      "vs_reference": vs_ref,
+                      "max_rel_diff_vs_classical": rel, "max_abs_diff_vs_classical": absd,
                       "max_rel_diff_vs_cublas": rel_cublas,
                       "max_rel_vs_exact_32_sampled_entries": ex_rel,
                       "max_vs_exact_over_absAB_32_sampled_entries": ex_scaled},
@@ -456,6 +574,14 @@ def run_ours(a):
             "gpu_launches": launches,
             "workspace_bytes": fmm.workspace_bytes(a.alg, m, k, n, a.num_steps, a.schedule, handle=h),
         }
+        if world == 1 and not a.no_extras:
+            # the north star's secondary targets, each with its own clock record
+            out["precision"] = precision_record(a, fmm, h, A, B, Cc, classical_tf, cublas_tf)
+            del A, B, C, Cc
+            h.release_workspace()
+            torch.cuda.empty_cache()
+            out["batch"] = {"fp64": batch_record(a, "fp64"), "split_bf16": batch_record(a, "split_bf16")}
+            out["serve"] = serve_record(a)
         print(json.dumps(out))
     rep.close()
     return 0
@@ -536,13 +662,21 @@ def run_batch_workload(a):
     per shape bucket; the whole batch is one CUDA-graph plan (all leaf
     products in one persistent grouped GEMM launch).  Compared with the same
     products launched one call at a time."""
+    import torch
+
+    torch.cuda.set_device(0)
+    print(json.dumps(batch_record(a, a.batch_precision)))
+    return 0
+
+
+def batch_record(a, precision):
+    """The batch workload's JSON record for leaf products of `precision`."""
     import numpy as np
     import torch
 
     import fast_matmul_b200 as fmm
 
-    torch.cuda.set_device(0)
-    h = fmm.default_handle(0)
+    h = fmm.default_handle(torch.cuda.current_device())
     rng = np.random.default_rng(2024)
     dims = np.floor(np.exp(rng.uniform(np.log(64), np.log(1024), size=(a.batch_count, 3)))).astype(int)
     probs = []
@@ -550,7 +684,7 @@ def run_batch_workload(a):
         probs.append({"A": fmm.random_matrix(int(m), int(k), 7000 + i, 1, -1.0, 1.0, handle=h),
                       "B": fmm.random_matrix(int(k), int(n), 7000 + i, 2, -1.0, 1.0, handle=h),
                       "C": fmm.colmajor_empty(int(m), int(n)), "alg": fmm.AUTO,
-                      "precision": a.batch_precision, "split_slices": 6})
+                      "precision": precision, "split_slices": 6})
     flops = float(sum(2.0 * m * n * k for m, k, n in dims))
     t0 = time.perf_counter()
     fmm.autotune([tuple(int(v) for v in d) for d in dims], max_steps=1, handle=h)
@@ -575,7 +709,7 @@ def run_batch_workload(a):
     for _ in range(a.warmup):
         plan.execute()
     launches0 = h.launches()
-    clocks = ClockSampler(0)
+    clocks = ClockSampler(torch.cuda.current_device())
     clocks.start()
     ms = timed(plan.execute, a.steps)
     clk = clocks.stop()
@@ -585,14 +719,14 @@ def run_batch_workload(a):
         for p, (m, k, n) in zip(probs, dims):
             alg, steps = fmm.autotune_choice(int(m), int(k), int(n), handle=h)
             if alg == fmm.CLASSICAL:
-                if a.batch_precision == "split_bf16":
+                if precision == "split_bf16":
                     fmm.matmul_split_bf16(p["A"], p["B"], p["C"], slices=6, handle=h)
-                elif a.batch_precision == "split_int8":
+                elif precision == "split_int8":
                     fmm.matmul_split_int8(p["A"], p["B"], p["C"], slices=6, handle=h)
                 else:
                     fmm.matmul(p["A"], p["B"], p["C"], handle=h)
             else:
-                fmm.fast_matmul(alg, p["A"], p["B"], p["C"], steps, precision=a.batch_precision, split_slices=6,
+                fmm.fast_matmul(alg, p["A"], p["B"], p["C"], steps, precision=precision, split_slices=6,
                                 handle=h)
 
     one_at_a_time()
@@ -601,11 +735,11 @@ def run_batch_workload(a):
         "metric": METRIC, "value": flops / (ms * 1e-3) / 1e12, "unit": "TFLOP/s", "n_gpus": 1, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": {"fp64": "f64", "split_bf16": "bf16 slices (FP64 in and out)",
-                  "split_int8": "int8 slices (FP64 in and out)"}[a.batch_precision], "data": "synthetic",
+                  "split_int8": "int8 slices (FP64 in and out)"}[precision], "data": "synthetic",
         "config": {"workload": "batch of %d independent %s products, M,K,N log-uniform in [64,1024], "
                                "uniform[-1,1), autotuned per shape bucket, one CUDA-graph plan"
                                % (a.batch_count, {"fp64": "FP64", "split_bf16": "split-BF16 (6 slices)",
-                                                  "split_int8": "split-INT8 (6 slices)"}[a.batch_precision]),
+                                                  "split_int8": "split-INT8 (6 slices)"}[precision]),
                    "total_gflop": flops / 1e9, "autotune_seconds": tune_s,
                    "choices": {("classical" if k[0] == fmm.CLASSICAL else "%s/%d" % (fmm.algorithm_names()[k[0]], k[1])): v
                                for k, v in choices.items()}},
@@ -614,9 +748,8 @@ def run_batch_workload(a):
         "clocks": clk,
         "gpu_launches": launches,
     }
-    print(json.dumps(out))
     plan.close()
-    return 0
+    return out
 
 
 def run_serve_workload(a):
@@ -627,6 +760,15 @@ def run_serve_workload(a):
     requests by workspace footprint into concurrent batches (--serve-slots).  Reports
     throughput, p50/p99 latency (submission to completion) and the
     one-at-a-time throughput on the same requests."""
+    import torch
+
+    torch.cuda.set_device(0)
+    print(json.dumps(serve_record(a)))
+    return 0
+
+
+def serve_record(a):
+    """The serving workload's JSON record (on the current device)."""
     import threading
 
     import numpy as np
@@ -634,8 +776,8 @@ def run_serve_workload(a):
 
     import fast_matmul_b200 as fmm
 
-    torch.cuda.set_device(0)
-    h = fmm.default_handle(0)
+    dev = torch.cuda.current_device()
+    h = fmm.default_handle(dev)
     rng = np.random.default_rng(77)
     N = a.serve_requests
     dims = np.floor(np.exp(rng.uniform(np.log(256), np.log(8192), size=(N, 3)))).astype(int)
@@ -684,7 +826,7 @@ def run_serve_workload(a):
 
     rate = 2.0 * N / t_single  # requests per second offered
     gaps = rng.exponential(1.0 / rate, size=N)
-    srv = fmm.Server(0, workspace_bytes=0, max_inflight=a.serve_slots, max_batch=64)
+    srv = fmm.Server(dev, workspace_bytes=0, max_inflight=a.serve_slots, max_batch=64)
     tickets = [None] * N
 
     def client():
@@ -698,7 +840,7 @@ def run_serve_workload(a):
             tickets[i] = srv.submit(A, B, C, fmm.AUTO, precision="split_bf16" if wants_split[i] else "fp64",
                                     split_slices=split_slices)
 
-    clocks = ClockSampler(0)
+    clocks = ClockSampler(dev)
     clocks.start()
     th = threading.Thread(target=client)
     th.start()
@@ -734,8 +876,9 @@ def run_serve_workload(a):
         "clocks": clk,
         "gpu_launches": stats["launches"],
     }
-    print(json.dumps(out))
-    return 0
+    del reqs, reference
+    torch.cuda.empty_cache()
+    return out
 
 
 def scaled_normal(m, n, seed, per, device):

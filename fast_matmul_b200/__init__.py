@@ -29,6 +29,8 @@ from .api import (  # noqa: F401
     diagonal_scaling,
     fast_matmul,
     fast_matmul_host,
+    fast_matmul_host_async,
+    host_sync,
     matmul,
     matmul_split_bf16,
     matmul_split_int8,

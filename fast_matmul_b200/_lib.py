@@ -117,6 +117,8 @@ SIGNATURES = {
     "fmm_handle_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "fmm_set_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "fmm_set_workspace_limit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t]),
+    "fmm_release_workspace": (ctypes.c_int, [ctypes.c_void_p]),
+    "fmm_debug_fill_workspace": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]),
     "fmm_last_error": (ctypes.c_char_p, []),
     "fmm_num_algorithms": (ctypes.c_int, []),
     "fmm_algorithm_name": (ctypes.c_char_p, [ctypes.c_int]),
@@ -133,6 +135,12 @@ SIGNATURES = {
                                              ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int,
                                              ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                              ctypes.POINTER(Options), c_double_p]),
+    "fmm_fast_matmul_host_async": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int64,
+                                                   ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64,
+                                                   ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int,
+                                                   ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                                   ctypes.POINTER(Options)]),
+    "fmm_host_sync": (ctypes.c_int, [ctypes.c_void_p]),
     "fmm_workspace_query": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_int64,
                                             ctypes.c_int64, ctypes.c_int, ctypes.POINTER(Options),
                                             ctypes.POINTER(ctypes.c_size_t)]),

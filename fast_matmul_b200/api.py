@@ -104,6 +104,14 @@ class Handle:
     def set_workspace_limit(self, nbytes: int):
         check(lib().fmm_set_workspace_limit(self._h, nbytes))
 
+    def release_workspace(self):
+        """Frees the handle's workspace and staging buffers (fmm_release_workspace)."""
+        check(lib().fmm_release_workspace(self._h))
+
+    def debug_fill_workspace(self, nbytes: int, pattern: int = 0xFF):
+        """Grows the workspace to nbytes and fills it with a byte pattern (test support)."""
+        check(lib().fmm_debug_fill_workspace(self._h, nbytes, pattern))
+
     def launches(self) -> int:
         return int(lib().fmm_kernel_launch_count(self._h))
 
@@ -227,31 +235,57 @@ def workspace_bytes(alg, m: int, k: int, n: int, num_steps: int, schedule: str =
     return out.value
 
 
+def _host_mat(a, rows, cols, name):
+    """(pointer, leading dimension) of a column-major float64 host matrix."""
+    import numpy as np
+
+    if hasattr(a, "data_ptr"):
+        if a.device.type != "cpu":
+            raise ValueError("%s must be in host memory" % name)
+        ld = a.stride(1) if cols > 1 else max(rows, 1)
+        if rows > 1 and cols > 1 and a.stride(0) != 1:
+            raise ValueError("%s must be column-major" % name)
+        return a.data_ptr(), max(ld, rows, 1)
+    arr = a
+    if arr.dtype != np.float64 or (rows > 1 and cols > 1 and not arr.flags.f_contiguous):
+        raise ValueError("%s must be a Fortran-ordered float64 array" % name)
+    return arr.ctypes.data, max(rows, 1)
+
+
+def fast_matmul_host_async(alg, A, B, C, num_steps: int, x: float = 1e-8, alpha: float = 1.0, beta: float = 0.0,
+                           schedule: str = "auto", handle: Optional[Handle] = None) -> None:
+    """Pipelined host-memory call (fmm_fast_matmul_host_async): queues the
+    copies in, the product and the copy of C out, and returns at once; the
+    host buffers must stay alive and unchanged until host_sync().  Pinned
+    buffers let consecutive calls overlap their copies with each other's
+    products."""
+    m, k = A.shape
+    n = B.shape[1]
+    pa, lda = _host_mat(A, m, k, "A")
+    pb, ldb = _host_mat(B, k, n, "B")
+    pc, ldc = _host_mat(C, m, n, "C")
+    h = handle or default_handle()
+    o = _options(schedule)
+    check(lib().fmm_fast_matmul_host_async(h.ptr, algorithm_index(alg), pa, lda, pb, ldb, pc, ldc, m, k, n,
+                                           num_steps, x, alpha, beta, ctypes.byref(o)))
+
+
+def host_sync(handle: Optional[Handle] = None) -> None:
+    """Waits for every queued fast_matmul_host_async call (fmm_host_sync)."""
+    h = handle or default_handle()
+    check(lib().fmm_host_sync(h.ptr))
+
+
 def fast_matmul_host(alg, A, B, C, num_steps: int, x: float = 1e-8, alpha: float = 1.0, beta: float = 0.0,
                      schedule: str = "auto", handle: Optional[Handle] = None) -> float:
     """Host-memory variant (fmm_fast_matmul_host): A, B, C are column-major
     float64 host arrays (numpy, Fortran order) or CPU torch tensors; returns
     the call's wall time in ms, copies included."""
-    import numpy as np
-
-    def info(a, rows, cols, name):
-        if hasattr(a, "data_ptr"):
-            if a.device.type != "cpu":
-                raise ValueError("%s must be in host memory" % name)
-            ld = a.stride(1) if cols > 1 else max(rows, 1)
-            if rows > 1 and cols > 1 and a.stride(0) != 1:
-                raise ValueError("%s must be column-major" % name)
-            return a.data_ptr(), max(ld, rows, 1)
-        arr = a
-        if arr.dtype != np.float64 or (rows > 1 and cols > 1 and not arr.flags.f_contiguous):
-            raise ValueError("%s must be a Fortran-ordered float64 array" % name)
-        return arr.ctypes.data, max(rows, 1)
-
     m, k = A.shape
     n = B.shape[1]
-    pa, lda = info(A, m, k, "A")
-    pb, ldb = info(B, k, n, "B")
-    pc, ldc = info(C, m, n, "C")
+    pa, lda = _host_mat(A, m, k, "A")
+    pb, ldb = _host_mat(B, k, n, "B")
+    pc, ldc = _host_mat(C, m, n, "C")
     h = handle or default_handle()
     o = _options(schedule)
     ms = ctypes.c_double()

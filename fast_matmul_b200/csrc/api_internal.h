@@ -48,6 +48,19 @@ struct fmm_handle_s {
   void* narrow_io = nullptr;  // device copies of host FP32 operands
   size_t narrow_io_cap = 0;
   int* d_err = nullptr;       // error codes of split-BF16 kernels (bounded waits that gave up)
+  // pipelined host-pointer calls (fmm_fast_matmul_host_async): two device
+  // staging slots used in turn, a copy-in and a copy-out stream
+  struct HostSlot {
+    double* io = nullptr;
+    size_t cap = 0;
+    cudaEvent_t in_ready = nullptr;   // copies of this call's operands landed
+    cudaEvent_t out_ready = nullptr;  // this call's C is computed
+    cudaEvent_t free = nullptr;       // this call's C is back on the host
+    bool used = false;
+  };
+  HostSlot slots[2];
+  int next_slot = 0;
+  cudaStream_t h2d = nullptr, d2h = nullptr;
   int64_t launches = 0;
   fmm::Program prog;
   bool profiling = false;

@@ -24,10 +24,11 @@ Profiler::~Profiler() {
 }
 
 cudaError_t run_program(const Program& prog, const void* h_desc, void* d_desc, int num_sms, cudaStream_t stream,
-                        int64_t* launches, Profiler* prof, int* d_err) {
+                        int64_t* launches, Profiler* prof, int* d_err, cudaEvent_t desc_copied) {
   if (!prog.desc.empty()) {
     cudaError_t e = cudaMemcpyAsync(d_desc, h_desc, prog.desc.size(), cudaMemcpyHostToDevice, stream);
     if (e != cudaSuccess) return e;
+    if (desc_copied && (e = cudaEventRecord(desc_copied, stream)) != cudaSuccess) return e;
   }
   const unsigned char* base = static_cast<const unsigned char*>(d_desc);
   int64_t count = 0;

@@ -88,13 +88,12 @@ fmm_status stage_descriptors(fmm_handle h, const fmm::Program& prog) {
 }
 
 fmm_status run_staged(fmm_handle h, const fmm::Program& prog) {
+  // desc_done marks the end of the descriptor copy: the pinned staging
+  // buffer can take the next call's descriptors while this call still runs
   cudaError_t e = fmm::run_program(prog, h->h_desc, h->d_desc, h->num_sms, h->stream, &h->launches,
-                                   h->profiling ? &h->prof : nullptr, h->d_err);
+                                   h->profiling ? &h->prof : nullptr, h->d_err, h->desc_done);
+  if (!prog.desc.empty()) h->desc_pending = true;
   if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
-  if (!prog.desc.empty()) {
-    FMM_CUDA_TRY(cudaEventRecord(h->desc_done, h->stream), "cudaEventRecord");
-    h->desc_pending = true;
-  }
   return FMM_OK;
 }
 
@@ -264,11 +263,49 @@ fmm_status fmm_handle_destroy(fmm_handle h) {
   if (h->d_desc) cudaFree(h->d_desc);
   if (h->h_desc) cudaFreeHost(h->h_desc);
   if (h->io) cudaFree(h->io);
+  if (h->wide) cudaFree(h->wide);
+  if (h->narrow_io) cudaFree(h->narrow_io);
+  if (h->d2h) cudaStreamSynchronize(h->d2h);
+  for (auto& sl : h->slots) {
+    if (sl.io) cudaFree(sl.io);
+    for (cudaEvent_t e : {sl.in_ready, sl.out_ready, sl.free})
+      if (e) cudaEventDestroy(e);
+  }
+  if (h->h2d) cudaStreamDestroy(h->h2d);
+  if (h->d2h) cudaStreamDestroy(h->d2h);
   if (h->d_small) cudaFree(h->d_small);
   if (h->scal) cudaFree(h->scal);
   if (h->d_err) cudaFree(h->d_err);
   if (h->desc_done) cudaEventDestroy(h->desc_done);
   delete h;
+  return FMM_OK;
+}
+
+fmm_status fmm_debug_fill_workspace(fmm_handle h, size_t bytes, int pattern) {
+  if (!h) return fail(FMM_ERR_INVALID_ARGUMENT, "null handle");
+  if (pattern < 0 || pattern > 255) return fail(FMM_ERR_INVALID_ARGUMENT, "pattern must be a byte value");
+  DeviceGuard g(h->device);
+  fmm_status s = ensure_device_buffer(h, &h->ws, &h->ws_cap, bytes ? bytes : 256, "workspace");
+  if (s != FMM_OK) return s;
+  FMM_CUDA_TRY(cudaMemsetAsync(h->ws, pattern, h->ws_cap, h->stream), "cudaMemsetAsync(workspace)");
+  FMM_CUDA_TRY(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+  return FMM_OK;
+}
+
+fmm_status fmm_release_workspace(fmm_handle h) {
+  if (!h) return fail(FMM_ERR_INVALID_ARGUMENT, "null handle");
+  DeviceGuard g(h->device);
+  FMM_CUDA_TRY(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+  if (h->d2h) FMM_CUDA_TRY(cudaStreamSynchronize(h->d2h), "cudaStreamSynchronize(copy-out)");
+  void** bufs[] = {&h->ws, reinterpret_cast<void**>(&h->io), &h->wide, &h->narrow_io,
+                   reinterpret_cast<void**>(&h->slots[0].io), reinterpret_cast<void**>(&h->slots[1].io)};
+  size_t* caps[] = {&h->ws_cap, &h->io_cap, &h->wide_cap, &h->narrow_io_cap, &h->slots[0].cap, &h->slots[1].cap};
+  for (int i = 0; i < 6; ++i) {
+    if (*bufs[i]) cudaFree(*bufs[i]);
+    *bufs[i] = nullptr;
+    *caps[i] = 0;
+  }
+  h->slots[0].used = h->slots[1].used = false;
   return FMM_OK;
 }
 
@@ -376,6 +413,7 @@ fmm_status fmm_fast_matmul_host(fmm_handle h, int alg, const double* A, int64_t 
   if (!h) return fail(FMM_ERR_INVALID_ARGUMENT, "null handle");
   fmm_status s = check_alg(alg);
   if (s != FMM_OK) return s;
+  if ((h->slots[0].used || h->slots[1].used) && (s = fmm_host_sync(h)) != FMM_OK) return s;
   if ((s = check_dims(m, k, n, lda, ldb, ldc)) != FMM_OK) return s;
   if (m == 0 || n == 0) {
     if (elapsed_ms) *elapsed_ms = 0.0;
@@ -415,6 +453,89 @@ fmm_status fmm_fast_matmul_host(fmm_handle h, int alg, const double* A, int64_t 
   if (elapsed_ms)
     *elapsed_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   return FMM_OK;
+}
+
+fmm_status fmm_fast_matmul_host_async(fmm_handle h, int alg, const double* A, int64_t lda, const double* B,
+                                      int64_t ldb, double* C, int64_t ldc, int64_t m, int64_t k, int64_t n,
+                                      int num_steps, double x, double alpha, double beta, const fmm_options* opts) {
+  if (!h) return fail(FMM_ERR_INVALID_ARGUMENT, "null handle");
+  fmm_status s = check_alg(alg);
+  if (s != FMM_OK) return s;
+  if ((s = check_dims(m, k, n, lda, ldb, ldc)) != FMM_OK) return s;
+  if (num_steps < 0 || num_steps > 16) return fail(FMM_ERR_INVALID_ARGUMENT, "num_steps must be in [0, 16]");
+  if (m == 0 || n == 0) return FMM_OK;
+  if (!C || (k > 0 && (!A || !B))) return fail(FMM_ERR_INVALID_ARGUMENT, "null matrix pointer");
+  DeviceGuard g(h->device);
+  if (!g.ok()) return fail(FMM_ERR_CUDA, "cudaSetDevice failed");
+  if (!h->h2d) {
+    FMM_CUDA_TRY(cudaStreamCreateWithFlags(&h->h2d, cudaStreamNonBlocking), "cudaStreamCreate(copy-in)");
+    FMM_CUDA_TRY(cudaStreamCreateWithFlags(&h->d2h, cudaStreamNonBlocking), "cudaStreamCreate(copy-out)");
+    for (auto& sl : h->slots)
+      for (cudaEvent_t* e : {&sl.in_ready, &sl.out_ready, &sl.free})
+        FMM_CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "cudaEventCreate");
+  }
+  fmm_handle_s::HostSlot& sl = h->slots[h->next_slot];
+  fmm_handle_s::HostSlot& other = h->slots[h->next_slot ^ 1];
+  const size_t na = (size_t)m * (size_t)k, nb = (size_t)k * (size_t)n, nc = (size_t)m * (size_t)n;
+  const size_t need = (((na + 31) & ~(size_t)31) + ((nb + 31) & ~(size_t)31) + nc) * sizeof(double) + 512;
+  if (need > sl.cap) {
+    // the slot's previous call must be finished before its buffer goes
+    if (sl.used) FMM_CUDA_TRY(cudaEventSynchronize(sl.free), "cudaEventSynchronize(slot)");
+    if (sl.io) cudaFree(sl.io);
+    sl.io = nullptr;
+    sl.cap = 0;
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, need);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return fail(FMM_ERR_OUT_OF_MEMORY, "cannot allocate " + std::to_string(need) + " bytes of host-call operands");
+    }
+    sl.io = static_cast<double*>(p);
+    sl.cap = need;
+  }
+  double* dA = sl.io;
+  double* dB = dA + ((na + 31) & ~(size_t)31);
+  double* dC = dB + ((nb + 31) & ~(size_t)31);
+  const int64_t ldA = m, ldB = k > 0 ? k : 1, ldC = m;
+  const bool read_c = beta != 0.0 && num_steps > 0;
+  // copy-in: after this slot's previous call has returned its C (the slot's
+  // buffers are free again); a call that reads C also waits for the other
+  // slot's copy-out, which may write the same host C
+  if (sl.used) FMM_CUDA_TRY(cudaStreamWaitEvent(h->h2d, sl.free, 0), "cudaStreamWaitEvent");
+  if (read_c && other.used) FMM_CUDA_TRY(cudaStreamWaitEvent(h->h2d, other.free, 0), "cudaStreamWaitEvent");
+  if (na)
+    FMM_CUDA_TRY(cudaMemcpy2DAsync(dA, ldA * sizeof(double), A, lda * sizeof(double), m * sizeof(double), k,
+                                   cudaMemcpyHostToDevice, h->h2d),
+                 "copy A to device");
+  if (nb)
+    FMM_CUDA_TRY(cudaMemcpy2DAsync(dB, ldB * sizeof(double), B, ldb * sizeof(double), k * sizeof(double), n,
+                                   cudaMemcpyHostToDevice, h->h2d),
+                 "copy B to device");
+  if (read_c)
+    FMM_CUDA_TRY(cudaMemcpy2DAsync(dC, ldC * sizeof(double), C, ldc * sizeof(double), m * sizeof(double), n,
+                                   cudaMemcpyHostToDevice, h->h2d),
+                 "copy C to device");
+  FMM_CUDA_TRY(cudaEventRecord(sl.in_ready, h->h2d), "cudaEventRecord");
+  FMM_CUDA_TRY(cudaStreamWaitEvent(h->stream, sl.in_ready, 0), "cudaStreamWaitEvent");
+  s = fmm_fast_matmul(h, alg, dA, ldA, dB, ldB, dC, ldC, m, k, n, num_steps, x, alpha, beta, opts);
+  if (s != FMM_OK) return s;
+  FMM_CUDA_TRY(cudaEventRecord(sl.out_ready, h->stream), "cudaEventRecord");
+  FMM_CUDA_TRY(cudaStreamWaitEvent(h->d2h, sl.out_ready, 0), "cudaStreamWaitEvent");
+  FMM_CUDA_TRY(cudaMemcpy2DAsync(C, ldc * sizeof(double), dC, ldC * sizeof(double), m * sizeof(double), n,
+                                 cudaMemcpyDeviceToHost, h->d2h),
+               "copy C to host");
+  FMM_CUDA_TRY(cudaEventRecord(sl.free, h->d2h), "cudaEventRecord");
+  sl.used = true;
+  h->next_slot ^= 1;
+  return FMM_OK;
+}
+
+fmm_status fmm_host_sync(fmm_handle h) {
+  if (!h) return fail(FMM_ERR_INVALID_ARGUMENT, "null handle");
+  DeviceGuard g(h->device);
+  if (h->d2h) FMM_CUDA_TRY(cudaStreamSynchronize(h->d2h), "cudaStreamSynchronize(copy-out)");
+  h->slots[0].used = h->slots[1].used = false;
+  return check_device_errors(h);
 }
 
 fmm_status fmm_dgemm(fmm_handle h, const double* A, int64_t lda, const double* B, int64_t ldb, double* C,

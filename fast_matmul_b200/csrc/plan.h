@@ -127,8 +127,11 @@ void build_batch_program(const BatchItem* items, int count, void* ws, Program* o
 // d_desc (which must hold prog.desc.size() bytes), then the launches in order.
 // Adds the number of kernels launched to *launches (may be null).
 // When prof is non-null every launch is bracketed by CUDA events.  d_err
-// (device int) collects the error codes of split launches.
+// (device int) collects the error codes of split launches.  desc_copied
+// (may be null) is recorded right after the descriptor copy: from then on
+// h_desc may be rewritten.
 cudaError_t run_program(const Program& prog, const void* h_desc, void* d_desc, int num_sms, cudaStream_t stream,
-                        int64_t* launches, Profiler* prof = nullptr, int* d_err = nullptr);
+                        int64_t* launches, Profiler* prof = nullptr, int* d_err = nullptr,
+                        cudaEvent_t desc_copied = nullptr);
 
 }  // namespace fmm

@@ -107,6 +107,19 @@ fmm_status fmm_handle_create(fmm_handle* out, int device);
 fmm_status fmm_handle_destroy(fmm_handle h);
 /* Stream for all work of the handle (a cudaStream_t; NULL = legacy default). */
 fmm_status fmm_set_stream(fmm_handle h, void* stream);
+/* Frees the handle's grow-on-demand device buffers (the S/T/M workspace and
+ * the staging of the host-pointer and FP32 entry points) once the work
+ * queued on its stream is done; the next call allocates again.  The
+ * reference's MemoryManager frees its pools when the multiply ends
+ * (util/MemoryManager.hpp:26-42); a handle keeps them across calls until
+ * this call or fmm_handle_destroy. */
+fmm_status fmm_release_workspace(fmm_handle h);
+/* Test support, no counterpart in the reference (which has no device
+ * workspace): grows the handle's workspace to at least `bytes` and fills all
+ * of it with the byte `pattern` (0xFF makes every double a NaN), then
+ * synchronises.  A later call that read a temporary before writing it would
+ * carry the pattern into C. */
+fmm_status fmm_debug_fill_workspace(fmm_handle h, size_t bytes, int pattern);
 /* Upper bound on the workspace the handle may allocate (0 = 60% of the
  * device memory that is free when the handle is created). */
 fmm_status fmm_set_workspace_limit(fmm_handle h, size_t bytes);
@@ -141,6 +154,25 @@ fmm_status fmm_fast_matmul(fmm_handle h, int alg, const double* A, int64_t lda, 
 fmm_status fmm_fast_matmul_host(fmm_handle h, int alg, const double* A, int64_t lda, const double* B, int64_t ldb,
                                 double* C, int64_t ldc, int64_t m, int64_t k, int64_t n, int num_steps, double x,
                                 double alpha, double beta, const fmm_options* opts, double* elapsed_ms);
+/* Pipelined form of fmm_fast_matmul_host, no counterpart in the reference
+ * (whose FastMatmul returns when C is done): queues the copy of A, B (and C
+ * when it is read) to the device, the product, and the copy of C back to
+ * the host, and returns without waiting.  Two calls may be in flight per
+ * handle; each uses one of two device staging slots in turn, so the next
+ * call's operands travel to the device and the previous call's C travels
+ * back while this call's product runs.  A third call waits, on the device,
+ * for the slot's earlier C to have left.  Every host buffer of a queued call
+ * must stay valid and unchanged until fmm_host_sync returns, and no queued
+ * call may read host memory that another queued call writes (a call that
+ * reads C, beta != 0, is ordered after the other slot's copy of C).  Pinned
+ * host memory lets the copies overlap the products; pageable memory works
+ * but serialises them.  fmm_fast_matmul_host first waits for queued calls. */
+fmm_status fmm_fast_matmul_host_async(fmm_handle h, int alg, const double* A, int64_t lda, const double* B,
+                                      int64_t ldb, double* C, int64_t ldc, int64_t m, int64_t k, int64_t n,
+                                      int num_steps, double x, double alpha, double beta, const fmm_options* opts);
+/* Waits until every call queued by fmm_fast_matmul_host_async has put its C
+ * on the host; returns the first device-side error of those calls. */
+fmm_status fmm_host_sync(fmm_handle h);
 
 /* Device workspace the call above needs (bytes), for the schedule chosen. */
 fmm_status fmm_workspace_query(fmm_handle h, int alg, int64_t m, int64_t k, int64_t n, int num_steps,
