@@ -77,6 +77,8 @@ def parse_args(argv=None):
                     help="square sizes of the precision workload")
     ap.add_argument("--batch-precision", default="fp64", choices=["fp64", "split_bf16", "split_int8"])
     ap.add_argument("--batch-count", type=int, default=4096)
+    ap.add_argument("--batch-tile", default="auto", choices=["auto", "large", "small"],
+                    help="FP64 GEMM tile configuration of the batch items (auto: the autotuned one per bucket)")
     ap.add_argument("--serve-requests", type=int, default=300)
     ap.add_argument("--serve-slots", type=int, default=6)
     ap.add_argument("--sweep", action="store_true",
@@ -684,15 +686,18 @@ def batch_record(a, precision):
         probs.append({"A": fmm.random_matrix(int(m), int(k), 7000 + i, 1, -1.0, 1.0, handle=h),
                       "B": fmm.random_matrix(int(k), int(n), 7000 + i, 2, -1.0, 1.0, handle=h),
                       "C": fmm.colmajor_empty(int(m), int(n)), "alg": fmm.AUTO,
-                      "precision": precision, "split_slices": 6})
+                      "precision": precision, "split_slices": 6, "gemm_tile": a.batch_tile})
     flops = float(sum(2.0 * m * n * k for m, k, n in dims))
     t0 = time.perf_counter()
     fmm.autotune([tuple(int(v) for v in d) for d in dims], max_steps=1, handle=h)
     tune_s = time.perf_counter() - t0
     choices = {}
+    tiles = {}
     for m, k, n in dims:
         c = fmm.autotune_choice(int(m), int(k), int(n), handle=h)
         choices[c] = choices.get(c, 0) + 1
+        t = a.batch_tile if a.batch_tile != "auto" else fmm.autotune_tile(int(m), int(k), int(n), handle=h)
+        tiles[t] = tiles.get(t, 0) + 1
     plan = fmm.Plan.for_batch(probs, handle=h)
 
     def timed(fn, reps):
@@ -742,7 +747,8 @@ def batch_record(a, precision):
                                                   "split_int8": "split-INT8 (6 slices)"}[precision]),
                    "total_gflop": flops / 1e9, "autotune_seconds": tune_s,
                    "choices": {("classical" if k[0] == fmm.CLASSICAL else "%s/%d" % (fmm.algorithm_names()[k[0]], k[1])): v
-                               for k, v in choices.items()}},
+                               for k, v in choices.items()},
+                   "gemm_tiles": tiles, "batch_tile": a.batch_tile},
         "one_at_a_time": {"value": flops / (ms_single * 1e-3) / 1e12, "ms": ms_single,
                           "speedup_of_batched": ms_single / ms},
         "clocks": clk,

@@ -20,6 +20,7 @@ from .api import (  # noqa: F401
     autotune_choice,
     autotune_load,
     autotune_table,
+    autotune_tile,
     fast_matmul_batched,
     algorithm_index,
     algorithm_info,

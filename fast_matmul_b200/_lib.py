@@ -33,6 +33,7 @@ STATUS_NAMES = {
 
 SCHEDULES = {"auto": 0, "dfs": 1, "bfs": 2, "hybrid": 3}
 PRECISIONS = {"fp64": 0, "split_bf16": 1, "split_int8": 2}
+GEMM_TILES = {"auto": 0, "large": 1, "small": 2}
 
 
 class FmmError(RuntimeError):
@@ -48,6 +49,7 @@ class Options(ctypes.Structure):
         ("split_slices", ctypes.c_int),
         ("dfs_levels", ctypes.c_int),
         ("workspace_limit", ctypes.c_size_t),
+        ("gemm_tile", ctypes.c_int),
     ]
 
 
@@ -79,6 +81,7 @@ class BatchItem(ctypes.Structure):
         ("m", ctypes.c_int64), ("k", ctypes.c_int64), ("n", ctypes.c_int64),
         ("x", ctypes.c_double), ("alpha", ctypes.c_double), ("beta", ctypes.c_double),
         ("precision", ctypes.c_int), ("split_slices", ctypes.c_int),
+        ("gemm_tile", ctypes.c_int),
     ]
 
 
@@ -213,6 +216,8 @@ SIGNATURES = {
                                                 ctypes.c_int64, ctypes.c_int64, ctypes.c_int, ctypes.c_double,
                                                 ctypes.c_double, ctypes.c_double, ctypes.c_void_p]),
     "fmm_fast_matmul_batched": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(BatchItem), ctypes.c_int]),
+    "fmm_autotune_tile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
+                                          ctypes.POINTER(ctypes.c_int)]),
     "fmm_autotune_choice": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
                                             ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     "fmm_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64), ctypes.c_int,

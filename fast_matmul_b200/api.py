@@ -175,7 +175,8 @@ def _mat(t, rows: int, cols: int, name: str, dtype=None) -> Tuple[int, int]:
     return t.data_ptr(), max(ld, rows, 1)
 
 
-def _options(schedule="auto", dfs_levels=-1, workspace_limit=0, precision="fp64", split_slices=0) -> Options:
+def _options(schedule="auto", dfs_levels=-1, workspace_limit=0, precision="fp64", split_slices=0,
+             gemm_tile="auto") -> Options:
     o = Options()
     lib().fmm_options_init(ctypes.byref(o))
     o.schedule = _lib.SCHEDULES[schedule]
@@ -183,17 +184,21 @@ def _options(schedule="auto", dfs_levels=-1, workspace_limit=0, precision="fp64"
     o.split_slices = split_slices
     o.dfs_levels = dfs_levels
     o.workspace_limit = workspace_limit
+    o.gemm_tile = _lib.GEMM_TILES[gemm_tile]
     return o
 
 
 def fast_matmul(alg, A, B, C, num_steps: int, x: float = 1e-8, alpha: float = 1.0, beta: float = 0.0,
                 schedule: str = "auto", dfs_levels: int = -1, workspace_limit: int = 0,
-                precision: Optional[str] = None, split_slices: int = 0, handle: Optional[Handle] = None) -> None:
+                precision: Optional[str] = None, split_slices: int = 0, handle: Optional[Handle] = None,
+                gemm_tile: str = "auto") -> None:
     """C := alpha * A * B + beta * C with `num_steps` levels of algorithm
     `alg` -- <alg>::FastMatmul(A, B, C, num_steps, x, alpha, beta).
     precision "split_bf16" runs the leaf products on the BF16 tensor cores
     over `split_slices` slices (0 = 5), "split_int8" on the INT8 tensor cores
-    over 7-bit slices (0 = 6).  Queued on torch's current stream.
+    over 7-bit slices (0 = 6).  gemm_tile ("auto", "large" 128 x 64, "small"
+    64 x 64) is the FP64 GEMM's tile configuration (speed only; the result
+    does not depend on it).  Queued on torch's current stream.
 
     float32 operands (all three) select FastMatmul<float>
     (fmm_fast_matmul_f32): computed on FP64 copies and rounded to FP32 once;
@@ -219,7 +224,7 @@ def fast_matmul(alg, A, B, C, num_steps: int, x: float = 1e-8, alpha: float = 1.
     pa, lda = _mat(A, m, k, "A")
     pb, ldb = _mat(B, k, n, "B")
     pc, ldc = _mat(C, m, n, "C")
-    o = _options(schedule, dfs_levels, workspace_limit, precision or "fp64", split_slices)
+    o = _options(schedule, dfs_levels, workspace_limit, precision or "fp64", split_slices, gemm_tile)
     check(lib().fmm_fast_matmul(h.ptr, idx, pa, lda, pb, ldb, pc, ldc, m, k, n, num_steps, x, alpha, beta,
                                 ctypes.byref(o)))
 
@@ -432,7 +437,8 @@ AUTO = _lib.FMM_ALG_AUTO
 
 def _batch_items(problems):
     """problems: iterable of dicts with A, B, C (column-major CUDA tensors) and
-    optional alg (name, index, AUTO or CLASSICAL), num_steps, x, alpha, beta."""
+    optional alg (name, index, AUTO or CLASSICAL), num_steps, x, alpha, beta,
+    precision, split_slices, gemm_tile ("auto", "large", "small")."""
     problems = list(problems)
     arr = (_lib.BatchItem * len(problems))()
     for i, p in enumerate(problems):
@@ -455,6 +461,7 @@ def _batch_items(problems):
         it.beta = float(p.get("beta", 0.0))
         it.precision = _lib.PRECISIONS[p.get("precision", "fp64")]
         it.split_slices = int(p.get("split_slices", 0))
+        it.gemm_tile = _lib.GEMM_TILES[p.get("gemm_tile", "auto")]
     return arr
 
 
@@ -483,6 +490,15 @@ def autotune_choice(m: int, k: int, n: int, handle: Optional[Handle] = None):
     s = ctypes.c_int()
     check(lib().fmm_autotune_choice(h.ptr, m, k, n, ctypes.byref(a), ctypes.byref(s)))
     return a.value, s.value
+
+
+def autotune_tile(m: int, k: int, n: int, handle: Optional[Handle] = None) -> str:
+    """The FP64 GEMM tile configuration tuned for the shape's bucket
+    ("large", "small", or "auto" where the bucket was not measured)."""
+    h = handle or default_handle()
+    t = ctypes.c_int()
+    check(lib().fmm_autotune_tile(h.ptr, m, k, n, ctypes.byref(t)))
+    return {v: name for name, v in _lib.GEMM_TILES.items()}[t.value]
 
 
 def autotune_table(handle: Optional[Handle] = None) -> str:

@@ -65,8 +65,12 @@ struct fmm_handle_s {
   fmm::Program prog;
   bool profiling = false;
   fmm::Profiler prof;
-  // autotuner: shape bucket (ceil log2 of m, k, n) -> (algorithm or -2 for classical, steps)
-  std::map<std::tuple<int, int, int>, std::pair<int, int>> tuned;
+  // autotuner: shape bucket (ceil log2 of m, k, n) -> algorithm (or FMM_ALG_CLASSICAL), steps and
+  // the FP64 GEMM tile configuration measured fastest
+  struct Tuned {
+    int alg, steps, tile;
+  };
+  std::map<std::tuple<int, int, int>, Tuned> tuned;
 };
 
 namespace fmm {
@@ -96,6 +100,9 @@ fmm_status ensure_device_buffer(fmm_handle h, void** buf, size_t* cap, size_t ne
 fmm_status stage_descriptors(fmm_handle h, const fmm::Program& prog);
 fmm_status run_staged(fmm_handle h, const fmm::Program& prog);
 fmm_status check_alg(int alg);
+// fmm_dgemm with a given tile configuration (fmm_gemm_tile; AUTO: per problem).
+fmm_status dgemm_tiled(fmm_handle h, const double* A, int64_t lda, const double* B, int64_t ldb, double* C,
+                       int64_t ldc, int64_t m, int64_t k, int64_t n, double alpha, double beta, int tile);
 fmm_status check_dims(int64_t m, int64_t k, int64_t n, int64_t lda, int64_t ldb, int64_t ldc);
 void resolve_options(const fmm_options* opts, fmm_options* out);
 // Slices of the leaf products for a precision (0 for FP64).

@@ -47,11 +47,13 @@ void rule_choice(int64_t m, int64_t k, int64_t n, int* alg, int* steps) {
   }
 }
 
-void choice_for(fmm_handle h, int64_t m, int64_t k, int64_t n, int* alg, int* steps) {
+void choice_for(fmm_handle h, int64_t m, int64_t k, int64_t n, int* alg, int* steps, int* tile = nullptr) {
   auto it = h->tuned.find(bucket_of(m, k, n));
+  if (tile) *tile = FMM_GEMM_TILE_AUTO;
   if (it != h->tuned.end()) {
-    *alg = it->second.first;
-    *steps = it->second.second;
+    *alg = it->second.alg;
+    *steps = it->second.steps;
+    if (tile) *tile = it->second.tile;
     return;
   }
   rule_choice(m, k, n, alg, steps);
@@ -73,8 +75,11 @@ fmm_status resolve_items(fmm_handle h, const fmm_batch_item* items, int count, s
     if (!it.C || (it.k > 0 && (!it.A || !it.B)))
       return fail(FMM_ERR_INVALID_ARGUMENT, "batch item " + std::to_string(i) + ": null matrix pointer");
     fmm::BatchItem b{};
-    int alg = it.alg, steps = it.num_steps;
-    if (alg == FMM_ALG_AUTO) choice_for(h, it.m, it.k, it.n, &alg, &steps);
+    int alg = it.alg, steps = it.num_steps, tuned_tile = FMM_GEMM_TILE_AUTO;
+    if (alg == FMM_ALG_AUTO) choice_for(h, it.m, it.k, it.n, &alg, &steps, &tuned_tile);
+    if (it.gemm_tile < FMM_GEMM_TILE_AUTO || it.gemm_tile > FMM_GEMM_TILE_SMALL)
+      return fail(FMM_ERR_INVALID_ARGUMENT, "batch item " + std::to_string(i) + ": unknown gemm_tile");
+    b.gemm_tile = it.gemm_tile != FMM_GEMM_TILE_AUTO ? it.gemm_tile : tuned_tile;
     if (alg == FMM_ALG_CLASSICAL) {
       b.classical = true;
       b.alg = 0;
@@ -217,6 +222,14 @@ fmm_status fmm_autotune_choice(fmm_handle h, int64_t m, int64_t k, int64_t n, in
   return FMM_OK;
 }
 
+fmm_status fmm_autotune_tile(fmm_handle h, int64_t m, int64_t k, int64_t n, int* tile) {
+  if (!h || !tile) return fail(FMM_ERR_INVALID_ARGUMENT, "null argument");
+  if (m <= 0 || k <= 0 || n <= 0) return fail(FMM_ERR_INVALID_ARGUMENT, "dimensions must be positive");
+  int alg = 0, steps = 0;
+  choice_for(h, m, k, n, &alg, &steps, tile);
+  return FMM_OK;
+}
+
 fmm_status fmm_autotune(fmm_handle h, const int64_t* shapes, int count, const int* candidates, int n_candidates,
                         int max_steps) {
   if (!h || (count > 0 && !shapes)) return fail(FMM_ERR_INVALID_ARGUMENT, "null argument");
@@ -270,8 +283,16 @@ fmm_status fmm_autotune(fmm_handle h, const int64_t* shapes, int count, const in
       cudaEventElapsedTime(&ms, e0, e1);
       return ms / 3.f;
     };
-    int best_alg = FMM_ALG_CLASSICAL, best_steps = 0;
-    float best = time_it([&] { return fmm_dgemm(h, A, m, B, k, C, m, m, k, n, 1.0, 0.0); });
+    // every candidate with each tile configuration of the FP64 GEMM
+    int best_alg = FMM_ALG_CLASSICAL, best_steps = 0, best_tile = FMM_GEMM_TILE_LARGE;
+    float best = -1.f;
+    for (int tile : {FMM_GEMM_TILE_LARGE, FMM_GEMM_TILE_SMALL}) {
+      const float ms = time_it([&] { return dgemm_tiled(h, A, m, B, k, C, m, m, k, n, 1.0, 0.0, tile); });
+      if (ms > 0.f && (best < 0.f || ms < best)) {
+        best = ms;
+        best_tile = tile;
+      }
+    }
     for (int alg : cands) {
       const fmm_alg_table& t = fmm_algorithms[alg];
       int64_t mm = m, kk = k, nn = n;
@@ -280,16 +301,22 @@ fmm_status fmm_autotune(fmm_handle h, const int64_t* shapes, int count, const in
         kk /= t.k0;
         nn /= t.n0;
         if (mm < 64 || kk < 64 || nn < 64) break;
-        const float ms = time_it(
-            [&] { return fmm_fast_matmul(h, alg, A, m, B, k, C, m, m, k, n, steps, 1e-8, 1.0, 0.0, nullptr); });
-        if (ms > 0.f && (best < 0.f || ms < best)) {
-          best = ms;
-          best_alg = alg;
-          best_steps = steps;
+        for (int tile : {FMM_GEMM_TILE_LARGE, FMM_GEMM_TILE_SMALL}) {
+          fmm_options o;
+          fmm_options_init(&o);
+          o.gemm_tile = tile;
+          const float ms = time_it(
+              [&] { return fmm_fast_matmul(h, alg, A, m, B, k, C, m, m, k, n, steps, 1e-8, 1.0, 0.0, &o); });
+          if (ms > 0.f && (best < 0.f || ms < best)) {
+            best = ms;
+            best_alg = alg;
+            best_steps = steps;
+            best_tile = tile;
+          }
         }
       }
     }
-    h->tuned[kv.first] = std::make_pair(best_alg, best_steps);
+    h->tuned[kv.first] = fmm_handle_s::Tuned{best_alg, best_steps, best_tile};
     cudaFree(A);
     cudaFree(B);
     cudaFree(C);
@@ -304,7 +331,7 @@ fmm_status fmm_autotune_export(fmm_handle h, char* buf, size_t cap, size_t* len)
   std::ostringstream os;
   for (const auto& kv : h->tuned)
     os << std::get<0>(kv.first) << ' ' << std::get<1>(kv.first) << ' ' << std::get<2>(kv.first) << ' '
-       << kv.second.first << ' ' << kv.second.second << '\n';
+       << kv.second.alg << ' ' << kv.second.steps << ' ' << kv.second.tile << '\n';
   const std::string text = os.str();
   if (len) *len = text.size() + 1;
   if (buf) {
@@ -316,12 +343,20 @@ fmm_status fmm_autotune_export(fmm_handle h, char* buf, size_t cap, size_t* len)
 
 fmm_status fmm_autotune_import(fmm_handle h, const char* text) {
   if (!h || !text) return fail(FMM_ERR_INVALID_ARGUMENT, "null argument");
+  // one bucket per line: "mb kb nb alg steps [tile]" (tables without the
+  // tile column load with the tile chosen per problem)
   std::istringstream is(text);
-  int mb, kb, nb, alg, steps;
-  while (is >> mb >> kb >> nb >> alg >> steps) {
+  std::string line;
+  while (std::getline(is, line)) {
+    std::istringstream ls(line);
+    int mb, kb, nb, alg, steps, tile = FMM_GEMM_TILE_AUTO;
+    if (!(ls >> mb >> kb >> nb >> alg >> steps)) continue;
+    if (!(ls >> tile)) tile = FMM_GEMM_TILE_AUTO;
     if (alg != FMM_ALG_CLASSICAL && (alg < 0 || alg >= FMM_NUM_ALGORITHMS))
       return fail(FMM_ERR_UNKNOWN_ALGORITHM, "tuning table names an unknown algorithm");
-    h->tuned[std::make_tuple(mb, kb, nb)] = std::make_pair(alg, steps);
+    if (tile < FMM_GEMM_TILE_AUTO || tile > FMM_GEMM_TILE_SMALL)
+      return fail(FMM_ERR_INVALID_ARGUMENT, "tuning table names an unknown gemm tile");
+    h->tuned[std::make_tuple(mb, kb, nb)] = fmm_handle_s::Tuned{alg, steps, tile};
   }
   return FMM_OK;
 }
@@ -353,7 +388,8 @@ fmm_status fmm_plan_create(fmm_handle h, int alg, const double* A, int64_t lda, 
     return fail(FMM_ERR_OUT_OF_MEMORY, "cannot allocate the plan's workspace");
   }
   fmm::build_program(alg, m, k, n, num_steps, x, alpha, beta, d, fmm::Operand{const_cast<double*>(A), lda},
-                     fmm::Operand{const_cast<double*>(B), ldb}, fmm::Operand{C, ldc}, p->ws, &p->prog, slices);
+                     fmm::Operand{const_cast<double*>(B), ldb}, fmm::Operand{C, ldc}, p->ws, &p->prog, slices,
+                     o.gemm_tile);
   if ((s = plan_capture(p)) != FMM_OK) {
     plan_free(p);
     return s;

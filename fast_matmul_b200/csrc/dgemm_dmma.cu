@@ -16,6 +16,19 @@
 // about 29 (both measured with a register-only probe).  Shared-memory rows
 // are padded so that every fragment load is conflict-free.  CTAs loop over
 // the tiles of all problems.
+//
+// Summation order: the FP64 MMA forms its 16 products as a chain of
+// round-to-nearest FMAs in k order (measured on B200 with inputs whose
+// result tells the orders apart), and consecutive k16 MMAs chain through
+// the accumulator registers.  A dot product of length k summed that way in
+// one chain has a rounding error that grows like sqrt(k) ulps of its final
+// value.  So the k loop is cut into blocks of kFlushSlices slices (256 k): a
+// block is chained in registers as above, then added with one FP64 add into
+// a per-thread running sum kept in tensor memory (which this kernel does not
+// otherwise use: each thread owns one TMEM lane, 32 columns per 16 doubles),
+// and the registers restart from zero.  The error of this blocked sum grows
+// like b / sqrt(k) + sqrt(k / b) ulps for blocks of b terms (8x less than one
+// chain at k = 4096, 13x at k = 16384) for one FP64 add per 256 FMAs.
 
 #include <cuda_runtime.h>
 
@@ -23,9 +36,22 @@
 #include <mutex>
 
 #include "fmm_internal.h"
+#include "sm100_primitives.cuh"
 
 namespace fmm {
 namespace {
+
+using sm100::tc_fence_after;
+using sm100::tc_fence_before;
+using sm100::tmem_alloc_cta;
+using sm100::tmem_dealloc_cta;
+using sm100::tmem_ld_32x32b_x8;
+using sm100::tmem_ld_wait;
+using sm100::tmem_st_32x32b_x8;
+using sm100::tmem_st_wait;
+
+// k-slices per block of the blocked sum (BK = 32: 256 k per block).
+constexpr int kFlushSlices = 8;
 
 // 64-bit shared loads are served per half-warp: a fragment load is
 // conflict-free when the 16 lanes of each half (4 row groups x 4 k lanes)
@@ -66,6 +92,10 @@ struct GemmCfg {
 // B200 (FP64, 8192^3 and grouped 1024x4096x1024 / 2048^3): 33.7-33.9
 // TFLOP/s against 31-32 for one 8-warp CTA of 128 x 128 and 36 for cuBLAS.
 using DefaultGemmCfg = GemmCfg<32, 2, kGemmBN, 2, kGemmBM, 64>;
+// 64 x 64 tiles, 4 warps of 32 x 32, three CTAs per SM: less padding on
+// problems whose rows are just above a multiple of 64, more CTAs to hide the
+// latency of short k loops.
+using SmallGemmCfg = GemmCfg<32, 2, kGemmBN, 3, kGemmBMSmall, 32>;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -195,7 +225,12 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
   constexpr int A_STAGE = Cfg::A_STAGE;
   constexpr int B_STAGE = Cfg::B_STAGE;
   constexpr int B_LD = Cfg::B_LD;
+  constexpr int ACC = MT * 16;         // accumulator doubles per thread
+  constexpr uint32_t TMEM_COLS = 2 * ACC;  // 32-bit TMEM columns of this thread's running sum
+  static_assert(THREADS == 128, "four warps: warp w owns TMEM lanes 32 w .. 32 w + 31");
+  static_assert(TMEM_COLS >= 32 && (TMEM_COLS & (TMEM_COLS - 1)) == 0, "TMEM allocations are powers of two");
   extern __shared__ __align__(128) double smem[];
+  __shared__ uint32_t tmem_slot;
   double* sA_all = smem;
   double* sB_all = smem + STAGES * A_STAGE;
 
@@ -206,6 +241,13 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
   const int tig = lane & 3;
   const int wm = warp % Cfg::WARPS_M;  // warps along M (WTM rows each)
   const int wn = warp / Cfg::WARPS_M;  // warps along N (32 columns each)
+
+  if (warp == 0) tmem_alloc_cta(&tmem_slot, TMEM_COLS);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  // this thread's lane: 32 (warp) + lane; its doubles at columns 2 i, 2 i + 1
+  const uint32_t tsum = tmem_slot + ((uint32_t)(32 * warp) << 16);
 
   for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
     // problem owning this tile: last p with tile_begin <= tile
@@ -262,6 +304,34 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
       for (int b = 0; b < 4; ++b)
 #pragma unroll
         for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.0;
+    // block sums of this tile so far live in tensor memory from the first
+    // flush on: sum = sum + acc (or sum = acc the first time), acc = 0
+    bool have_sum = false;
+    auto flush = [&]() {
+#pragma unroll
+      for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+          const uint32_t col = tsum + (uint32_t)(8 * (mt * 4 + nt));
+          uint32_t w[8];
+          if (have_sum) {
+            tmem_ld_32x32b_x8(col, w);
+            tmem_ld_wait();
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+              acc[mt][nt][q] = __dadd_rn(__hiloint2double((int)w[2 * q + 1], (int)w[2 * q]), acc[mt][nt][q]);
+          }
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            w[2 * q] = (uint32_t)__double2loint(acc[mt][nt][q]);
+            w[2 * q + 1] = (uint32_t)__double2hiint(acc[mt][nt][q]);
+            acc[mt][nt][q] = 0.0;
+          }
+          tmem_st_32x32b_x8(col, w);
+        }
+      tmem_st_wait();  // a later load of these columns sees the stores
+      have_sum = true;
+    };
 
 #pragma unroll
     for (int s = 0; s < STAGES - 1; ++s) {
@@ -302,13 +372,44 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
           for (int nt = 0; nt < 4; ++nt) dmma_16x8x16(acc[mt][nt], af, bf[nt]);
         }
       }
+      if ((kt + 1) % kFlushSlices == 0 && kt + 1 < ktiles) flush();
     }
     cp_async_wait<0>();
     __syncthreads();  // shared buffers are refilled by the next tile
+    if (have_sum) {  // the last block: acc = sum + acc
+#pragma unroll
+      for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+          uint32_t w[8];
+          tmem_ld_32x32b_x8(tsum + (uint32_t)(8 * (mt * 4 + nt)), w);
+          tmem_ld_wait();
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            acc[mt][nt][q] = __dadd_rn(__hiloint2double((int)w[2 * q + 1], (int)w[2 * q]), acc[mt][nt][q]);
+        }
+    }
 
-    // epilogue: C = alpha * acc + beta * C
+    // epilogue: C = alpha * acc + beta * C.  With beta != 0 the 16 C values
+    // of a row fragment are loaded before any is used, so their memory
+    // latencies overlap (fringe products with k = 1 are nothing but this
+    // read-modify-write of C).
 #pragma unroll
     for (int mt = 0; mt < MT; ++mt) {
+      double cin[2][4][2];
+      if (beta != 0.0) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int r = row0 + wm * WTM + mt * 16 + g + h * 8;
+#pragma unroll
+          for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+              const int cidx = col0 + wn * 32 + nt * 8 + tig * 2 + q;
+              cin[h][nt][q] = (r < M && cidx < N) ? Cp[r + (int64_t)cidx * ldc] : 0.0;
+            }
+        }
+      }
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const int r = row0 + wm * WTM + mt * 16 + g + h * 8;
@@ -321,7 +422,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
             if (cidx < N) {
               double* cp = Cp + r + (int64_t)cidx * ldc;
               double v = alpha * acc[mt][nt][h * 2 + q];
-              if (beta != 0.0) v += beta * *cp;
+              if (beta != 0.0) v += beta * cin[h][nt][q];
               *cp = v;
             }
           }
@@ -329,37 +430,52 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
       }
     }
   }
+  // every tensor-memory access of the CTA is done before the columns go
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0) tmem_dealloc_cta(tmem_slot, TMEM_COLS);
 }
 
 }  // namespace
 
-template <class Cfg>
-cudaError_t gemm_launch_cfg(const GemmDesc* d_descs, int n, int64_t total_tiles, int num_sms, cudaStream_t stream) {
-  if (total_tiles <= 0 || n <= 0) return cudaSuccess;
-  // the shared-memory opt-in is per device; set it once so launches can be
-  // captured into CUDA graphs without other API calls in between
-  // (handles on several host threads may launch concurrently)
+// The shared-memory opt-in is per device; both configurations get it on the
+// first launch of either, so later launches can be captured into CUDA graphs
+// without other API calls in between (handles on several host threads may
+// launch concurrently).
+cudaError_t gemm_opt_in() {
   static bool opted_in[64] = {};
   static std::mutex mu;
   int dev = 0;
   cudaError_t err = cudaGetDevice(&dev);
   if (err != cudaSuccess) return err;
-  {
-    std::lock_guard<std::mutex> lock(mu);
-    if (dev < 0 || dev >= 64 || !opted_in[dev]) {
-      err = cudaFuncSetAttribute(grouped_dgemm_kernel<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)Cfg::SMEM_BYTES);
-      if (err != cudaSuccess) return err;
-      if (dev >= 0 && dev < 64) opted_in[dev] = true;
-    }
-  }
+  std::lock_guard<std::mutex> lock(mu);
+  if (dev >= 0 && dev < 64 && opted_in[dev]) return cudaSuccess;
+  err = cudaFuncSetAttribute(grouped_dgemm_kernel<DefaultGemmCfg>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)DefaultGemmCfg::SMEM_BYTES);
+  if (err == cudaSuccess)
+    err = cudaFuncSetAttribute(grouped_dgemm_kernel<SmallGemmCfg>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)SmallGemmCfg::SMEM_BYTES);
+  if (err == cudaSuccess && dev >= 0 && dev < 64) opted_in[dev] = true;
+  return err;
+}
+
+template <class Cfg>
+cudaError_t gemm_launch_cfg(const GemmDesc* d_descs, int n, int64_t total_tiles, int num_sms, cudaStream_t stream) {
+  if (total_tiles <= 0 || n <= 0) return cudaSuccess;
+  cudaError_t err = gemm_opt_in();
+  if (err != cudaSuccess) return err;
+  // one CTA per resident slot (Cfg::MINB per SM), each holding 2 * MT * 16
+  // TMEM columns: at most 256 of an SM's 512 (3 x 64 for the small tiles)
   const int64_t slots = (int64_t)num_sms * Cfg::MINB;
   const int64_t grid = total_tiles < slots ? total_tiles : slots;
   grouped_dgemm_kernel<Cfg><<<(unsigned)grid, Cfg::THREADS, Cfg::SMEM_BYTES, stream>>>(d_descs, n, (int)total_tiles);
   return cudaGetLastError();
 }
 
-cudaError_t gemm_launch(const GemmDesc* d_descs, int n, int64_t total_tiles, int num_sms, cudaStream_t stream) {
+cudaError_t gemm_launch(const GemmDesc* d_descs, int n, int64_t total_tiles, int num_sms, cudaStream_t stream,
+                        int tile) {
+  if (tile == kGemmTileSmall) return gemm_launch_cfg<SmallGemmCfg>(d_descs, n, total_tiles, num_sms, stream);
   return gemm_launch_cfg<DefaultGemmCfg>(d_descs, n, total_tiles, num_sms, stream);
 }
 

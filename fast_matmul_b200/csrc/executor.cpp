@@ -54,7 +54,7 @@ cudaError_t run_program(const Program& prog, const void* h_desc, void* d_desc, i
       }
       case OpKind::kGemm:
         e = gemm_launch(reinterpret_cast<const GemmDesc*>(base + op.desc_off), op.n, op.total_tiles, num_sms,
-                        stream);
+                        stream, op.gemm_tile);
         break;
       case OpKind::kSplitGemm: {
         int64_t n_launched = 0;

@@ -211,6 +211,7 @@ void fmm_options_init(fmm_options* opts) {
   opts->split_slices = 0;
   opts->dfs_levels = -1;
   opts->workspace_limit = 0;
+  opts->gemm_tile = FMM_GEMM_TILE_AUTO;
 }
 
 const char* fmm_last_error(void) { return fmm::api::g_last_error.c_str(); }
@@ -398,7 +399,8 @@ fmm_status fmm_fast_matmul(fmm_handle h, int alg, const double* A, int64_t lda, 
   if ((s = ensure_device_buffer(h, &h->ws, &h->ws_cap, bytes ? bytes : 256, "workspace")) != FMM_OK) return s;
   try {
     fmm::build_program(alg, m, k, n, num_steps, x, alpha, beta, d, fmm::Operand{const_cast<double*>(A), lda},
-                       fmm::Operand{const_cast<double*>(B), ldb}, fmm::Operand{C, ldc}, h->ws, &h->prog, slices);
+                       fmm::Operand{const_cast<double*>(B), ldb}, fmm::Operand{C, ldc}, h->ws, &h->prog, slices,
+                       o.gemm_tile);
   } catch (const std::exception& ex) {
     return fail(FMM_ERR_OUT_OF_MEMORY, std::string("planning failed: ") + ex.what());
   }
@@ -540,6 +542,16 @@ fmm_status fmm_host_sync(fmm_handle h) {
 
 fmm_status fmm_dgemm(fmm_handle h, const double* A, int64_t lda, const double* B, int64_t ldb, double* C,
                      int64_t ldc, int64_t m, int64_t k, int64_t n, double alpha, double beta) {
+  return fmm::api::dgemm_tiled(h, A, lda, B, ldb, C, ldc, m, k, n, alpha, beta, FMM_GEMM_TILE_AUTO);
+}
+
+}  // extern "C"
+
+namespace fmm {
+namespace api {
+
+fmm_status dgemm_tiled(fmm_handle h, const double* A, int64_t lda, const double* B, int64_t ldb, double* C,
+                       int64_t ldc, int64_t m, int64_t k, int64_t n, double alpha, double beta, int tile_choice) {
   if (!h) return fail(FMM_ERR_INVALID_ARGUMENT, "null handle");
   fmm_status s = check_dims(m, k, n, lda, ldb, ldc);
   if (s != FMM_OK) return s;
@@ -561,19 +573,28 @@ fmm_status fmm_dgemm(fmm_handle h, const double* A, int64_t lda, const double* B
   d.k = (int)k;
   d.alpha = alpha;
   d.beta = beta;
-  const int64_t tiles = fmm::gemm_prepare(&d, 1);
+  const int tile = (tile_choice == fmm::kGemmTileLarge || tile_choice == fmm::kGemmTileSmall)
+                       ? tile_choice
+                       : fmm::gemm_tile_rule(d.m);
+  const int64_t tiles = fmm::gemm_prepare(&d, 1, fmm::kGemmBN, fmm::gemm_tile_rows(tile));
   prog.desc.resize(sizeof(d));
   std::memcpy(prog.desc.data(), &d, sizeof(d));
   fmm::Op op;
   op.kind = fmm::OpKind::kGemm;
   op.n = 1;
   op.total_tiles = tiles;
+  op.gemm_tile = tile;
   op.desc_off = 0;
   op.flops = 2.0 * (double)m * (double)n * (double)k;
   prog.ops.push_back(op);
   if ((s = stage_descriptors(h, prog)) != FMM_OK) return s;
   return run_staged(h, prog);
 }
+
+}  // namespace api
+}  // namespace fmm
+
+extern "C" {
 
 fmm_status fmm_dgemm_host(fmm_handle h, const double* A, int64_t lda, const double* B, int64_t ldb, double* C,
                           int64_t ldc, int64_t m, int64_t k, int64_t n, double alpha, double beta) {

@@ -25,14 +25,37 @@ struct GemmDesc {
   double alpha, beta;
 };
 
-constexpr int kGemmBM = 128;
-constexpr int kGemmBN = 64;   // tile columns of the launched configuration
+// Tile configurations of the grouped FP64 GEMM (values of fmm_options::gemm_tile):
+//   kGemmTileLarge  128 x 64 tiles, 4 warps of 64 x 32, 2 CTAs per SM
+//   kGemmTileSmall   64 x 64 tiles, 4 warps of 32 x 32, 3 CTAs per SM
+// Both accumulate every output element over the same k16 blocks in the same
+// order, so they give bit-identical results.  kGemmTileAuto picks one per
+// problem (gemm_tile_rule).
+constexpr int kGemmTileAuto = 0;
+constexpr int kGemmTileLarge = 1;
+constexpr int kGemmTileSmall = 2;
+constexpr int kGemmBM = 128;  // tile rows of the large configuration
+constexpr int kGemmBN = 64;   // tile columns (both configurations)
+constexpr int kGemmBMSmall = 64;
+inline int gemm_tile_rows(int tile) { return tile == kGemmTileSmall ? kGemmBMSmall : kGemmBM; }
+// Choice for one problem (a launch of several Auto problems applies the same
+// test to their padded areas in total): the small tiles where 128-row tiles
+// would pad the rows by more than 7% beyond what 64-row tiles pad (the small
+// configuration runs about 6% slower on large problems).
+inline int gemm_tile_rule(int m) {
+  const int64_t large = (int64_t)((m + kGemmBM - 1) / kGemmBM) * kGemmBM;
+  const int64_t small = (int64_t)((m + kGemmBMSmall - 1) / kGemmBMSmall) * kGemmBMSmall;
+  return (double)large > 1.07 * (double)small ? kGemmTileSmall : kGemmTileLarge;
+}
 
 // Fills tiles_m / tile_begin / flags for descs[0..n) and returns the total
 // number of tile_m x tile_n tiles.
 int64_t gemm_prepare(GemmDesc* descs, int n, int tile_n = kGemmBN, int tile_m = kGemmBM);
-// Launches the grouped GEMM over descs (device copy) with `total_tiles` tiles.
-cudaError_t gemm_launch(const GemmDesc* d_descs, int n, int64_t total_tiles, int num_sms, cudaStream_t stream);
+// Launches the grouped GEMM over descs (device copy) with `total_tiles`
+// tiles of configuration `tile` (kGemmTileLarge or kGemmTileSmall; the
+// descriptors must have been prepared with that configuration's tile).
+cudaError_t gemm_launch(const GemmDesc* d_descs, int n, int64_t total_tiles, int num_sms, cudaStream_t stream,
+                        int tile = kGemmTileLarge);
 
 // ---------------------------------------------------------------------------
 // Split-BF16 leaf products on the tensor cores (split_bf16.cu):

@@ -273,9 +273,13 @@ void emit_combine(Program* prog, int alg, int cf, int level, const std::vector<C
   prog->ops.push_back(op);
 }
 
-void emit_gemm(Program* prog, int level, std::vector<GemmDesc>& g, bool leaves) {
+// One grouped GEMM launch per tile configuration in use: problem i of g
+// runs with tiles[i]; tiles may be null (every problem Auto) or hold one
+// entry (all problems alike).  The Auto problems of a launch share one
+// configuration, the one gemm_tile_rule favours over their rows in total,
+// so a launch splits in two only where problems ask for different ones.
+void emit_gemm(Program* prog, int level, std::vector<GemmDesc>& g, bool leaves, const std::vector<int>* tiles) {
   if (g.empty()) return;
-  const int64_t tiles = gemm_prepare(g.data(), (int)g.size());
   double flops = 0.0;
   for (const GemmDesc& d : g) flops += 2.0 * d.m * d.n * (double)d.k;
   if (leaves) {
@@ -284,16 +288,43 @@ void emit_gemm(Program* prog, int level, std::vector<GemmDesc>& g, bool leaves) 
   } else {
     prog->peel_flops += flops;
   }
-  if (tiles == 0) return;
-  Op op;
-  op.kind = OpKind::kGemm;
-  op.n = (int)g.size();
-  op.total_tiles = tiles;
-  op.level = level;
-  op.peel = !leaves;
-  op.flops = flops;
-  op.desc_off = append_desc(prog, g);
-  prog->ops.push_back(op);
+  auto asked = [&](size_t i) {
+    const int c = (tiles && !tiles->empty()) ? (*tiles)[tiles->size() == 1 ? 0 : i] : kGemmTileAuto;
+    return (c == kGemmTileLarge || c == kGemmTileSmall) ? c : kGemmTileAuto;
+  };
+  // padded tile area of the Auto problems under each configuration
+  double area_large = 0.0, area_small = 0.0;
+  for (size_t i = 0; i < g.size(); ++i) {
+    if (asked(i) != kGemmTileAuto) continue;
+    const double cols = (double)((g[i].n + kGemmBN - 1) / kGemmBN) * kGemmBN;
+    area_large += cols * (double)((g[i].m + kGemmBM - 1) / kGemmBM) * kGemmBM;
+    area_small += cols * (double)((g[i].m + kGemmBMSmall - 1) / kGemmBMSmall) * kGemmBMSmall;
+  }
+  const int auto_cfg = area_large > 1.07 * area_small ? kGemmTileSmall : kGemmTileLarge;
+  std::vector<GemmDesc> part[2];
+  double part_flops[2] = {0.0, 0.0};
+  for (size_t i = 0; i < g.size(); ++i) {
+    int cfg = asked(i);
+    if (cfg == kGemmTileAuto) cfg = auto_cfg;
+    part[cfg == kGemmTileSmall].push_back(g[i]);
+    part_flops[cfg == kGemmTileSmall] += 2.0 * g[i].m * g[i].n * (double)g[i].k;
+  }
+  for (int c = 0; c < 2; ++c) {
+    if (part[c].empty()) continue;
+    const int cfg = c ? kGemmTileSmall : kGemmTileLarge;
+    const int64_t ntiles = gemm_prepare(part[c].data(), (int)part[c].size(), kGemmBN, gemm_tile_rows(cfg));
+    if (ntiles == 0) continue;
+    Op op;
+    op.kind = OpKind::kGemm;
+    op.n = (int)part[c].size();
+    op.total_tiles = ntiles;
+    op.gemm_tile = cfg;
+    op.level = level;
+    op.peel = !leaves;
+    op.flops = part_flops[c];
+    op.desc_off = append_desc(prog, part[c]);
+    prog->ops.push_back(op);
+  }
 }
 
 // Leaf products of one launch as split products of split code `slices`
@@ -350,9 +381,9 @@ void place_split_scratch(Program* prog, char* ws) {
 class Builder {
  public:
   Builder(int alg, int steps, int dfs_levels, const std::vector<LevelDims>& dims, const std::vector<LevelLayout>& lay,
-          const double* slots, char* ws, Program* prog)
+          const double* slots, char* ws, Program* prog, int gemm_tile)
       : alg_(alg), t_(fmm_algorithms[alg]), steps_(steps), d_(dfs_levels), dims_(dims), lay_(lay), slots_(slots),
-        ws_(ws), prog_(prog) {}
+        ws_(ws), prog_(prog), tile_(1, gemm_tile) {}
 
   void level(int l, const std::vector<SubProblem>& F) {
     if (F.empty()) return;
@@ -363,7 +394,7 @@ class Builder {
       if (prog_->split_slices > 0)
         emit_split_gemm(prog_, l, g, prog_->split_slices);
       else
-        emit_gemm(prog_, l, g, true);
+        emit_gemm(prog_, l, g, true, &tile_);
       return;
     }
     if (l < d_) {
@@ -406,7 +437,7 @@ class Builder {
     }
     std::vector<GemmDesc> g;
     for (int64_t q = 0; q < nf; ++q) add_peel_descs(t_, dims_[l], F[q], &g);
-    emit_gemm(prog_, l, g, false);
+    emit_gemm(prog_, l, g, false, &tile_);
   }
 
   int alg_;
@@ -418,6 +449,7 @@ class Builder {
   const double* slots_;
   char* ws_;
   Program* prog_;
+  std::vector<int> tile_;  // the program's tile configuration (one entry)
 };
 
 struct ItemState {
@@ -488,7 +520,8 @@ size_t workspace_bytes(const fmm_alg_table& t, int64_t m, int64_t k, int64_t n, 
 }
 
 void build_program(int alg, int64_t m, int64_t k, int64_t n, int steps, double x, double alpha, double beta,
-                   int dfs_levels, Operand A, Operand B, Operand C, void* ws, Program* out, int split_slices) {
+                   int dfs_levels, Operand A, Operand B, Operand C, void* ws, Program* out, int split_slices,
+                   int gemm_tile) {
   const fmm_alg_table& t = fmm_algorithms[alg];
   const std::vector<LevelDims> dims = level_dims(t, m, k, n, steps);
   size_t total = 0;
@@ -503,7 +536,7 @@ void build_program(int alg, int64_t m, int64_t k, int64_t n, int steps, double x
   // FastMatmul (strassen.hpp:661-722): A's multiplier is alpha; the first
   // recursion folds it into C's (C.mult = 1 * alpha * 1).
   SubProblem root{A, B, C, 1.0 * alpha * 1.0, beta};
-  Builder b(alg, steps, dfs_levels, dims, lay, out->coefs[0].v, static_cast<char*>(ws), out);
+  Builder b(alg, steps, dfs_levels, dims, lay, out->coefs[0].v, static_cast<char*>(ws), out, gemm_tile);
   b.level(0, std::vector<SubProblem>{root});
   place_split_scratch(out, static_cast<char*>(ws));
 }
@@ -619,19 +652,22 @@ void build_batch_program(const BatchItem* items, int count, void* ws, Program* o
   // distinct slice count
   {
     std::map<int, std::vector<GemmDesc>> g;
+    std::vector<int> fp64_tiles;  // tile configuration of each FP64 leaf (g[0])
     for (int i = 0; i < count; ++i) {
       const ItemState& s = st[(size_t)i];
       const size_t steps = (size_t)steps_of(i);
-      std::vector<GemmDesc>& dst = g[std::max(0, items[i].split_slices)];
+      const int code = std::max(0, items[i].split_slices);
+      std::vector<GemmDesc>& dst = g[code];
       for (const SubProblem& p : s.frontier[steps]) {
         GemmDesc d = leaf_desc(s.dims[steps], p);
         if (items[i].classical) d.beta = items[i].beta;
         dst.push_back(d);
+        if (code == 0) fp64_tiles.push_back(items[i].gemm_tile);
       }
     }
     for (auto& kv : g) {
       if (kv.first == 0)
-        emit_gemm(out, max_steps, kv.second, true);
+        emit_gemm(out, max_steps, kv.second, true, &fp64_tiles);
       else
         emit_split_gemm(out, max_steps, kv.second, kv.first);
     }
@@ -658,13 +694,15 @@ void build_batch_program(const BatchItem* items, int count, void* ws, Program* o
       emit_combine(out, g.first.first, g.first.second, l, cd, vec2, mx, bytes);
     }
     std::vector<GemmDesc> peel;
+    std::vector<int> peel_tiles;
     for (int i = 0; i < count; ++i) {
       if (steps_of(i) <= l) continue;
       const fmm_alg_table& t = fmm_algorithms[items[i].alg];
       const ItemState& s = st[(size_t)i];
       for (const SubProblem& p : s.frontier[(size_t)l]) add_peel_descs(t, s.dims[(size_t)l], p, &peel);
+      peel_tiles.resize(peel.size(), items[i].gemm_tile);
     }
-    emit_gemm(out, l, peel, false);
+    emit_gemm(out, l, peel, false, &peel_tiles);
   }
   place_split_scratch(out, base);
 }

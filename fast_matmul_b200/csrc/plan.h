@@ -28,6 +28,7 @@ struct Op {
   int n_s = 0, n_t = 0; // form: sub-problems on the A and B side
   int64_t max_items = 0;     // form / combine: largest per-problem work-item count
   int64_t total_tiles = 0;   // gemm
+  int gemm_tile = kGemmTileLarge;  // gemm: tile configuration the descriptors were prepared for
   bool vec2 = false;
   bool peel = false;     // gemm: dynamic-peeling fringe products
   int level = 0;         // recursion level the launch belongs to (steps = leaves)
@@ -85,8 +86,11 @@ size_t workspace_bytes(const fmm_alg_table& t, int64_t m, int64_t k, int64_t n, 
 // Builds the launch program of one call.  ws must hold workspace_bytes(...) bytes.
 // split_slices > 0 (a split code: slice count, BF16 or INT8 digits) runs
 // the leaf products (not the fringe products of dynamic peeling) split.
+// gemm_tile (kGemmTileAuto / Large / Small) is the tile configuration of
+// the FP64 leaf and fringe products; Auto picks one per problem.
 void build_program(int alg, int64_t m, int64_t k, int64_t n, int steps, double x, double alpha, double beta,
-                   int dfs_levels, Operand A, Operand B, Operand C, void* ws, Program* out, int split_slices = 0);
+                   int dfs_levels, Operand A, Operand B, Operand C, void* ws, Program* out, int split_slices = 0,
+                   int gemm_tile = kGemmTileAuto);
 
 // One independent product of a batch.  A classical item is one GEMM
 // C = alpha * A * B + beta * C (beta honoured; alg and steps unused); the
@@ -99,6 +103,7 @@ struct BatchItem {
   double x, alpha, beta;
   bool classical;
   int split_slices = 0;  // > 0: split code of this item's leaf products
+  int gemm_tile = kGemmTileAuto;  // tile configuration of this item's FP64 products
 };
 
 // Workspace of a batch (every item planned breadth-first, regions back to back).

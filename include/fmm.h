@@ -91,12 +91,28 @@ typedef enum fmm_precision {
 
 typedef struct fmm_handle_s* fmm_handle;
 
+/* Tile configuration of the FP64 tensor-core GEMM (no counterpart in the
+ * reference, whose leaves call the host BLAS).  Both configurations sum every
+ * output element over the same k order, so the choice changes speed only,
+ * never a result.
+ *   AUTO   per launch: SMALL where 128-row tiles would pad the rows of the
+ *          launch's problems by more than 7% beyond 64-row tiles, else LARGE
+ *          (a batch whose items ask for different ones gets two launches).
+ *   LARGE  128 x 64 tiles, two CTAs per SM (the faster one on large products).
+ *   SMALL  64 x 64 tiles, three CTAs per SM. */
+typedef enum fmm_gemm_tile {
+  FMM_GEMM_TILE_AUTO = 0,
+  FMM_GEMM_TILE_LARGE = 1,
+  FMM_GEMM_TILE_SMALL = 2
+} fmm_gemm_tile;
+
 typedef struct fmm_options {
   fmm_schedule schedule;    /* default FMM_SCHEDULE_AUTO */
   fmm_precision precision;  /* default FMM_PRECISION_FP64 */
   int split_slices;         /* slices per operand: SPLIT_BF16 2..6 (0 = default 5), SPLIT_INT8 2..8 (0 = 6) */
   int dfs_levels;           /* HYBRID only: depth-first levels; -1 = choose */
   size_t workspace_limit;   /* bytes; 0 = the handle's limit */
+  int gemm_tile;            /* fmm_gemm_tile of the FP64 leaf and fringe products */
 } fmm_options;
 
 /* Fills *opts with the defaults above. */
@@ -359,6 +375,8 @@ typedef struct fmm_batch_item {
   double x, alpha, beta; /* as in fmm_fast_matmul */
   int precision;         /* fmm_precision of the item's leaf products (0 = FP64) */
   int split_slices;      /* slices: SPLIT_BF16 2..6, SPLIT_INT8 2..8 (0 = default) */
+  int gemm_tile;         /* fmm_gemm_tile of the item's FP64 products (AUTO: the autotuned choice of
+                            the item's shape bucket for FMM_ALG_AUTO items, else per problem) */
 } fmm_batch_item;
 
 /* Independent products in one program: the operand formations of all items
@@ -376,17 +394,22 @@ fmm_status fmm_fast_matmul_batched(fmm_handle h, const fmm_batch_item* items, in
  * 4000; Strassen with 2 steps from 4000; fast424_26_206 with 2 steps from
  * 12000 in every dimension).  *alg is FMM_ALG_CLASSICAL for a plain GEMM. */
 fmm_status fmm_autotune_choice(fmm_handle h, int64_t m, int64_t k, int64_t n, int* alg, int* num_steps);
+/* The FP64 GEMM tile configuration (fmm_gemm_tile) the autotuner measured
+ * fastest for the shape's bucket, FMM_GEMM_TILE_AUTO for an unmeasured
+ * bucket.  FMM_ALG_AUTO batch items with gemm_tile AUTO use it. */
+fmm_status fmm_autotune_tile(fmm_handle h, int64_t m, int64_t k, int64_t n, int* tile);
 
 /* Times, for one representative shape per bucket of `shapes` (count x 3:
  * m, k, n), the classical GEMM and every candidate algorithm with 1 ..
- * max_steps levels (leaf blocks of at least 64), and records the fastest per
- * bucket in the handle.  candidates may be NULL (Strassen, fast424_26_206,
+ * max_steps levels (leaf blocks of at least 64), each with both FP64 GEMM
+ * tile configurations, and records the fastest per bucket in the handle.  candidates may be NULL (Strassen, fast424_26_206,
  * fast333_23_125, smirnov333_23_128).  Allocates scratch matrices. */
 fmm_status fmm_autotune(fmm_handle h, const int64_t* shapes, int count, const int* candidates, int n_candidates,
                         int max_steps);
 
-/* The tuning table as text lines "mb kb nb alg steps" (buckets are
- * ceil(log2(dim))), and loading it back. */
+/* The tuning table as text lines "mb kb nb alg steps tile" (buckets are
+ * ceil(log2(dim)), tile an fmm_gemm_tile), and loading it back (lines
+ * without the tile column load with FMM_GEMM_TILE_AUTO). */
 fmm_status fmm_autotune_export(fmm_handle h, char* buf, size_t cap, size_t* len);
 fmm_status fmm_autotune_import(fmm_handle h, const char* text);
 

@@ -114,11 +114,14 @@ def test_autotune_records_valid_choices_and_roundtrips():
     table = fmm.autotune_table(handle=h)
     lines = [l.split() for l in table.strip().splitlines()]
     assert len(lines) == 2
-    for mb, kb, nb, alg, steps in lines:
+    for mb, kb, nb, alg, steps, tile in lines:
         assert int(alg) == fmm.CLASSICAL or 0 <= int(alg) < fmm.num_algorithms()
+        assert int(tile) in (1, 2)  # the measured FP64 GEMM tile configuration
     alg, steps = fmm.autotune_choice(256, 256, 256, handle=h)
+    tile = fmm.autotune_tile(256, 256, 256, handle=h)
     h2 = fmm.Handle(0)
     fmm.autotune_load(table, handle=h2)
     assert fmm.autotune_choice(256, 256, 256, handle=h2) == (alg, steps)
+    assert fmm.autotune_tile(256, 256, 256, handle=h2) == tile
     h.close()
     h2.close()
