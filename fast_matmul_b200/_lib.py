@@ -12,7 +12,9 @@ import os
 import threading
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libfmm.so")
+# FMM_LIBRARY selects another build of the engine, e.g. libfmm_checked.so
+# (device-side checks, see fmm_debug_check_flags); the default is libfmm.so.
+LIB_PATH = os.environ.get("FMM_LIBRARY") or os.path.join(_HERE, "libfmm.so")
 
 _lock = threading.Lock()
 _lib = None
@@ -121,6 +123,7 @@ SIGNATURES = {
     "fmm_set_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "fmm_set_workspace_limit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t]),
     "fmm_release_workspace": (ctypes.c_int, [ctypes.c_void_p]),
+    "fmm_debug_check_flags": (ctypes.c_int, [ctypes.POINTER(ctypes.c_uint)]),
     "fmm_debug_fill_workspace": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]),
     "fmm_last_error": (ctypes.c_char_p, []),
     "fmm_num_algorithms": (ctypes.c_int, []),

@@ -20,6 +20,7 @@
 
 #include <cstdint>
 
+#include "device_checks.cuh"
 #include "fmm_internal.h"
 
 namespace fmm {
@@ -88,7 +89,10 @@ __global__ void __launch_bounds__(kAddThreads) form_kernel(FormLaunch L, CoefSlo
         const int bi = b / nbc, bj = b % nbc;
         return ld_block<T>(in + bi * rows + bj * cols * d.ld_in);
       };
-      auto st = [&](int o, T v) { st_block<T>(out + o * d.out_stride, v); };
+      auto st = [&](int o, T v) {
+        double* p = out + o * d.out_stride;
+        if (FMM_CHECK(FMM_IN_WORKSPACE(p, sizeof(T)), kCheckFormOut)) st_block<T>(p, v);
+      };
       if (s_side)
         ALG::template form_s<T>(cf.v, ld, st);
       else
@@ -113,7 +117,10 @@ __global__ void __launch_bounds__(kAddThreads) combine_kernel(CombineLaunch L, C
       if (i >= rows) continue;
       const double* mp = d.m + i + j * d.ld_m;
       double* cp = d.c + i + j * d.ld_c;
-      auto ld = [&](int r) -> T { return ld_block<T>(mp + r * d.m_stride); };
+      auto ld = [&](int r) -> T {
+        const double* p = mp + r * d.m_stride;
+        return FMM_CHECK(FMM_IN_WORKSPACE(p, sizeof(T)), kCheckCombineIn) ? ld_block<T>(p) : T{};
+      };
       auto cptr = [&](int c) -> double* {
         const int ci = c / ALG::kN0, cj = c % ALG::kN0;
         return cp + ci * rows + cj * cols * d.ld_c;
@@ -167,6 +174,23 @@ cudaError_t launch_combine(const CombineLaunch& L, const CoefSlots& cf, bool vec
 }
 
 }  // namespace
+
+bool device_checks_built() { return kDeviceChecks; }
+
+cudaError_t device_checks_arm(const void* ws, size_t bytes, cudaStream_t stream) {
+  if (!kDeviceChecks) return cudaSuccess;
+  const uintptr_t lo = reinterpret_cast<uintptr_t>(ws);
+  cudaError_t e = fmm_checks_arm_tu(CheckRange{lo, ws ? lo + bytes : 0}, stream);
+  if (e == cudaSuccess) e = gemm_checks_arm(ws, bytes, stream);
+  return e;
+}
+
+cudaError_t device_checks_take(unsigned* word) {
+  *word = 0;
+  cudaError_t e = fmm_checks_take_tu(word);
+  if (e == cudaSuccess) e = gemm_checks_take(word);
+  return e;
+}
 
 cudaError_t form_launch(int alg, const FormLaunch& L, const CoefSlots& cf, bool vec2, int num_sms,
                         cudaStream_t stream) {

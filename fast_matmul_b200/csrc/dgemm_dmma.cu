@@ -35,6 +35,7 @@
 #include <cstdint>
 #include <mutex>
 
+#include "device_checks.cuh"
 #include "fmm_internal.h"
 #include "sm100_primitives.cuh"
 
@@ -265,6 +266,12 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
     const int local = tile - d.tile_begin;
     const int row0 = (local % d.tiles_m) * BM;
     const int col0 = (local / d.tiles_m) * BN;  // tiles_m / tile_begin count tiles of this BN
+    // debug builds: the decoded problem and tile (uniform over the CTA, so a
+    // skipped tile skips every barrier of it for all threads alike)
+    if (!FMM_CHECK(lo >= 0 && lo < nprob && local >= 0 && local < d.tiles_m * ((d.n + BN - 1) / BN),
+                   kCheckGemmProblem))
+      continue;
+    if (!FMM_CHECK(row0 < d.m && col0 < d.n, kCheckGemmTile)) continue;
     const int K = launder(d.k);
     const int ktiles = (K + BK - 1) / BK;
     TileCopy tc;
@@ -472,6 +479,13 @@ cudaError_t gemm_launch_cfg(const GemmDesc* d_descs, int n, int64_t total_tiles,
   grouped_dgemm_kernel<Cfg><<<(unsigned)grid, Cfg::THREADS, Cfg::SMEM_BYTES, stream>>>(d_descs, n, (int)total_tiles);
   return cudaGetLastError();
 }
+
+cudaError_t gemm_checks_arm(const void* ws, size_t bytes, cudaStream_t stream) {
+  const uintptr_t lo = reinterpret_cast<uintptr_t>(ws);
+  return fmm_checks_arm_tu(CheckRange{lo, ws ? lo + bytes : 0}, stream);
+}
+
+cudaError_t gemm_checks_take(unsigned* word) { return fmm_checks_take_tu(word); }
 
 cudaError_t gemm_launch(const GemmDesc* d_descs, int n, int64_t total_tiles, int num_sms, cudaStream_t stream,
                         int tile) {

@@ -25,6 +25,16 @@ Profiler::~Profiler() {
 
 cudaError_t run_program(const Program& prog, const void* h_desc, void* d_desc, int num_sms, cudaStream_t stream,
                         int64_t* launches, Profiler* prof, int* d_err, cudaEvent_t desc_copied) {
+  if (device_checks_built()) {
+    // debug builds: register the program's workspace for the kernels'
+    // checks (not while a graph is captured: the range would be read at
+    // every replay from a host buffer the next program reuses)
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(stream, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone) {
+      cudaError_t e = device_checks_arm(prog.ws_base, prog.workspace_bytes, stream);
+      if (e != cudaSuccess) return e;
+    }
+  }
   if (!prog.desc.empty()) {
     cudaError_t e = cudaMemcpyAsync(d_desc, h_desc, prog.desc.size(), cudaMemcpyHostToDevice, stream);
     if (e != cudaSuccess) return e;

@@ -293,6 +293,15 @@ fmm_status fmm_debug_fill_workspace(fmm_handle h, size_t bytes, int pattern) {
   return FMM_OK;
 }
 
+fmm_status fmm_debug_check_flags(unsigned* flags) {
+  if (!flags) return fail(FMM_ERR_INVALID_ARGUMENT, "null argument");
+  *flags = 0;
+  if (!fmm::device_checks_built())
+    return fail(FMM_ERR_NOT_SUPPORTED, "this library was built without device checks (FMM_DEVICE_CHECKS)");
+  FMM_CUDA_TRY(fmm::device_checks_take(flags), "reading the device check word");
+  return FMM_OK;
+}
+
 fmm_status fmm_release_workspace(fmm_handle h) {
   if (!h) return fail(FMM_ERR_INVALID_ARGUMENT, "null handle");
   DeviceGuard g(h->device);

@@ -48,6 +48,16 @@ inline int gemm_tile_rule(int m) {
   return (double)large > 1.07 * (double)small ? kGemmTileSmall : kGemmTileLarge;
 }
 
+// Device-side checks of the descriptor walks (device_checks.cuh; built in
+// with -DFMM_DEVICE_CHECKS): whether this build has them, registering the
+// workspace of the program about to run, and reading (and clearing) the
+// word of failed checks.  Without them, arming and reading do nothing.
+bool device_checks_built();
+cudaError_t device_checks_arm(const void* ws, size_t bytes, cudaStream_t stream);
+cudaError_t device_checks_take(unsigned* word);
+cudaError_t gemm_checks_arm(const void* ws, size_t bytes, cudaStream_t stream);
+cudaError_t gemm_checks_take(unsigned* word);
+
 // Fills tiles_m / tile_begin / flags for descs[0..n) and returns the total
 // number of tile_m x tile_n tiles.
 int64_t gemm_prepare(GemmDesc* descs, int n, int tile_n = kGemmBN, int tile_m = kGemmBM);

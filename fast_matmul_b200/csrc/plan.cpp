@@ -473,6 +473,7 @@ void Program::clear() {
   split_slices = 0;
   split_scratch = nullptr;
   split_bytes = 0;
+  ws_base = nullptr;
 }
 
 std::vector<LevelDims> level_dims(const fmm_alg_table& t, int64_t m, int64_t k, int64_t n, int steps) {
@@ -539,6 +540,7 @@ void build_program(int alg, int64_t m, int64_t k, int64_t n, int steps, double x
   Builder b(alg, steps, dfs_levels, dims, lay, out->coefs[0].v, static_cast<char*>(ws), out, gemm_tile);
   b.level(0, std::vector<SubProblem>{root});
   place_split_scratch(out, static_cast<char*>(ws));
+  out->ws_base = ws;
 }
 
 // Split scratch of a batch: one split launch per distinct slice count, all
@@ -705,6 +707,7 @@ void build_batch_program(const BatchItem* items, int count, void* ws, Program* o
     emit_gemm(out, l, peel, false, &peel_tiles);
   }
   place_split_scratch(out, base);
+  out->ws_base = ws;
 }
 
 }  // namespace fmm

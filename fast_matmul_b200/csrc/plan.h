@@ -67,6 +67,7 @@ struct Program {
   int split_slices = 0;         // > 0: split code of the leaf products (slices, BF16 or INT8 digits)
   char* split_scratch = nullptr;  // scratch shared by the split launches (inside the workspace)
   size_t split_bytes = 0;       // its size
+  const void* ws_base = nullptr;  // the workspace the program was planned into (workspace_bytes of it)
   void clear();
 };
 

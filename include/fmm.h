@@ -136,6 +136,16 @@ fmm_status fmm_release_workspace(fmm_handle h);
  * synchronises.  A later call that read a temporary before writing it would
  * carry the pattern into C. */
 fmm_status fmm_debug_fill_workspace(fmm_handle h, size_t bytes, int pattern);
+/* Test support, no counterpart in the reference: in a library built with
+ * device-side checks (libfmm_checked.so, -DFMM_DEVICE_CHECKS) the grouped
+ * GEMM and the formation and combination kernels check the problems and
+ * tiles they decode from their descriptors and that the temporaries they
+ * write or read lie inside the running program's workspace; a failed check
+ * skips the access and sets a bit here (1: GEMM problem index, 2: GEMM tile
+ * origin, 4: formation write, 8: combination read).  Reads the bits of the
+ * current device's launches since the last call, clears them, and returns
+ * FMM_ERR_NOT_SUPPORTED (flags 0) in the regular library. */
+fmm_status fmm_debug_check_flags(unsigned* flags);
 /* Upper bound on the workspace the handle may allocate (0 = 60% of the
  * device memory that is free when the handle is created). */
 fmm_status fmm_set_workspace_limit(fmm_handle h, size_t bytes);

@@ -46,7 +46,23 @@ def test_registry_without_gpu():
 def test_options_defaults():
     o = _lib.Options()
     _lib.lib().fmm_options_init(ctypes.byref(o))
-    assert (o.schedule, o.precision, o.dfs_levels, o.workspace_limit) == (0, 0, -1, 0)
+    assert (o.schedule, o.precision, o.dfs_levels, o.workspace_limit, o.gemm_tile) == (0, 0, -1, 0, 0)
+
+
+CHECKED = os.path.join(REPO, "fast_matmul_b200", "libfmm_checked.so")
+
+
+@pytest.mark.skipif(not os.path.exists(CHECKED), reason="libfmm_checked.so not built")
+def test_checked_library_exports_every_symbol():
+    L = ctypes.CDLL(CHECKED)
+    for name in declared_functions("fmm.h"):
+        assert hasattr(L, name), name
+
+
+def test_regular_library_has_no_device_checks():
+    flags = ctypes.c_uint(7)
+    assert _lib.lib().fmm_debug_check_flags(ctypes.byref(flags)) == 5  # FMM_ERR_NOT_SUPPORTED
+    assert flags.value == 0
 
 
 @pytest.mark.skipif(gpu_available(), reason="checks the no-GPU error path")
