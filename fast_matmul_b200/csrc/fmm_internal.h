@@ -132,6 +132,10 @@ __host__ __device__ inline SplitGroup split_group(int cp, int nch, int slices, i
   return g;
 }
 
+// The exponent recorded for a row of A or column of B holding an Inf or a
+// NaN: its digits are zero and every entry of C it reaches is NaN.
+constexpr int kSplitNonFinite = 1 << 28;
+
 struct SplitDesc {
   const double* A;
   const double* B;

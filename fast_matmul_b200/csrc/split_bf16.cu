@@ -16,7 +16,10 @@
 //     magnitude <= 2^24,
 //     so the accumulation is exact.  Each group's sum is scaled by
 //     2^-8(t+u) and added into an FP64 accumulator: all rounding happens in
-//     FP64, in a fixed order.
+//     FP64, in a fixed order;
+//   * a row of A or column of B holding an Inf or a NaN gets the exponent
+//     kSplitNonFinite and zero digits, and the entries of C it reaches are
+//     NaN.
 // Error: |x - sum_t d_t 2^-8t| <= 2^-(8S+1) 2^e per operand entry plus the
 // dropped diagonals, so |C - AB| <~ 3 * 2^-8S * k * max|a_i.| * max|b_.j|.
 //
@@ -107,10 +110,20 @@ __device__ __forceinline__ int find_desc(const SplitDesc* __restrict__ d, int n,
   return lo;
 }
 
-__device__ __forceinline__ int exponent_above(double maxabs) {
-  if (!(maxabs > 0.0)) return 0;
+// |x| as ordered bits: the patterns of non-negative doubles order like their
+// values, and every NaN orders above Inf, so an integer maximum of these
+// finds the largest magnitude and sees a NaN.
+__device__ __forceinline__ unsigned long long abs_bits(double x) {
+  return (unsigned long long)__double_as_longlong(x) & 0x7fffffffffffffffull;
+}
+
+// The least e with max |x| < 2^e from the maximum of abs_bits, 0 for an
+// all-zero row, kSplitNonFinite when it holds an Inf or a NaN.
+__device__ __forceinline__ int exponent_above(unsigned long long maxbits) {
+  if (maxbits >= 0x7ff0000000000000ull) return kSplitNonFinite;
+  if (maxbits == 0) return 0;
   int e;
-  frexp(maxabs, &e);  // maxabs = f 2^e, f in [0.5, 1)
+  frexp(__longlong_as_double((long long)maxbits), &e);  // maxabs = f 2^e, f in [0.5, 1)
   return e;
 }
 
@@ -133,14 +146,14 @@ constexpr int kExpWarps = 16;
 
 __global__ void __launch_bounds__(kExpWarps * 32) split_row_exponents(const SplitDesc* __restrict__ d, int nd,
                                                                       int64_t row_tiles, int* __restrict__ ea) {
-  __shared__ double part[kExpWarps][32];
+  __shared__ unsigned long long part[kExpWarps][32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int64_t w = blockIdx.x; w < row_tiles; w += gridDim.x) {
     const int64_t x0 = w * 32;  // padded rows of one problem come in multiples of 256
     const int q = find_desc(d, nd, x0, [](const SplitDesc& s) { return s.e_off; });
     const SplitDesc& s = d[q];
     const int64_t i = x0 - s.e_off + lane;
-    double mx = 0.0;
+    unsigned long long mx = 0;
     if (i < s.m) {
       const double* a = s.A + i;
       const int64_t lda = s.lda;
@@ -150,16 +163,16 @@ __global__ void __launch_bounds__(kExpWarps * 32) split_row_exponents(const Spli
 #pragma unroll
         for (int u = 0; u < 8; ++u) v[u] = a[(int64_t)(p + u * kExpWarps) * lda];
 #pragma unroll
-        for (int u = 0; u < 8; ++u) mx = fmax(mx, fabs(v[u]));
+        for (int u = 0; u < 8; ++u) mx = max(mx, abs_bits(v[u]));
       }
-      for (; p < s.k; p += kExpWarps) mx = fmax(mx, fabs(a[(int64_t)p * lda]));
+      for (; p < s.k; p += kExpWarps) mx = max(mx, abs_bits(a[(int64_t)p * lda]));
     }
     part[warp][lane] = mx;
     __syncthreads();
     if (warp == 0) {
-      double v = part[0][lane];
+      unsigned long long v = part[0][lane];
 #pragma unroll
-      for (int u = 1; u < kExpWarps; ++u) v = fmax(v, part[u][lane]);
+      for (int u = 1; u < kExpWarps; ++u) v = max(v, part[u][lane]);
       ea[x0 + lane] = exponent_above(v);
     }
     __syncthreads();  // part is reused by the next row tile
@@ -311,7 +324,7 @@ __global__ void __launch_bounds__(256) split_a(const SplitDesc* __restrict__ d, 
     const int e = ea[s.e_off + i0 + row];
     double x[8];
 #pragma unroll
-    for (int c = 0; c < 8; ++c) x[c] = scale_pow2(tile[at(kc + c, row)], e);
+    for (int c = 0; c < 8; ++c) x[c] = e == kSplitNonFinite ? 0.0 : scale_pow2(tile[at(kc + c, row)], e);
     const int64_t slice_bytes = (int64_t)s.kblocks * mp * 128;
     if constexpr (kInt8) {
       const int64_t orow = s.a_row + (kb >> 1) * mp + i0 + row;
@@ -364,17 +377,17 @@ __global__ void __launch_bounds__(32 * kSplitBWarps) split_b(const SplitDesc* __
         for (int c = 0; c < 8; ++c) v[c] = p0 + c < k ? b[p0 + c] : 0.0;
       }
     };
-    double mx = 0.0;
+    unsigned long long mx = 0;
     if (live) {
 #pragma unroll 4
       for (int p0 = lane * 8; p0 < k; p0 += 256) {
         double v[8];
         load8(p0, v);
 #pragma unroll
-        for (int c = 0; c < 8; ++c) mx = fmax(mx, fabs(v[c]));
+        for (int c = 0; c < 8; ++c) mx = max(mx, abs_bits(v[c]));
       }
     }
-    for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+    for (int off = 16; off > 0; off >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, off));
     const int f = exponent_above(mx);
     if (lane == 0) fb[x] = f;
     const int64_t slice_bytes = (int64_t)s.kblocks * np * 128;
@@ -388,7 +401,7 @@ __global__ void __launch_bounds__(32 * kSplitBWarps) split_b(const SplitDesc* __
         for (int c = 0; c < 8; ++c) v[c] = 0.0;
       }
 #pragma unroll
-      for (int c = 0; c < 8; ++c) v[c] = scale_pow2(v[c], f);
+      for (int c = 0; c < 8; ++c) v[c] = f == kSplitNonFinite ? 0.0 : scale_pow2(v[c], f);
       const int64_t orow = s.b_row + (int64_t)(p0 / kRowValues) * np + j;
       if constexpr (kInt8)
         store_digits_i8(v, slices, out + orow * 128 + (p0 % kRowValues), slice_bytes);
@@ -796,6 +809,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(gemm_threads(kEpiGro
           if (col < s.n) {
             double v = __dmul_rn(alpha, ldexp(acc[j], er + fcol[j]));
             if (beta != 0.0) v = __dadd_rn(v, __dmul_rn(beta, cp[col * s.ldc]));
+            if (er == kSplitNonFinite || fcol[j] == kSplitNonFinite) v = __longlong_as_double(0x7ff8000000000000ll);
             cp[col * s.ldc] = v;
           }
         }

@@ -138,6 +138,18 @@ int exponent_above(double maxabs) {
   return e;
 }
 
+// The split kernels' exponent of a row or column: kSplitNonFinite when it
+// holds an Inf or a NaN, else exponent_above of its largest magnitude.
+int split_exponent(const double* x, int64_t stride, int k) {
+  double mx = 0.0;
+  for (int p = 0; p < k; ++p) {
+    const double v = x[(int64_t)p * stride];
+    if (!std::isfinite(v)) return fmm::kSplitNonFinite;
+    mx = std::fmax(mx, std::fabs(v));
+  }
+  return exponent_above(mx);
+}
+
 // Digits of x (|x| < 1): d_t = rint(256 r_{t-1}), r_t = 256 r_{t-1} - d_t.
 void digits(double x, int slices, double* out) {
   for (int t = 0; t < slices; ++t) {
@@ -169,26 +181,19 @@ void split_product(const fmm::SplitDesc& d, int code) {
   const int S = fmm::split_code_slices(code);
   const bool int8 = fmm::split_code_int8(code);
   std::vector<int> ea((size_t)m), fb((size_t)n);
-  for (int i = 0; i < m; ++i) {
-    double mx = 0.0;
-    for (int p = 0; p < k; ++p) mx = std::fmax(mx, std::fabs(d.A[i + (int64_t)p * d.lda]));
-    ea[(size_t)i] = exponent_above(mx);
-  }
-  for (int j = 0; j < n; ++j) {
-    double mx = 0.0;
-    for (int p = 0; p < k; ++p) mx = std::fmax(mx, std::fabs(d.B[p + (int64_t)j * d.ldb]));
-    fb[(size_t)j] = exponent_above(mx);
-  }
+  for (int i = 0; i < m; ++i) ea[(size_t)i] = split_exponent(d.A + i, d.lda, k);
+  for (int j = 0; j < n; ++j) fb[(size_t)j] = split_exponent(d.B + (int64_t)j * d.ldb, 1, k);
+  auto scaled = [](double x, int e) { return e == fmm::kSplitNonFinite ? 0.0 : std::ldexp(x, -e); };
   // dA[(t * k + p) * m + i], dB[(t * k + p) * n + j]
   std::vector<double> dA((size_t)S * k * m), dB((size_t)S * k * n);
   double dg[8];
   for (int p = 0; p < k; ++p) {
     for (int i = 0; i < m; ++i) {
-      (int8 ? digits_i8 : digits)(std::ldexp(d.A[i + (int64_t)p * d.lda], -ea[(size_t)i]), S, dg);
+      (int8 ? digits_i8 : digits)(scaled(d.A[i + (int64_t)p * d.lda], ea[(size_t)i]), S, dg);
       for (int t = 0; t < S; ++t) dA[((size_t)t * k + p) * m + i] = dg[t];
     }
     for (int j = 0; j < n; ++j) {
-      (int8 ? digits_i8 : digits)(std::ldexp(d.B[p + (int64_t)j * d.ldb], -fb[(size_t)j]), S, dg);
+      (int8 ? digits_i8 : digits)(scaled(d.B[p + (int64_t)j * d.ldb], fb[(size_t)j]), S, dg);
       for (int t = 0; t < S; ++t) dB[((size_t)t * k + p) * n + j] = dg[t];
     }
   }
@@ -220,8 +225,24 @@ void split_product(const fmm::SplitDesc& d, int code) {
       }
     }
   }
+  // C = alpha 2^(e_i + f_j) acc (+ beta C); NaN where a non-finite row or column reaches
+  auto store = [&]() {
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < m; ++i) {
+        double* c = &d.C[i + (int64_t)j * d.ldc];
+        double v = d.alpha * std::ldexp(acc[(size_t)j * m + i], ea[(size_t)i] + fb[(size_t)j]);
+        if (d.beta != 0.0) v = v + d.beta * *c;
+        if (ea[(size_t)i] == fmm::kSplitNonFinite || fb[(size_t)j] == fmm::kSplitNonFinite)
+          v = std::numeric_limits<double>::quiet_NaN();
+        *c = v;
+      }
+  };
+  if (int8) {
+    store();
+    return;
+  }
   const int chunks = std::max(1, (k + fmm::kSplitChunk - 1) / fmm::kSplitChunk);
-  for (int cp = 0; !int8 && cp < chunks; cp += fmm::split_chunk_span(S)) {
+  for (int cp = 0; cp < chunks; cp += fmm::split_chunk_span(S)) {
     const int nch = std::min(fmm::split_chunk_span(S), chunks - cp);
     for (int gi = 0; gi < fmm::split_groups_in_pair(nch, S); ++gi) {
       const fmm::SplitGroup G = fmm::split_group(cp, nch, S, gi);
@@ -234,13 +255,7 @@ void split_product(const fmm::SplitDesc& d, int code) {
       }
     }
   }
-  for (int j = 0; j < n; ++j)
-    for (int i = 0; i < m; ++i) {
-      double* c = &d.C[i + (int64_t)j * d.ldc];
-      double v = d.alpha * std::ldexp(acc[(size_t)j * m + i], ea[(size_t)i] + fb[(size_t)j]);
-      if (d.beta != 0.0) v = v + d.beta * *c;
-      *c = v;
-    }
+  store();
 }
 
 void run_split(const fmm::Op& op, const unsigned char* desc) {

@@ -3,7 +3,8 @@
 * the device result equals the CPU model of the split arithmetic
   (tests/native/plan_emulator.cpp) bit for bit: the FP32 accumulation of
   every diagonal and k-chunk is exact and the FP64 recombination runs in a
-  fixed order, so nothing may differ;
+  fixed order, so nothing may differ -- deep k and Inf / NaN inputs (NaN in
+  every entry they reach) included;
 * FastMatmul with split leaves equals the model's planner run bit for bit
   (every schedule), and stays within the stated error of the FP64 oracle;
 * batches and the request server give every split item the result it gets
@@ -87,6 +88,52 @@ def test_split_gemm_equals_model_bit_exact(shape):
         got = to_host(Cd)
         want = model_gemm(A, B, C0, alpha, beta, slices)
         assert np.array_equal(got, want), (shape, slices, float(np.abs(got - want).max()))
+
+
+@pytest.mark.parametrize("slices", [3, 5])
+def test_split_gemm_deep_k_equals_model(slices):
+    # k = 33000: 258 chunks (3 slices: 129 chunk pairs)
+    m, k, n = 40, 33000, 36
+    A = oracle.uniform(m, k, 12, 1)
+    B = oracle.uniform(k, n, 12, 2)
+    C0 = oracle.uniform(m, n, 12, 3)
+    Cd = to_device(C0)
+    fmm.matmul_split_bf16(to_device(A), to_device(B), Cd, 1.25, -0.5, slices)
+    fmm.synchronize()
+    got = to_host(Cd)
+    assert np.array_equal(got, model_gemm(A, B, C0, 1.25, -0.5, slices))
+    want = 1.25 * (A @ B) - 0.5 * C0
+    assert float(np.abs(got - want).max() / np.abs(want).max()) <= 3.0 * k * 2.0 ** (-8 * slices)
+
+
+@pytest.mark.parametrize("code", [5, 6, 16 + 6], ids=["bf16-s5", "bf16-s6", "int8-s6"])
+def test_split_gemm_non_finite_inputs_give_nan_where_they_reach(code):
+    m, k, n = 300, 500, 260
+    A = oracle.uniform(m, k, 13, 1)
+    B = oracle.uniform(k, n, 13, 2)
+    A[7, 33] = np.nan
+    A[150, 0] = np.inf
+    B[499, 5] = -np.inf
+    B[250, 259] = np.nan
+    C0 = oracle.uniform(m, n, 13, 3)
+    Cd = to_device(C0)
+    if code >= 16:
+        fmm.matmul_split_int8(to_device(A), to_device(B), Cd, 1.0, 0.5, code - 16)
+    else:
+        fmm.matmul_split_bf16(to_device(A), to_device(B), Cd, 1.0, 0.5, code)
+    fmm.synchronize()
+    got = to_host(Cd)
+    bad = np.zeros((m, n), bool)
+    bad[[7, 150], :] = True
+    bad[:, [5, 259]] = True
+    assert np.array_equal(np.isnan(got), bad)
+    assert np.array_equal(got, model_gemm(A, B, C0, 1.0, 0.5, code), equal_nan=True)
+    # the other entries are those of the inputs with the bad rows and columns cleared
+    A2, B2 = A.copy(order="F"), B.copy(order="F")
+    A2[[7, 150], :] = 0.0
+    B2[:, [5, 259]] = 0.0
+    clean = model_gemm(A2, B2, C0, 1.0, 0.5, code)
+    assert np.array_equal(got[~bad], clean[~bad])
 
 
 def test_split_gemm_scaled_normal_inputs():

@@ -3,7 +3,8 @@
 The test interpreter (tests/native/plan_emulator.cpp) models the device
 arithmetic of the split-BF16 products exactly: power-of-two row / column
 scaling, 8-bit digit slices, exact integer sums per diagonal and 128-deep
-k-chunk, FP64 recombination in the device's order.  These tests check that
+k-chunk, FP64 recombination in the device's order, NaN from Inf / NaN
+inputs.  These tests check that
 model against the FP64 oracle (error bound per slice count), that the
 planner gives every schedule and batch the same split products, and that the
 workspace query covers the split scratch.  The GPU tests compare the device
@@ -66,6 +67,27 @@ def test_split_product_within_its_error_bound(slices):
     assert err <= 3.0 * 2.0 ** (-8 * slices) + 1e-15, (slices, err)
     if slices >= 3:
         assert err <= 1e-5 * 2.0 ** (-8 * (slices - 3))
+
+
+@pytest.mark.parametrize("code", [3, 5, 6, 16 + 6])
+def test_non_finite_rows_and_columns_give_nan(code):
+    E = emulator()
+    m, k, n = 20, 300, 15
+    A = oracle.uniform(m, k, 6, 1)
+    B = oracle.uniform(k, n, 6, 2)
+    A[3, 10] = np.nan
+    B[0, 4] = np.inf
+    got = np.zeros((m, n), order="F")
+    split_gemm(E, A, B, got, 1.0, 0.0, code)
+    bad = np.zeros((m, n), bool)
+    bad[3, :] = True
+    bad[:, 4] = True
+    assert np.array_equal(np.isnan(got), bad)
+    A[3, :] = 0.0
+    B[:, 4] = 0.0
+    clean = np.zeros((m, n), order="F")
+    split_gemm(E, A, B, clean, 1.0, 0.0, code)
+    assert np.array_equal(got[~bad], clean[~bad])
 
 
 def test_more_slices_are_more_accurate():
