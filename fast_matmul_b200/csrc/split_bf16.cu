@@ -86,8 +86,6 @@ constexpr uint16_t kPairMask = 0x3;  // both CTAs of the cluster
 // warpgroups of 32 columns (measured +6-8% at 3 slices), more slices two of
 // 64 (four were 2% slower at 5).
 constexpr int gemm_threads(int epi_groups) { return 32 * (2 + 4 * epi_groups); }
-// epilogue warpgroups of the BF16 form at 4 slices or more
-constexpr int kManyEpiGroups = 2;
 // INT8 digits pair the diagonals (D, D + 1): a stage holds A_t with B_{D-t}
 // and B_{D+1-t} (64 KB, two products from one A tile), 3 stages.
 constexpr int kI8StageBytes = kStageKBlocks * (kATileBytes + 2 * kBTileBytes);
@@ -484,28 +482,6 @@ __device__ __forceinline__ bool for_each_group(int chunks, int S, Fn&& fn) {
   return true;
 }
 
-// Paired stages: a stage holds A_t with B_{D0-t} and B_{D0+1-t}, so one A
-// tile feeds the products of two diagonals (D0, D0 + 1) in two accumulators,
-// and the lone product (D0 + 1, 0) of the upper diagonal follows (16 MMAs per
-// stage wait instead of 8, a third fewer shared-memory bytes per MMA).
-// Calls fn(D0, two) for the diagonal pairs of one chunk group in diagonal
-// order (two = false: D0 alone).  INT8 digits pair from the bottom, (0, 1),
-// (2, 3), ..., an odd last diagonal alone; BF16 digits from the top, a lone
-// diagonal 0 at odd slice counts, then (1, 2), (3, 4), ...: the lone
-// diagonal is then the one with a single product (9 stages per chunk at 5
-// slices against 11).
-template <bool kInt8, class Fn>
-__device__ __forceinline__ bool for_each_pair(int S, Fn&& fn) {
-  int D0 = 0;
-  if (!kInt8 && (S & 1)) {
-    if (!fn(0, false)) return false;
-    D0 = 1;
-  }
-  for (; D0 < S; D0 += 2)
-    if (!fn(D0, D0 + 1 < S)) return false;
-  return true;
-}
-
 // A drained accumulator value as a double (exact either way) and the weight
 // of diagonal D: FP32 sums of BF16 digits weigh 2^-8(D+2), int32 sums of
 // INT8 digits 2^-(12+7D).
@@ -522,15 +498,15 @@ __device__ __forceinline__ double diagonal_weight(int D) {
   return kInt8 ? ldexp(1.0, -(12 + 7 * D)) : ldexp(1.0, -8 * (D + 2));
 }
 
-template <int kEpiGroups, bool kInt8, bool kFewSlices>
+template <int kEpiGroups, bool kInt8>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(gemm_threads(kEpiGroups), 1)
     split_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                       const GemmParams g) {
   constexpr int kEpiCols = kBN / kEpiGroups;
   constexpr int kEpiWarps = 4 * kEpiGroups;
-  // chunks per accumulation pair: BF16 digits at 3 slices or fewer
-  // (kFewSlices), where split_chunk_span pairs chunks (the launch checks this)
-  constexpr int kSpan = kFewSlices ? 2 : 1;
+  // chunks per accumulation pair: the four-warpgroup form runs 3 slices or
+  // fewer, where split_chunk_span pairs chunks (the launch checks this)
+  constexpr int kSpan = kEpiGroups == 4 ? 2 : 1;
   static_assert(kEpiCols % 16 == 0, "drains move pairs of 8-column pieces");
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -561,14 +537,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(gemm_threads(kEpiGro
   cluster_sync();  // barriers of both CTAs initialised, tensor memory allocated
   tc_fence_after();
   const uint32_t tmem = tmem_slot;
-  // paired stages (for_each_pair): INT8 digits, and BF16 digits at 4 slices
-  // or more; 3 stages of a diagonal pair, else 4 stages of one slice product
-  constexpr bool kPaired = kInt8 || !kFewSlices;
-  static_assert(!(kInt8 && kFewSlices), "INT8 digits walk their own groups");
-  constexpr int kSt = kPaired ? kI8Stages : kStages;
-  constexpr int kStB = kPaired ? kI8StageBytes : kStageBytes;
-  // chunks over which a diagonal accumulates: one (BF16) or a group (INT8)
-  constexpr int kPairGroup = kInt8 ? kSplitI8GroupChunks : 1;
+  // the stage ring: 4 stages of one slice product (BF16), 3 of a diagonal pair (INT8)
+  constexpr int kSt = kInt8 ? kI8Stages : kStages;
+  constexpr int kStB = kInt8 ? kI8StageBytes : kStageBytes;
 
   if (warp == 0) {
     if (lane == 0) {
@@ -585,9 +556,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(gemm_threads(kEpiGro
         const int64_t ya_tile = s.a_row + (int64_t)tc.tm * kSplitPairRows + rank * kBM;
         const int64_t yb_tile = s.b_row + (int64_t)tc.tn * kBN + rank * kBHalf;
         const int chunks = s.kblocks / kChunkBlocks;
-        if constexpr (kPaired) {
+        if constexpr (kInt8) {
           // one stage: A_t with B_u1 and, for a paired product, B_u2, over
-          // one chunk (two 128-byte k-block rows) starting at k-block blk
+          // one 256-deep chunk starting at k-block blk
           auto load_stage = [&](int t, int u1, int u2, int64_t blk) -> bool {
             if (n >= (uint32_t)kSt && !mbar_wait(&empty[st], ph ^ 1u, g.err, 1)) return false;
             uint8_t* dst = base + st * kStB;
@@ -618,18 +589,17 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(gemm_threads(kEpiGro
           };
           // per group of chunks, the diagonal pairs (D0, D0 + 1) in order;
           // per chunk the stages t = 0..D0 (products (t, D0 - t) and
-          // (t, D0 + 1 - t)) and the lone (D0 + 1, 0); a lone diagonal D0
-          // has the stages t = 0..D0 alone
-          for (int cg = 0; cg < chunks && ok; cg += kPairGroup) {
-            const int cend = min(cg + kPairGroup, chunks);
-            ok = for_each_pair<kInt8>(S, [&](int D0, bool two) {
-              for (int c = cg; c < cend; ++c)
-                for (int t = 0; t <= D0 + (two ? 1 : 0); ++t)
-                  if (!load_stage(t, t <= D0 ? D0 - t : 0, (two && t <= D0) ? D0 + 1 - t : -1,
-                                  (int64_t)c * kChunkBlocks))
-                    return false;
-              return true;
-            });
+          // (t, D0 + 1 - t)) and the lone (D0 + 1, 0); an odd last diagonal
+          // alone
+          for (int cg = 0; cg < chunks && ok; cg += kSplitI8GroupChunks) {
+            const int cend = min(cg + kSplitI8GroupChunks, chunks);
+            for (int D0 = 0; D0 < S && ok; D0 += 2) {
+              const bool two = D0 + 1 < S;
+              for (int c = cg; c < cend && ok; ++c)
+                for (int t = 0; t <= D0 + (two ? 1 : 0) && ok; ++t)
+                  ok = load_stage(t, t <= D0 ? D0 - t : 0, (two && t <= D0) ? D0 + 1 - t : -1,
+                                  (int64_t)c * kChunkBlocks);
+            }
           }
           continue;
         }
@@ -678,51 +648,52 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(gemm_threads(kEpiGro
       for (int64_t tile = pair; tile < g.tiles && ok; tile += pairs) {
         const TileCoord tc = tile_coord(g, tile);
         const int chunks = g.desc[tc.q].kblocks / kChunkBlocks;
-        if constexpr (kPaired) {
+        if constexpr (kInt8) {
           // the producer's order: per group of chunks, per diagonal pair
           // (D0, D0 + 1) in accumulators b0, b1, per chunk the stages
           // t = 0..D0 (8 MMAs into b0 from B_{D0-t}, 8 into b1 from
           // B_{D0+1-t}) and the lone (D0 + 1, 0) into b1
-          for (int cg = 0; cg < chunks && ok; cg += kPairGroup) {
-            const int cend = min(cg + kPairGroup, chunks);
-            ok = for_each_pair<kInt8>(S, [&](int D0, bool two) {
+          for (int cg = 0; cg < chunks && ok; cg += kSplitI8GroupChunks) {
+            const int cend = min(cg + kSplitI8GroupChunks, chunks);
+            for (int D0 = 0; D0 < S && ok; D0 += 2) {
+              const bool two = D0 + 1 < S;
               const uint32_t b0 = ai % kAccBufs, b1 = (ai + 1) % kAccBufs;
-              if (ai >= (uint32_t)kAccBufs && !mbar_wait(&acc_empty[b0], ((ai / kAccBufs) - 1) & 1, g.err, 2))
-                return false;
+              if (ai >= (uint32_t)kAccBufs && !mbar_wait(&acc_empty[b0], ((ai / kAccBufs) - 1) & 1, g.err, 2)) {
+                ok = false;
+                break;
+              }
               if (two && ai + 1 >= (uint32_t)kAccBufs &&
-                  !mbar_wait(&acc_empty[b1], (((ai + 1) / kAccBufs) - 1) & 1, g.err, 2))
-                return false;
+                  !mbar_wait(&acc_empty[b1], (((ai + 1) / kAccBufs) - 1) & 1, g.err, 2)) {
+                ok = false;
+                break;
+              }
               tc_fence_after();
-              for (int c = cg; c < cend; ++c)
+              for (int c = cg; c < cend && ok; ++c)
                 for (int t = 0; t <= D0 + (two ? 1 : 0); ++t) {
-                  if (!mbar_wait(&full[st], ph, g.err, 3)) return false;
+                  if (!mbar_wait(&full[st], ph, g.err, 3)) {
+                    ok = false;
+                    break;
+                  }
                   tc_fence_after();
                   const bool paired = two && t <= D0;
                   const uint32_t d_first = tmem + ((two && t > D0) ? b1 : b0) * kBN;
                   const uint32_t a = smem_addr(base + st * kStB);
                   const uint32_t bb1 = a + kStageKBlocks * kATileBytes;
                   const uint32_t bb2 = bb1 + kStageKBlocks * kBTileBytes;
-                  const bool acc0 = c > cg || t > 0;  // the accumulator holds earlier sums
 #pragma unroll
                   for (int kk = 0; kk < kStageKBlocks * kBK / 16; ++kk) {
                     const uint32_t koff = (kk & 3) * 32;
-                    const uint64_t ad = smem_desc_sw128(a + (kk >> 2) * kATileBytes + koff);
-                    const uint64_t bd = smem_desc_sw128(bb1 + (kk >> 2) * kBTileBytes + koff);
-                    if constexpr (kInt8)
-                      mma_s8_pair(d_first, ad, bd, idesc, acc0 || kk > 0);
-                    else
-                      mma_bf16_pair(d_first, ad, bd, idesc, acc0 || kk > 0);
+                    mma_s8_pair(d_first, smem_desc_sw128(a + (kk >> 2) * kATileBytes + koff),
+                                smem_desc_sw128(bb1 + (kk >> 2) * kBTileBytes + koff), idesc,
+                                c > cg || t > 0 || kk > 0);
                   }
                   if (paired) {
 #pragma unroll
                     for (int kk = 0; kk < kStageKBlocks * kBK / 16; ++kk) {
                       const uint32_t koff = (kk & 3) * 32;
-                      const uint64_t ad = smem_desc_sw128(a + (kk >> 2) * kATileBytes + koff);
-                      const uint64_t bd = smem_desc_sw128(bb2 + (kk >> 2) * kBTileBytes + koff);
-                      if constexpr (kInt8)
-                        mma_s8_pair(tmem + b1 * kBN, ad, bd, idesc, acc0 || kk > 0);
-                      else
-                        mma_bf16_pair(tmem + b1 * kBN, ad, bd, idesc, acc0 || kk > 0);
+                      mma_s8_pair(tmem + b1 * kBN, smem_desc_sw128(a + (kk >> 2) * kATileBytes + koff),
+                                  smem_desc_sw128(bb2 + (kk >> 2) * kBTileBytes + koff), idesc,
+                                  c > cg || t > 0 || kk > 0);
                     }
                   }
                   mma_commit_pair(&empty[st], kPairMask);
@@ -731,11 +702,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(gemm_threads(kEpiGro
                     ph ^= 1u;
                   }
                 }
+              if (!ok) break;
               mma_commit_pair(&acc_full[b0], kPairMask);
               if (two) mma_commit_pair(&acc_full[b1], kPairMask);
               ai += two ? 2 : 1;
-              return true;
-            });
+            }
           }
           continue;
         }
@@ -954,13 +925,13 @@ cudaError_t split_gemm_launch(const SplitDesc* d_descs, int n, const SplitPlan& 
   {
     std::lock_guard<std::mutex> lock(mu);
     if (dev < 0 || dev >= 64 || !opted_in[dev]) {
-      e = cudaFuncSetAttribute(split_gemm_kernel<kManyEpiGroups, false, false>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem);
+      e = cudaFuncSetAttribute(split_gemm_kernel<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kGemmSmem);
       if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(split_gemm_kernel<4, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        e = cudaFuncSetAttribute(split_gemm_kernel<4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)kGemmSmem);
       if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(split_gemm_kernel<2, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        e = cudaFuncSetAttribute(split_gemm_kernel<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)kGemmSmem);
       if (e != cudaSuccess) return e;
       if (dev >= 0 && dev < 64) opted_in[dev] = true;
@@ -970,12 +941,11 @@ cudaError_t split_gemm_launch(const SplitDesc* d_descs, int n, const SplitPlan& 
   const unsigned pairs = grid_for(plan.tiles, num_sms / 2 > 0 ? num_sms / 2 : 1);
   if (split_chunk_span(plan.slices) != (plan.slices <= 3 ? 2 : 1)) return cudaErrorInvalidValue;
   if (plan.int8)  // one drain per diagonal and tile: two epilogue warpgroups suffice
-    split_gemm_kernel<2, true, false><<<2 * pairs, gemm_threads(2), kGemmSmem, stream>>>(tA, tB, gp);
+    split_gemm_kernel<2, true><<<2 * pairs, gemm_threads(2), kGemmSmem, stream>>>(tA, tB, gp);
   else if (plan.slices <= 3)
-    split_gemm_kernel<4, false, true><<<2 * pairs, gemm_threads(4), kGemmSmem, stream>>>(tA, tB, gp);
+    split_gemm_kernel<4, false><<<2 * pairs, gemm_threads(4), kGemmSmem, stream>>>(tA, tB, gp);
   else
-    split_gemm_kernel<kManyEpiGroups, false, false>
-        <<<2 * pairs, gemm_threads(kManyEpiGroups), kGemmSmem, stream>>>(tA, tB, gp);
+    split_gemm_kernel<2, false><<<2 * pairs, gemm_threads(2), kGemmSmem, stream>>>(tA, tB, gp);
   e = cudaGetLastError();
   if (e == cudaSuccess && launches) *launches += 4;
   return e;
