@@ -165,10 +165,13 @@ void add_combine_desc(const fmm_alg_table& t, const LevelLayout& L, const SubPro
 }
 
 // Dynamic peeling of the fringes of p (linalg/linalg.hpp:201-244).
-void add_peel_descs(const fmm_alg_table& t, const LevelDims& D, const SubProblem& p, std::vector<GemmDesc>* g) {
-  const int64_t xr = D.m - (D.m / t.m0) * t.m0;
-  const int64_t xk = D.k - (D.k / t.k0) * t.k0;
-  const int64_t xc = D.n - (D.n / t.n0) * t.n0;
+// D: p's dimensions, Ch: its children's (level_dims); the fringes are what the
+// m0 x k0 x n0 blocks of Ch leave over.
+void add_peel_descs(const fmm_alg_table& t, const LevelDims& D, const LevelDims& Ch, const SubProblem& p,
+                    std::vector<GemmDesc>* g) {
+  const int64_t xr = D.m - Ch.m * t.m0;
+  const int64_t xk = D.k - Ch.k * t.k0;
+  const int64_t xc = D.n - Ch.n * t.n0;
   if (xk > 0) {  // C(core, core) += A(core, kx) * B(kx, core)
     const int64_t rd = D.m - xr, cdim = D.n - xc, inner = D.k - xk;
     GemmDesc d{};
@@ -436,7 +439,7 @@ class Builder {
       emit_combine(prog_, alg_, 0, l, cd, vec2, items, bytes);
     }
     std::vector<GemmDesc> g;
-    for (int64_t q = 0; q < nf; ++q) add_peel_descs(t_, dims_[l], F[q], &g);
+    for (int64_t q = 0; q < nf; ++q) add_peel_descs(t_, dims_[l], dims_[l + 1], F[q], &g);
     emit_gemm(prog_, l, g, false, &tile_);
   }
 
@@ -476,10 +479,22 @@ void Program::clear() {
   ws_base = nullptr;
 }
 
+// Rows and inner dimension of a block: floor(x / b), one less when that is
+// odd and at least kEvenBlockMin, so that every block of an operand with an
+// even leading dimension starts on a 16-byte boundary (the leaf GEMM's and
+// the formation kernels' 16-byte copies) at the cost of peeling up to
+// 2b - 1 instead of b - 1 rows; the fringe products that take them are
+// padded to whole GEMM tiles either way.
+int64_t block_dim(int64_t x, int b) {
+  const int64_t c = x / b;
+  return (c >= kEvenBlockMin && (c & 1)) ? c - 1 : c;
+}
+
 std::vector<LevelDims> level_dims(const fmm_alg_table& t, int64_t m, int64_t k, int64_t n, int steps) {
   std::vector<LevelDims> d((size_t)steps + 1);
   d[0] = LevelDims{m, k, n};
-  for (int l = 1; l <= steps; ++l) d[l] = LevelDims{d[l - 1].m / t.m0, d[l - 1].k / t.k0, d[l - 1].n / t.n0};
+  for (int l = 1; l <= steps; ++l)
+    d[l] = LevelDims{block_dim(d[l - 1].m, t.m0), block_dim(d[l - 1].k, t.k0), d[l - 1].n / t.n0};
   return d;
 }
 
@@ -701,7 +716,8 @@ void build_batch_program(const BatchItem* items, int count, void* ws, Program* o
       if (steps_of(i) <= l) continue;
       const fmm_alg_table& t = fmm_algorithms[items[i].alg];
       const ItemState& s = st[(size_t)i];
-      for (const SubProblem& p : s.frontier[(size_t)l]) add_peel_descs(t, s.dims[(size_t)l], p, &peel);
+      for (const SubProblem& p : s.frontier[(size_t)l])
+        add_peel_descs(t, s.dims[(size_t)l], s.dims[(size_t)l + 1], p, &peel);
       peel_tiles.resize(peel.size(), items[i].gemm_tile);
     }
     emit_gemm(out, l, peel, false, &peel_tiles);

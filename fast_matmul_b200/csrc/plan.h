@@ -75,8 +75,11 @@ struct LevelDims {
   int64_t m, k, n;
 };
 
-// Dimensions of the sub-problems at each level 0..steps (floor splitting,
-// linalg/linalg.hpp:179-184).
+// Dimensions of the sub-problems at each level 0..steps: floor splitting
+// (linalg/linalg.hpp:179-184), except that block rows and inner dimensions
+// of at least kEvenBlockMin are made even (one more row or inner index goes
+// to the fringe products), which keeps every block view 16-byte aligned.
+constexpr int64_t kEvenBlockMin = 256;
 std::vector<LevelDims> level_dims(const fmm_alg_table& t, int64_t m, int64_t k, int64_t n, int steps);
 
 // Workspace bytes for `dfs_levels` depth-first levels (0 = all breadth-first);

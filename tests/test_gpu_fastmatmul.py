@@ -211,5 +211,7 @@ def test_profile_accounts_every_phase():
     h.profile(False)
     assert p["form_launches"] == 2 and p["gemm_launches"] == 1 and p["combine_launches"] == 2
     assert p["peel_launches"] == 2  # 1031 x 1030 x 1029 leaves fringes at both levels
-    assert p["gemm_flops"] == 2.0 * 49 * 257 * 257 * 257
+    # block rows and inner dimensions of 256 or more are made even: m and k
+    # go 1031 -> 514 -> 256 and 1030 -> 514 -> 256, n 1029 -> 514 -> 257
+    assert p["gemm_flops"] == 2.0 * 49 * 256 * 256 * 257
     assert p["gemm_ms"] > 0 and p["form_ms"] > 0 and p["combine_ms"] > 0
