@@ -400,15 +400,22 @@ class Builder {
         emit_gemm(prog_, l, g, true, &tile_);
       return;
     }
+    // depth-first: one unit per sub-problem, and the fringe products of all
+    // of them in one launch after the last (they touch only their own
+    // operands and C, which live until the parent's combination reads them)
+    std::vector<GemmDesc> peel;
     if (l < d_) {
-      for (const SubProblem& p : F) unit(l, &p, 1);
+      for (const SubProblem& p : F) unit(l, &p, 1, &peel);
     } else {
-      unit(l, F.data(), (int64_t)F.size());
+      unit(l, F.data(), (int64_t)F.size(), &peel);
     }
+    emit_gemm(prog_, l, peel, false, &tile_);
   }
 
  private:
-  void unit(int l, const SubProblem* F, int64_t nf) {
+  // Forms, recurses and combines F[0..nf) as one unit; appends its fringe
+  // products to *peel.
+  void unit(int l, const SubProblem* F, int64_t nf, std::vector<GemmDesc>* peel) {
     const LevelLayout& L = lay_[l];
     const int R = t_.rank;
     double* S = reinterpret_cast<double*>(ws_ + L.off_S);
@@ -438,9 +445,7 @@ class Builder {
       for (int64_t q = 0; q < nf; ++q) add_combine_desc(t_, L, F[q], M + q * R * L.sizeM, &cd, &vec2, &items, &bytes);
       emit_combine(prog_, alg_, 0, l, cd, vec2, items, bytes);
     }
-    std::vector<GemmDesc> g;
-    for (int64_t q = 0; q < nf; ++q) add_peel_descs(t_, dims_[l], dims_[l + 1], F[q], &g);
-    emit_gemm(prog_, l, g, false, &tile_);
+    for (int64_t q = 0; q < nf; ++q) add_peel_descs(t_, dims_[l], dims_[l + 1], F[q], peel);
   }
 
   int alg_;
