@@ -182,6 +182,7 @@ cudaError_t device_checks_arm(const void* ws, size_t bytes, cudaStream_t stream)
   const uintptr_t lo = reinterpret_cast<uintptr_t>(ws);
   cudaError_t e = fmm_checks_arm_tu(CheckRange{lo, ws ? lo + bytes : 0}, stream);
   if (e == cudaSuccess) e = gemm_checks_arm(ws, bytes, stream);
+  if (e == cudaSuccess) e = thin_checks_arm(ws, bytes, stream);
   return e;
 }
 
@@ -189,6 +190,7 @@ cudaError_t device_checks_take(unsigned* word) {
   *word = 0;
   cudaError_t e = fmm_checks_take_tu(word);
   if (e == cudaSuccess) e = gemm_checks_take(word);
+  if (e == cudaSuccess) e = thin_checks_take(word);
   return e;
 }
 

@@ -57,13 +57,33 @@ cudaError_t device_checks_arm(const void* ws, size_t bytes, cudaStream_t stream)
 cudaError_t device_checks_take(unsigned* word);
 cudaError_t gemm_checks_arm(const void* ws, size_t bytes, cudaStream_t stream);
 cudaError_t gemm_checks_take(unsigned* word);
+cudaError_t thin_checks_arm(const void* ws, size_t bytes, cudaStream_t stream);
+cudaError_t thin_checks_take(unsigned* word);
+
+// Fringe products with at most kThinMax rows or columns (thin_gemm.cu): the
+// peeled rows or columns of a sub-problem against its whole inner dimension,
+// on the FP64 pipe with each element of the long operand read once.  A
+// kGemm launch of configuration kGemmTileThin runs them; thin_prepare sets
+// tile_begin / tiles_m of its descriptors to work items.
+constexpr int kGemmTileThin = 3;
+constexpr int kThinMax = 16;
+constexpr int kThinColumnsPerItem = 8;  // few rows: a work item is 8 columns (a warp each)
+constexpr int kThinRowsPerItem = 64;    // few columns: a work item is 64 rows
+__host__ __device__ inline int64_t thin_items(int64_t m, int64_t n) {
+  if (m <= 0 || n <= 0) return 0;
+  return m <= kThinMax ? (n + kThinColumnsPerItem - 1) / kThinColumnsPerItem
+                       : (m + kThinRowsPerItem - 1) / kThinRowsPerItem;
+}
+int64_t thin_prepare(GemmDesc* descs, int n);
+cudaError_t thin_launch(const GemmDesc* d_descs, int n, int64_t total_items, int num_sms, cudaStream_t stream);
 
 // Fills tiles_m / tile_begin / flags for descs[0..n) and returns the total
 // number of tile_m x tile_n tiles.
 int64_t gemm_prepare(GemmDesc* descs, int n, int tile_n = kGemmBN, int tile_m = kGemmBM);
 // Launches the grouped GEMM over descs (device copy) with `total_tiles`
 // tiles of configuration `tile` (kGemmTileLarge or kGemmTileSmall; the
-// descriptors must have been prepared with that configuration's tile).
+// descriptors must have been prepared with that configuration's tile), or
+// with kGemmTileThin the thin kernel over `total_tiles` work items.
 cudaError_t gemm_launch(const GemmDesc* d_descs, int n, int64_t total_tiles, int num_sms, cudaStream_t stream,
                         int tile = kGemmTileLarge);
 

@@ -304,18 +304,24 @@ void emit_gemm(Program* prog, int level, std::vector<GemmDesc>& g, bool leaves, 
     area_small += cols * (double)((g[i].m + kGemmBMSmall - 1) / kGemmBMSmall) * kGemmBMSmall;
   }
   const int auto_cfg = area_large > 1.07 * area_small ? kGemmTileSmall : kGemmTileLarge;
-  std::vector<GemmDesc> part[2];
-  double part_flops[2] = {0.0, 0.0};
+  // fringe products with few rows or columns go to the thin kernel whatever
+  // the tile configuration (which changes no result), so results stay the
+  // same under every configuration
+  auto thin = [&](const GemmDesc& d) { return !leaves && (d.m <= kThinMax || d.n <= kThinMax); };
+  std::vector<GemmDesc> part[3];
+  double part_flops[3] = {0.0, 0.0, 0.0};
   for (size_t i = 0; i < g.size(); ++i) {
     int cfg = asked(i);
     if (cfg == kGemmTileAuto) cfg = auto_cfg;
-    part[cfg == kGemmTileSmall].push_back(g[i]);
-    part_flops[cfg == kGemmTileSmall] += 2.0 * g[i].m * g[i].n * (double)g[i].k;
+    const int c = thin(g[i]) ? 2 : cfg == kGemmTileSmall ? 1 : 0;
+    part[c].push_back(g[i]);
+    part_flops[c] += 2.0 * g[i].m * g[i].n * (double)g[i].k;
   }
-  for (int c = 0; c < 2; ++c) {
+  for (int c = 0; c < 3; ++c) {
     if (part[c].empty()) continue;
-    const int cfg = c ? kGemmTileSmall : kGemmTileLarge;
-    const int64_t ntiles = gemm_prepare(part[c].data(), (int)part[c].size(), kGemmBN, gemm_tile_rows(cfg));
+    const int cfg = c == 2 ? kGemmTileThin : c ? kGemmTileSmall : kGemmTileLarge;
+    const int64_t ntiles = c == 2 ? thin_prepare(part[c].data(), (int)part[c].size())
+                                  : gemm_prepare(part[c].data(), (int)part[c].size(), kGemmBN, gemm_tile_rows(cfg));
     if (ntiles == 0) continue;
     Op op;
     op.kind = OpKind::kGemm;
@@ -501,6 +507,19 @@ std::vector<LevelDims> level_dims(const fmm_alg_table& t, int64_t m, int64_t k, 
   for (int l = 1; l <= steps; ++l)
     d[l] = LevelDims{block_dim(d[l - 1].m, t.m0), block_dim(d[l - 1].k, t.k0), d[l - 1].n / t.n0};
   return d;
+}
+
+int64_t thin_prepare(GemmDesc* descs, int n) {
+  int64_t total = 0;
+  for (int i = 0; i < n; ++i) {
+    GemmDesc& d = descs[i];
+    const int64_t items = thin_items(d.m, d.n);
+    d.tiles_m = (int)items;
+    d.tile_begin = (int)total;
+    d.flags = 0;
+    total += items;
+  }
+  return total;
 }
 
 int64_t gemm_prepare(GemmDesc* descs, int n, int tile_n, int tile_m) {
