@@ -22,7 +22,7 @@
 // result tells the orders apart), and consecutive k16 MMAs chain through
 // the accumulator registers.  A dot product of length k summed that way in
 // one chain has a rounding error that grows like sqrt(k) ulps of its final
-// value.  So the k loop is cut into blocks of kFlushSlices slices (256 k): a
+// value.  So the k loop is cut into blocks of kFlushK = 256 k: a
 // block is chained in registers as above, then added with one FP64 add into
 // a per-thread running sum kept in tensor memory (which this kernel does not
 // otherwise use: each thread owns one TMEM lane, 32 columns per 16 doubles),
@@ -52,7 +52,7 @@ using sm100::tmem_st_32x32b_x8;
 using sm100::tmem_st_wait;
 
 // k-slices per block of the blocked sum (BK = 32: 256 k per block).
-constexpr int kFlushSlices = 8;
+constexpr int kFlushK = 256;  // k indices per block of the running sum (every configuration)
 
 // 64-bit shared loads are served per half-warp: a fragment load is
 // conflict-free when the 16 lanes of each half (4 row groups x 4 k lanes)
@@ -86,6 +86,7 @@ struct GemmCfg {
   static_assert(SMEM_BYTES * MINB <= 227 * 1024, "shared memory budget");
   static_assert(THREADS % (BK / 2) == 0 && THREADS % (BM / 2) == 0, "copy mapping");
   static_assert((A_LD * 8) % 128 == 32, "conflict-free A fragments");
+  static_assert(kFlushK % BK == 0, "slices tile the running-sum blocks");
 };
 
 // 128 x 64 tiles, 4 warps, 32-deep slices, 2 stages, two CTAs per SM: one
@@ -95,8 +96,12 @@ struct GemmCfg {
 using DefaultGemmCfg = GemmCfg<32, 2, kGemmBN, 2, kGemmBM, 64>;
 // 64 x 64 tiles, 4 warps of 32 x 32, three CTAs per SM: less padding on
 // problems whose rows are just above a multiple of 64, more CTAs to hide the
-// latency of short k loops.
-using SmallGemmCfg = GemmCfg<32, 2, kGemmBN, 3, kGemmBMSmall, 32>;
+// latency of short k loops; 16-deep slices in 4 stages (3 in flight) for
+// the same reason (the 4096-product batch 21.9 against 21.1 TFLOP/s with 32
+// x 2; the 128 x 64 tiles are faster with 32 x 2: 47.6 against 46.9 on the
+// headline's leaves).  Both sum every output in the same 256-k blocks, so
+// their results are identical.
+using SmallGemmCfg = GemmCfg<16, 4, kGemmBN, 3, kGemmBMSmall, 32>;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -379,7 +384,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
           for (int nt = 0; nt < 4; ++nt) dmma_16x8x16(acc[mt][nt], af, bf[nt]);
         }
       }
-      if ((kt + 1) % kFlushSlices == 0 && kt + 1 < ktiles) flush();
+      if ((kt + 1) % (kFlushK / BK) == 0 && kt + 1 < ktiles) flush();
     }
     cp_async_wait<0>();
     __syncthreads();  // shared buffers are refilled by the next tile
