@@ -76,7 +76,9 @@ typedef enum fmm_schedule {
  *               accumulation over k groups of up to 32768, recombined in
  *               FP64.  Error of one leaf product:
  *               |C - AB|_ij <~ (S + 2) * 2^-7S * k * max|A_i.| * max|B_.j|;
- *               6 slices are about as accurate as 5 BF16 slices. */
+ *               6 slices are about as accurate as 5 BF16 slices.
+ * In both split forms a row of a leaf A or a column of a leaf B that holds an
+ * Inf or a NaN makes every entry of that leaf's product it reaches NaN. */
 typedef enum fmm_precision {
   FMM_PRECISION_FP64 = 0,
   FMM_PRECISION_SPLIT_BF16 = 1,
