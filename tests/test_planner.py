@@ -119,3 +119,28 @@ def test_batch_program_matches_oracle_per_item():
         oracle.fast_matmul(alg, Ai, Bi, want, s, 1e-8, 1.25, 0.5)
         got = np.asfortranarray(C[c_off[i]:c_off[i] + m * n].reshape(n, m).T)
         assert np.array_equal(want, got), (i, alg, s, m, k, n)
+
+
+def test_even_blocks_agree_across_schedules_and_with_the_oracle():
+    """Block rows and inner dimensions of 256 or more are made even (one more
+    row or inner index peeled), so 1031 x 1030 x 1029 splits as 1031 -> 514
+    -> 256 where the reference's floor splitting gives 515 -> 257: the
+    programs differ from the oracle's recursion, every depth-first split of
+    them gives the same bits, and the result stays within rounding of the
+    oracle's."""
+    E = emulator()
+    idx = NAMES.index("strassen")
+    m, k, n = 1031, 1030, 1029
+    A = oracle.uniform(m, k, 41, 1)
+    B = oracle.uniform(k, n, 41, 2)
+    C0 = oracle.uniform(m, n, 41, 3)
+    want = C0.copy(order="F")
+    oracle.fast_matmul("strassen", A, B, want, 2, 1e-8, 1.25, -0.5)
+    got = []
+    for d in range(3):
+        C = C0.copy(order="F")
+        run_emu(E, idx, A, B, C, 2, 1e-8, 1.25, -0.5, d)
+        got.append(C)
+    for C in got[1:]:
+        assert np.array_equal(C, got[0])
+    assert float(np.abs(got[0] - want).max() / np.abs(want).max()) <= 1e-13
