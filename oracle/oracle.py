@@ -89,11 +89,32 @@ def ref_available() -> bool:
     return os.path.exists(REF_LIB)
 
 
+def _pin_blas_kernels() -> None:
+    """The reference build's BLAS (OpenBLAS with run-time kernel dispatch)
+    picks its DGEMM kernels by CPU model, and kernels for different models
+    sum in different orders.  The committed reference digests were made with
+    its SkylakeX (AVX-512) kernels; on a CPU with AVX-512 the same kernels
+    are selected here, before the library loads, so the leaf products of the
+    reference build give the same bits on every such host.  (Without
+    AVX-512 those kernels cannot run; the default choice stays and
+    bit-for-bit pins against the digests may then differ.)"""
+    if "OPENBLAS_CORETYPE" in os.environ:
+        return
+    try:
+        with open("/proc/cpuinfo") as fh:
+            flags = fh.read()
+    except OSError:
+        return
+    if " avx512f" in flags and " avx512dq" in flags and " avx512vl" in flags:
+        os.environ["OPENBLAS_CORETYPE"] = "SkylakeX"
+
+
 def ref_lib() -> Optional[ctypes.CDLL]:
     global _ref
     if _ref is None:
         if not ref_available():
             return None
+        _pin_blas_kernels()
         L = ctypes.CDLL(REF_LIB)
         L.fmmref_fast_matmul.argtypes = [ctypes.c_char_p, _P, _I, _P, _I, _P, _I, _I, _I, _I, _I, _D, _D, _D]
         L.fmmref_fast_matmul.restype = _D
