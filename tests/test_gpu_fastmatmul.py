@@ -4,6 +4,8 @@
 * every generated algorithm against the CPU oracle;
 * the reference's extra alpha/beta GEMM cases (tests/matmul_tests.cpp:47-135);
 * the DFS / BFS / HYBRID schedules give bit-identical results;
+* Inf and NaN inputs spread to exactly the entries they reach in the
+  reference (the oracle's result);
 * the host-memory entry point equals the device entry point;
 * at full size (4096^3), the error against the classical product stays at
   the level the reference reports for exact algorithms.
@@ -217,3 +219,30 @@ def test_profile_accounts_every_phase():
     # go 1031 -> 514 -> 256 and 1030 -> 514 -> 256, n 1029 -> 514 -> 257
     assert p["gemm_flops"] == 2.0 * 49 * 256 * 256 * 257
     assert p["gemm_ms"] > 0 and p["form_ms"] > 0 and p["combine_ms"] > 0
+
+
+@pytest.mark.parametrize("alg,shape,steps", [("strassen", (300, 280, 260), 2), ("grey333_23_125", (190, 200, 170), 1),
+                                             ("grey424_26_206", (203, 150, 201), 1)])
+def test_non_finite_inputs_propagate_like_the_reference(alg, shape, steps):
+    """FP64 forms: an Inf or a NaN in A or B spreads through the S/T
+    formations, the leaf products and the M -> C combinations exactly as in
+    the reference, whose additions the engine repeats term for term (a sum's
+    class -- NaN, +-Inf or finite -- does not depend on its order), so the
+    NaN and Inf entries of C are those of the oracle's result and the finite
+    ones agree within the parity tolerance."""
+    m, k, n = shape
+    A = oracle.uniform(m, k, 17, 1)
+    B = oracle.uniform(k, n, 17, 2)
+    C0 = oracle.uniform(m, n, 17, 3)
+    A[7, 33] = np.nan
+    A[100, 5] = np.inf
+    B[k - 3, 17] = -np.inf
+    want = C0.copy(order="F")
+    oracle.fast_matmul(alg, A, B, want, steps, 1e-8, 1.0, 0.5)
+    got = gpu_fast(alg, A, B, C0, steps, 1e-8, 1.0, 0.5)
+    assert np.isnan(want).any() and np.isinf(want).any()
+    assert np.array_equal(np.isnan(got), np.isnan(want))
+    assert np.array_equal(np.isposinf(got), np.isposinf(want))
+    assert np.array_equal(np.isneginf(got), np.isneginf(want))
+    fin = np.isfinite(want)
+    assert float(np.abs(got[fin] - want[fin]).max() / np.abs(want[fin]).max()) <= EXACT_TOL
