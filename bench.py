@@ -577,7 +577,7 @@ def run_ours(a):
             "workspace_bytes": fmm.workspace_bytes(a.alg, m, k, n, a.num_steps, a.schedule, handle=h),
         }
         if world == 1 and not a.no_extras:
-            # the north star's secondary targets, each with its own clock record
+            # the precision, batch and serving records, each with its own clock record
             out["precision"] = precision_record(a, fmm, h, A, B, Cc, classical_tf, cublas_tf)
             del A, B, C, Cc
             h.release_workspace()

@@ -49,7 +49,7 @@ inline int gemm_tile_rule(int m) {
 }
 
 // Device-side checks of the descriptor walks (device_checks.cuh; built in
-// with -DFMM_DEVICE_CHECKS): whether this build has them, registering the
+// with -DFMM_DEVICE_CHECKS): whether the library was compiled with them, registering the
 // workspace of the program about to run, and reading (and clearing) the
 // word of failed checks.  Without them, arming and reading do nothing.
 bool device_checks_built();
