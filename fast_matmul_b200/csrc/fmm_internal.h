@@ -122,8 +122,11 @@ __host__ __device__ inline bool split_code_int8(int code) { return code >= kSpli
 // diagonals 2..S-1 of the first chunk and of the second (a last single chunk
 // forms its own pair).  Pairs are used at 3 slices or fewer, where they save
 // a third of the drains; with more slices every chunk forms its own group
-// set (diagonals 0..S-1), which measured faster on Strassen's leaf launches.  With digits |d_1| <= 256 and |d_t| <= 128 every FP32
-// partial sum of a group stays an integer of magnitude <= 2^24 -- diagonals
+// set (diagonals 0..S-1), which measured faster on Strassen's leaf launches
+// and on single products (pairs at 5 slices: 1000 against 1045 TFLOP/s at
+// 4096^3, Strassen 2 steps -1.3%; at 4 slices +2%).  With digits
+// |d_1| <= 256 and |d_t| <= 128 every FP32 partial sum of a group stays an
+// integer of magnitude <= 2^24 -- diagonals
 // 0 and 1 add at most 2^16 per k over 256 k, diagonal D >= 2 at most
 // (D + 3) 2^14 per k over 128 k -- so the tensor cores accumulate each group
 // exactly, and the FP64 recombination adds the groups in this order.
