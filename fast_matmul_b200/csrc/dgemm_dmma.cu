@@ -494,7 +494,8 @@ cudaError_t gemm_checks_take(unsigned* word) { return fmm_checks_take_tu(word); 
 
 cudaError_t gemm_launch(const GemmDesc* d_descs, int n, int64_t total_tiles, int num_sms, cudaStream_t stream,
                         int tile) {
-  if (tile == kGemmTileThin) return thin_launch(d_descs, n, total_tiles, num_sms, stream);
+  if (tile == kGemmTileThin || tile == kGemmTileThinInner)
+    return thin_launch(d_descs, n, total_tiles, num_sms, stream, tile == kGemmTileThinInner);
   if (tile == kGemmTileSmall) return gemm_launch_cfg<SmallGemmCfg>(d_descs, n, total_tiles, num_sms, stream);
   return gemm_launch_cfg<DefaultGemmCfg>(d_descs, n, total_tiles, num_sms, stream);
 }

@@ -60,22 +60,30 @@ cudaError_t gemm_checks_take(unsigned* word);
 cudaError_t thin_checks_arm(const void* ws, size_t bytes, cudaStream_t stream);
 cudaError_t thin_checks_take(unsigned* word);
 
-// Fringe products with at most kThinMax rows or columns (thin_gemm.cu): the
-// peeled rows or columns of a sub-problem against its whole inner dimension,
-// on the FP64 pipe with each element of the long operand read once.  A
-// kGemm launch of configuration kGemmTileThin runs them; thin_prepare sets
-// tile_begin / tiles_m of its descriptors to work items.
+// Fringe products with at most kThinMax rows, columns or inner indices
+// (thin_gemm.cu): the peeled rows or columns of a sub-problem against its
+// whole inner dimension, and the update of its core by its peeled inner
+// indices, on the FP64 pipe with each element of the long operand (or of C)
+// read once.  A kGemm launch of configuration kGemmTileThin runs those with
+// few rows or columns, one of kGemmTileThinInner those with few inner
+// indices only; thin_prepare sets tile_begin / tiles_m of their descriptors
+// to work items.
 constexpr int kGemmTileThin = 3;
+constexpr int kGemmTileThinInner = 4;
 constexpr int kThinMax = 16;
 constexpr int kThinColumnsPerItem = 8;  // few rows: a work item is 8 columns (a warp each)
 constexpr int kThinRowsPerItem = 64;    // few columns: a work item is 64 rows
-__host__ __device__ inline int64_t thin_items(int64_t m, int64_t n) {
+constexpr int kThinBlock = 64;          // few inner indices: a work item is a 64 x 64 block of C
+__host__ __device__ inline int64_t thin_items(int64_t m, int64_t n, int64_t k) {
   if (m <= 0 || n <= 0) return 0;
-  return m <= kThinMax ? (n + kThinColumnsPerItem - 1) / kThinColumnsPerItem
-                       : (m + kThinRowsPerItem - 1) / kThinRowsPerItem;
+  if (m <= kThinMax) return (n + kThinColumnsPerItem - 1) / kThinColumnsPerItem;
+  if (n <= kThinMax) return (m + kThinRowsPerItem - 1) / kThinRowsPerItem;
+  (void)k;  // k <= kThinMax
+  return ((m + kThinBlock - 1) / kThinBlock) * ((n + kThinBlock - 1) / kThinBlock);
 }
 int64_t thin_prepare(GemmDesc* descs, int n);
-cudaError_t thin_launch(const GemmDesc* d_descs, int n, int64_t total_items, int num_sms, cudaStream_t stream);
+cudaError_t thin_launch(const GemmDesc* d_descs, int n, int64_t total_items, int num_sms, cudaStream_t stream,
+                        bool inner);
 
 // Fills tiles_m / tile_begin / flags for descs[0..n) and returns the total
 // number of tile_m x tile_n tiles.
@@ -83,7 +91,8 @@ int64_t gemm_prepare(GemmDesc* descs, int n, int tile_n = kGemmBN, int tile_m = 
 // Launches the grouped GEMM over descs (device copy) with `total_tiles`
 // tiles of configuration `tile` (kGemmTileLarge or kGemmTileSmall; the
 // descriptors must have been prepared with that configuration's tile), or
-// with kGemmTileThin the thin kernel over `total_tiles` work items.
+// with kGemmTileThin / kGemmTileThinInner the thin kernels over
+// `total_tiles` work items.
 cudaError_t gemm_launch(const GemmDesc* d_descs, int n, int64_t total_tiles, int num_sms, cudaStream_t stream,
                         int tile = kGemmTileLarge);
 

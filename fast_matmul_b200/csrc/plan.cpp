@@ -304,23 +304,28 @@ void emit_gemm(Program* prog, int level, std::vector<GemmDesc>& g, bool leaves, 
     area_small += cols * (double)((g[i].m + kGemmBMSmall - 1) / kGemmBMSmall) * kGemmBMSmall;
   }
   const int auto_cfg = area_large > 1.07 * area_small ? kGemmTileSmall : kGemmTileLarge;
-  // fringe products with few rows or columns go to the thin kernel whatever
+  // fringe products with few rows, columns or inner indices go to the thin kernel whatever
   // the tile configuration (which changes no result), so results stay the
   // same under every configuration
-  auto thin = [&](const GemmDesc& d) { return !leaves && (d.m <= kThinMax || d.n <= kThinMax); };
-  std::vector<GemmDesc> part[3];
-  double part_flops[3] = {0.0, 0.0, 0.0};
+  // parts: 0 large tiles, 1 small tiles, 2 few rows or columns, 3 few inner indices
+  auto part_of = [&](const GemmDesc& d, int cfg) {
+    if (!leaves && (d.m <= kThinMax || d.n <= kThinMax)) return 2;
+    if (!leaves && d.k <= kThinMax) return 3;
+    return cfg == kGemmTileSmall ? 1 : 0;
+  };
+  std::vector<GemmDesc> part[4];
+  double part_flops[4] = {0.0, 0.0, 0.0, 0.0};
   for (size_t i = 0; i < g.size(); ++i) {
     int cfg = asked(i);
     if (cfg == kGemmTileAuto) cfg = auto_cfg;
-    const int c = thin(g[i]) ? 2 : cfg == kGemmTileSmall ? 1 : 0;
+    const int c = part_of(g[i], cfg);
     part[c].push_back(g[i]);
     part_flops[c] += 2.0 * g[i].m * g[i].n * (double)g[i].k;
   }
-  for (int c = 0; c < 3; ++c) {
+  for (int c = 0; c < 4; ++c) {
     if (part[c].empty()) continue;
-    const int cfg = c == 2 ? kGemmTileThin : c ? kGemmTileSmall : kGemmTileLarge;
-    const int64_t ntiles = c == 2 ? thin_prepare(part[c].data(), (int)part[c].size())
+    const int cfg = c == 3 ? kGemmTileThinInner : c == 2 ? kGemmTileThin : c ? kGemmTileSmall : kGemmTileLarge;
+    const int64_t ntiles = c >= 2 ? thin_prepare(part[c].data(), (int)part[c].size())
                                   : gemm_prepare(part[c].data(), (int)part[c].size(), kGemmBN, gemm_tile_rows(cfg));
     if (ntiles == 0) continue;
     Op op;
@@ -513,7 +518,7 @@ int64_t thin_prepare(GemmDesc* descs, int n) {
   int64_t total = 0;
   for (int i = 0; i < n; ++i) {
     GemmDesc& d = descs[i];
-    const int64_t items = thin_items(d.m, d.n);
+    const int64_t items = thin_items(d.m, d.n, d.k);
     d.tiles_m = (int)items;
     d.tile_begin = (int)total;
     d.flags = 0;

@@ -18,8 +18,16 @@
 //     four groups of threads per row block, group g taking the g-th quarter
 //     of k in 256-deep blocks into a running sum; the four sums are added
 //     (g0 + g1) + (g2 + g3).
-// A work item is 8 columns (few rows) or 64 rows (few columns) of one problem;
-// tile_begin / tiles_m of the descriptors count work items (thin_prepare).
+//   * few inner indices (k <= kThinMax, the k fringe C_core += A(:, kx)
+//     B(kx, :)): a 64 x 64 block of C per work item, a thread per pair of
+//     rows and 8 columns; C is read and written once with 16-byte accesses
+//     where it allows them, the short panels come from L1 / L2, and each
+//     entry is the FMA chain over k in order plus +0 (what the tensor-core
+//     GEMM's zero-padded MMA steps add), times alpha, plus beta C -- the
+//     bits the tensor-core GEMM gives, at the cost of one pass over C.
+// A work item is 8 columns (few rows), 64 rows (few columns) or a 64 x 64
+// block (few inner indices) of one problem; tile_begin / tiles_m of the
+// descriptors count work items (thin_prepare).
 
 #include <cuda_runtime.h>
 
@@ -42,7 +50,7 @@ struct ThinSmem {
   double part[kColsGroups - 1][kColsRows][kThinMax + 1];  // few columns: sums of k groups 1..3
 };
 
-__device__ __forceinline__ int64_t item_count(const GemmDesc& d) { return thin_items(d.m, d.n); }
+__device__ __forceinline__ int64_t item_count(const GemmDesc& d) { return thin_items(d.m, d.n, d.k); }
 
 template <int MAXM>
 __device__ void few_rows(const GemmDesc& d, int local) {
@@ -137,6 +145,71 @@ __device__ void few_columns(const GemmDesc& d, int local, ThinSmem& sm) {
     }
 }
 
+// C(r..r+1, c0..c0+7) of a problem with few inner indices.
+__device__ void few_inner(const GemmDesc& d, int local) {
+  const int tid = threadIdx.x;
+  const int rp = tid & 31, cg = tid >> 5;  // row pair, column group (a warp: 64 rows of 8 columns)
+  const int blocks_m = (d.m + kThinBlock - 1) / kThinBlock;
+  const int r = (local % blocks_m) * kThinBlock + 2 * rp;
+  const int c0 = (local / blocks_m) * kThinBlock + cg * 8;
+  if (r >= d.m || c0 >= d.n) return;
+  const bool r1 = r + 1 < d.m;
+  const int K = d.k;
+  const double* __restrict__ A = d.A;
+  const double* __restrict__ B = d.B;
+  const int64_t lda = d.lda, ldb = d.ldb, ldc = d.ldc;
+  double* const Cp = d.C;
+  const bool pair = r1 && (reinterpret_cast<uintptr_t>(Cp) & 15) == 0 && (ldc & 1) == 0;  // r is even
+  const double alpha = d.alpha, beta = d.beta;
+  // C first: its loads are in flight while the short panels are multiplied
+  double cin[8][2];
+  if (beta != 0.0) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const double* cp = Cp + r + (int64_t)(c0 + j) * ldc;
+      if (c0 + j >= d.n) {
+        cin[j][0] = cin[j][1] = 0.0;
+      } else if (pair) {
+        const double2 v = *reinterpret_cast<const double2*>(cp);
+        cin[j][0] = v.x;
+        cin[j][1] = v.y;
+      } else {
+        cin[j][0] = cp[0];
+        cin[j][1] = r1 ? cp[1] : 0.0;
+      }
+    }
+  }
+  double acc[8][2];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) acc[j][0] = acc[j][1] = 0.0;
+  for (int p = 0; p < K; ++p) {
+    const double a0 = A[r + (int64_t)p * lda], a1 = r1 ? A[r + 1 + (int64_t)p * lda] : 0.0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const double b = c0 + j < d.n ? B[p + (int64_t)(c0 + j) * ldb] : 0.0;
+      acc[j][0] = fma(a0, b, acc[j][0]);
+      acc[j][1] = fma(a1, b, acc[j][1]);
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    if (c0 + j >= d.n) continue;
+    double* cp = Cp + r + (int64_t)(c0 + j) * ldc;
+    // the padded MMA steps of the tensor-core GEMM add +0 after the last k
+    double v0 = alpha * (acc[j][0] + 0.0), v1 = alpha * (acc[j][1] + 0.0);
+    if (beta != 0.0) {
+      v0 += beta * cin[j][0];
+      v1 += beta * cin[j][1];
+    }
+    if (pair) {
+      *reinterpret_cast<double2*>(cp) = make_double2(v0, v1);
+    } else {
+      cp[0] = v0;
+      if (r1) cp[1] = v1;
+    }
+  }
+}
+
 __global__ void __launch_bounds__(kThreads) thin_gemm_kernel(const GemmDesc* __restrict__ descs, int nprob,
                                                              int total) {
   __shared__ ThinSmem sm;
@@ -176,6 +249,29 @@ __global__ void __launch_bounds__(kThreads) thin_gemm_kernel(const GemmDesc* __r
   }
 }
 
+// Problems with few inner indices only (a launch of its own, so that its
+// registers are its own).
+__global__ void __launch_bounds__(kThreads, 2) thin_inner_kernel(const GemmDesc* __restrict__ descs, int nprob,
+                                                              int total) {
+  for (int item = blockIdx.x; item < total; item += gridDim.x) {
+    int lo = 0, hi = nprob - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (descs[mid].tile_begin <= item)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    const GemmDesc& d = descs[lo];
+    const int local = item - d.tile_begin;
+    if (!FMM_CHECK(lo >= 0 && lo < nprob && local >= 0 && local < item_count(d) && d.m > kThinMax &&
+                       d.n > kThinMax && d.k <= kThinMax,
+                   kCheckGemmProblem))
+      continue;
+    few_inner(d, local);
+  }
+}
+
 }  // namespace
 
 cudaError_t thin_checks_arm(const void* ws, size_t bytes, cudaStream_t stream) {
@@ -185,12 +281,16 @@ cudaError_t thin_checks_arm(const void* ws, size_t bytes, cudaStream_t stream) {
 
 cudaError_t thin_checks_take(unsigned* word) { return fmm_checks_take_tu(word); }
 
-cudaError_t thin_launch(const GemmDesc* d_descs, int n, int64_t total_items, int num_sms, cudaStream_t stream) {
+cudaError_t thin_launch(const GemmDesc* d_descs, int n, int64_t total_items, int num_sms, cudaStream_t stream,
+                        bool inner) {
   if (total_items <= 0 || n <= 0) return cudaSuccess;
   if (total_items >= (int64_t(1) << 31)) return cudaErrorInvalidValue;
-  const int64_t cap = (int64_t)num_sms * 4;
+  const int64_t cap = (int64_t)num_sms * (inner ? 8 : 4);
   const int64_t grid = total_items < cap ? total_items : cap;
-  thin_gemm_kernel<<<(unsigned)grid, kThreads, 0, stream>>>(d_descs, n, (int)total_items);
+  if (inner)
+    thin_inner_kernel<<<(unsigned)grid, kThreads, 0, stream>>>(d_descs, n, (int)total_items);
+  else
+    thin_gemm_kernel<<<(unsigned)grid, kThreads, 0, stream>>>(d_descs, n, (int)total_items);
   return cudaGetLastError();
 }
 

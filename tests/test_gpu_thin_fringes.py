@@ -4,7 +4,9 @@ Dynamic peeling (linalg/linalg.hpp:201-244) leaves, at each level, a row
 fringe C(mx, :) = A(mx, :) B and a column fringe C(:, nx) = A B(:, nx) of
 1..2 m0 - 1 rows (blocks of 256 or more rows are made even) and 1..n0 - 1
 columns against the level's whole inner dimension; these run on the thin
-kernel, whose sums are sized for 4, 8 or 16 rows or columns.  The shapes
+kernel, whose sums are sized for 4, 8 or 16 rows or columns, and the k
+fringe C_core += A(:, kx) B(kx, :) of 1..2 k0 - 1 inner indices runs on its
+block kernel (16-byte C accesses where C allows them).  The shapes
 below reach each of those paths (with alpha / beta, odd leading
 dimensions' views, and depth-first levels whose sibling fringes share one
 launch), and the result must match the CPU oracle's FastMatmul within the
@@ -30,6 +32,7 @@ CASES = [
     ("smirnov336_40_960", 3 * 270 + 2, 3 * 100 + 1, 6 * 60 + 5, 1),   # 2 rows, 5 columns (8-wide)
     ("grey333_23_125", 3 * (3 * 90 + 2) + 2, 3 * (3 * 60 + 1) + 1, 3 * (3 * 70 + 2) + 2, 2),  # both levels
     ("strassen", 2 * 255 + 1, 2 * 254 + 1, 2 * 253 + 1, 2),  # 1 row and column at both levels
+    ("smirnov363_40_960", 3 * 200 + 1, 6 * 258 + 11, 3 * 150 + 2, 1),  # 11 inner indices (the k fringe)
 ]
 
 
