@@ -49,7 +49,10 @@ typedef enum fmm_status {
  *           least two depth-first levels when num_steps >= 3 (one
  *           depth-first level plans exactly like BFS, since the top level
  *           has a single sub-problem).
- *   AUTO    breadth-first as deep as the workspace limit allows. */
+ *   AUTO    BFS for num_steps <= 2 (or the shallowest split that fits the
+ *           workspace limit), HYBRID for num_steps >= 3, which measured as
+ *           fast as BFS or faster there (no result changes: every schedule
+ *           gives the same bits). */
 typedef enum fmm_schedule {
   FMM_SCHEDULE_AUTO = 0,
   FMM_SCHEDULE_DFS = 1,
