@@ -246,3 +246,17 @@ def test_non_finite_inputs_propagate_like_the_reference(alg, shape, steps):
     assert np.array_equal(np.isneginf(got), np.isneginf(want))
     fin = np.isfinite(want)
     assert float(np.abs(got[fin] - want[fin]).max() / np.abs(want[fin]).max()) <= EXACT_TOL
+
+
+def test_auto_schedule_takes_the_hybrid_split_from_three_steps():
+    """AUTO plans breadth-first up to 2 steps and with two depth-first levels
+    from 3 steps on (the workspace query reports the chosen split's bytes),
+    and every split gives the same bits."""
+    ws = lambda steps, sched: fmm.workspace_bytes("strassen", 1024, 1024, 1024, steps, sched)
+    assert ws(2, "auto") == ws(2, "bfs")
+    assert ws(3, "auto") == ws(3, "hybrid") < ws(3, "bfs")
+    A = oracle.uniform(300, 280, 9, 1)
+    B = oracle.uniform(280, 290, 9, 2)
+    C0 = oracle.uniform(300, 290, 9, 3)
+    got = {s: gpu_fast("strassen", A, B, C0, 3, 1e-8, 1.0, 0.5, schedule=s) for s in ("auto", "bfs", "dfs")}
+    assert np.array_equal(got["auto"], got["bfs"]) and np.array_equal(got["auto"], got["dfs"])
